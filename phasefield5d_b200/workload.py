@@ -1,0 +1,310 @@
+"""Seeded synthetic workloads for the Cahn-Hilliard step loop.
+
+The real ThermoCalc tables of phasefield5d are not distributed, so solves run
+on a synthetic regular-solution table with the same column semantics
+(data/FeMnNiCoCu_fcc/DATA_FORMAT.md; phasefield5d/thermodynamics/io.py:9-33):
+
+* rows on every node of the 4D composition simplex at spacing ``resolution``,
+  columns [x1..x4, μ1..μ4, M_Fe, M1..M4] (five mobilities, Fe first);
+* G = RT Σ_a x_a ln x_a + Σ_{a<b} Ω_ab x_a x_b over the five species, with
+  x_0 = 1 − Σx (Fe, dependent) and x clipped to ≥ 1e-12 inside the log;
+  μ_i = ∂G/∂x_i = RT(ln x_i − ln x_0) + Σ_b Ω_ib x_b − Σ_b Ω_0b x_b;
+* Ω_ab ~ U[5, 25] kJ/mol from ``numpy.random.default_rng(seed)``;
+* M_a = exp(N(−30, 0.5)) per node and species.
+
+Ω seeds are rejection-sampled: a seed is accepted only when the reference
+setup (FD Hessian + elastic term + kinetic scan) finds an unstable mode at
+X0, since otherwise the CTLD setup raises ``ValueError``.
+
+Everything here is host setup; it produces the inputs (table, initial field,
+scalars, B(k)) that the device step consumes.
+"""
+from __future__ import annotations
+
+import math
+from dataclasses import dataclass, field
+
+import numpy as np
+
+from .solver import system as sysm
+from .solver import elastic_setup as els
+from .solver.table import build_4d_grid, build_calphad_kdtree, host_table_eval, node_coordinates
+
+R_GAS = 8.314462618  # J/(mol K)
+
+# Partial molar volumes [m^3/mol] of Fe, Mn, Ni, Co, Cu (atomic weight / density).
+MOLAR_VOLUMES_FEMNNICOCU = np.array([7.09e-6, 7.35e-6, 6.59e-6, 6.67e-6, 7.11e-6])
+ELEMENTS = ["Fe", "Mn", "Ni", "Co", "Cu"]
+
+
+# ---------------------------------------------------------------------------
+# Synthetic CALPHAD table
+# ---------------------------------------------------------------------------
+
+def simplex_node_indices(n):
+    """All (i1..i4) with i_d >= 0 and Σ i_d <= n-1, lexicographic order."""
+    N = n - 1
+    out = []
+    for a in range(n):
+        for b in range(n - a):
+            for c in range(n - a - b):
+                m = N - a - b - c + 1
+                blk = np.empty((m, 4), dtype=np.int64)
+                blk[:, 0] = a
+                blk[:, 1] = b
+                blk[:, 2] = c
+                blk[:, 3] = np.arange(m)
+                out.append(blk)
+    return np.concatenate(out, axis=0)
+
+
+def draw_omega(seed):
+    """Symmetric 5×5 interaction matrix, zero diagonal, upper triangle in row
+    order drawn U[5, 25] kJ/mol (returned in J/mol)."""
+    rng = np.random.default_rng(seed)
+    om = np.zeros((5, 5))
+    iu = np.triu_indices(5, k=1)
+    vals = rng.uniform(5.0e3, 25.0e3, size=len(iu[0]))
+    om[iu] = vals
+    om[(iu[1], iu[0])] = vals
+    return om, rng
+
+
+@dataclass
+class SyntheticTable:
+    resolution: float
+    temperature: float
+    seed: int
+    omega: np.ndarray
+    data: np.ndarray           # (rows, 13): x1..x4, mu1..mu4, M_Fe, M1..M4
+
+    @property
+    def n(self):
+        return int(round(1.0 / self.resolution)) + 1
+
+    def dataframe(self):
+        import pandas as pd
+        cols = ([f"X_{e}" for e in ELEMENTS[1:]] + [f"Gx_{e}" for e in ELEMENTS[1:]]
+                + [f"Mob_{e}" for e in ELEMENTS])
+        return pd.DataFrame(self.data, columns=cols)
+
+
+def make_table(resolution, temperature, seed):
+    """Regular-solution table on all simplex nodes (see module docstring).
+
+    Node coordinates are the doubles nearest the decimals k·res, as a parsed
+    text table would hold them.  Logs are taken on the n distinct axis values
+    with ``math.log`` so the table is the same on every host.
+    """
+    n = int(round(1.0 / resolution)) + 1
+    N = n - 1
+    axis = np.round(np.arange(n) * resolution, 12)
+    idx = simplex_node_indices(n)
+    i0 = N - idx.sum(axis=1)
+    xs = [axis[i0]] + [axis[idx[:, d]] for d in range(4)]   # species 0..4
+    logs = np.array([math.log(max(v, 1e-12)) for v in axis])
+    omega, rng = draw_omega(seed)
+    RT = R_GAS * float(temperature)
+    rows = idx.shape[0]
+    data = np.empty((rows, 13))
+    for d in range(4):
+        data[:, d] = xs[d + 1]
+    for i in range(1, 5):
+        ideal = RT * (logs[idx[:, i - 1]] - logs[i0])
+        inter = np.zeros(rows)
+        for b in range(5):
+            inter = inter + omega[i, b] * xs[b]
+        ref = np.zeros(rows)
+        for b in range(5):
+            ref = ref + omega[0, b] * xs[b]
+        data[:, 3 + i] = ideal + inter - ref
+    logm = rng.normal(-30.0, 0.5, size=(rows, 5))
+    data[:, 8:13] = np.exp(logm)
+    return SyntheticTable(float(resolution), float(temperature), int(seed), omega, data)
+
+
+# ---------------------------------------------------------------------------
+# Solve configuration and host setup
+# ---------------------------------------------------------------------------
+
+@dataclass
+class SolveConfig:
+    """Per-solve parameters; field names follow phasefield5d's SimulationConfig
+    (phasefield5d/solver/config.py:30-71) where one exists."""
+    system_dim: int = 1
+    initial_composition: tuple = (0.1, 0.2, 0.2, 0.3)
+    fluctuation: float = 1e-3
+    mw: int = 80
+    ppw: int = 16
+    kappa_value: float = 5e-16
+    kappa_i: tuple = (1.0, 1.0, 1.0, 1.0)
+    resolution: float = 0.025
+    temperature: float = 873.0
+    include_cubic_anisotropy: bool = True
+    direction: tuple = (1, 0, 0)
+    c11: float = 240.0
+    c12: float = 150.0
+    c44: float = 120.0
+    steps_per_ctld: int = 1000
+    total_timesteps: int = 10_000
+    lower_limit: float = 1e-5
+    upper_limit: float = 1e-3
+    safety: float = 0.1
+    adaptive: bool = True
+    omega_seed: int = 0            # first candidate; rejection sampling moves up
+    misfit_seed: int = 1
+    ic_seed: int = 2
+    shape: tuple | None = None     # override mw*ppw cells per axis (batched solves)
+    n_k: int = 10_000
+
+
+@dataclass
+class Problem:
+    cfg: SolveConfig
+    table: SyntheticTable
+    grid: np.ndarray
+    node_coord: np.ndarray
+    tree: object
+    calphad_values: np.ndarray
+    X0: np.ndarray
+    kappa: np.ndarray            # (4,) = kappa_i * kappa_value
+    misfit: np.ndarray           # Vegard coefficients η
+    molar_volume: float
+    Lambda: np.ndarray | None    # linear elastic coupling matrix (× V_m)
+    lvec: np.ndarray | None      # rank-1 factor of Lambda
+    bk: np.ndarray | None        # B(k) on the rfft half-grid
+    ctld: float
+    wavenumber_max: float
+    dx: float
+    shape: tuple
+    t_cfl: float
+    dt0: float                   # initial Δt
+    hessian_max: float
+    mobility_max: float
+    X_init: np.ndarray           # (*shape, 4) float64
+    omega_seed: int = 0
+    rejected_seeds: list = field(default_factory=list)
+
+    @property
+    def dim(self):
+        return len(self.shape)
+
+    @property
+    def n_points(self):
+        return int(np.prod(self.shape))
+
+
+def _misfit(seed):
+    return np.random.default_rng(seed).uniform(-0.02, 0.02, size=4)
+
+
+def _setup_for_table(cfg, table):
+    X0 = np.asarray(cfg.initial_composition, dtype=float)
+    df = table.data
+    _, grid = build_4d_grid(df, cfg.resolution)
+    tree, values = build_calphad_kdtree(df)
+
+    def ev(pts):
+        return host_table_eval(pts, grid, cfg.resolution, tree, values)
+
+    ref = ev(X0[None, :])[0]
+    hessian_max = float(np.abs(ref[:4]).max())
+    mobility_max = float(ref[4:].max())
+    misfit = _misfit(cfg.misfit_seed)
+    vm = float(els.calculate_molar_volume(X0, MOLAR_VOLUMES_FEMNNICOCU))
+    lam = el_mat = None
+    if cfg.include_cubic_anisotropy:
+        lam = els.coupling_matrix(misfit) * vm
+        el_mat = els.get_elastic_matrix(misfit, vm, cfg.c11, cfg.c12, cfg.c44, cfg.direction)
+    ctld, kmax = sysm.compute_initial_kinetics(
+        X0, cfg.resolution, cfg.kappa_value, np.asarray(cfg.kappa_i, dtype=float).reshape(1, 4),
+        ev, elastic_matrix=el_mat, n_k=cfg.n_k)
+    return dict(X0=X0, grid=grid, tree=tree, values=values, hessian_max=hessian_max,
+                mobility_max=mobility_max, misfit=misfit, vm=vm, lam=lam, ctld=ctld, kmax=kmax)
+
+
+def find_unstable_table(cfg, max_tries=200):
+    """First Ω seed ≥ cfg.omega_seed whose table puts X0 inside the spinodal."""
+    rejected = []
+    for seed in range(cfg.omega_seed, cfg.omega_seed + max_tries):
+        table = make_table(cfg.resolution, cfg.temperature, seed)
+        try:
+            setup = _setup_for_table(cfg, table)
+        except ValueError:
+            rejected.append(seed)
+            continue
+        if not np.isfinite(setup["ctld"]):
+            rejected.append(seed)
+            continue
+        return table, setup, rejected
+    raise RuntimeError(f"no unstable Ω seed in [{cfg.omega_seed}, {cfg.omega_seed + max_tries})")
+
+
+def build_problem(cfg: SolveConfig, table: SyntheticTable | None = None) -> Problem:
+    """Host setup of one solve, in the order of examples/simulate.py:59-192."""
+    rejected = []
+    if table is None:
+        table, setup, rejected = find_unstable_table(cfg)
+    else:
+        setup = _setup_for_table(cfg, table)
+    X0 = setup["X0"]
+    ctld, kmax = setup["ctld"], setup["kmax"]
+    dim = cfg.system_dim
+    _, dx, _, ncells = sysm.get_system_dimensions(kmax, ppw=cfg.ppw, mw=cfg.mw, dim=dim)
+    shape = tuple(cfg.shape) if cfg.shape is not None else tuple(ncells)
+    if len(shape) != dim:
+        raise ValueError(f"shape {shape} does not match system_dim={dim}")
+    t_cfl = sysm.cahn_hilliard_cfl_dt(dx, setup["mobility_max"], setup["hessian_max"],
+                                      cfg.kappa_value, cfg.safety)
+    dt_nominal = sysm.get_time_increment(ctld, cfg.steps_per_ctld)
+    if cfg.adaptive:
+        dt0 = dt_nominal
+    else:
+        # Fixed Δt: the nominal CTLD/steps_per_ctld value capped the way the
+        # reference loop caps every Δt (0.005·ctld and the CFL bound).
+        dt0 = min(dt_nominal, 0.005 * ctld, t_cfl)
+    lvec = bk = None
+    if cfg.include_cubic_anisotropy:
+        k_grid, k_norm = sysm.build_fourier_grid_for(dim, shape, dx, cfg.direction)
+        bk = els.build_khachaturyan_kernel(k_grid, k_norm, cfg.c11, cfg.c12, cfg.c44)
+        lvec = els.rank1_factor(setup["lam"])
+    np.random.seed(cfg.ic_seed)
+    X_init = sysm.apply_fluctuations(X0, shape, cfg.fluctuation).astype(np.float64)
+    kappa = (np.asarray(cfg.kappa_i, dtype=float).reshape(-1) * cfg.kappa_value)
+    node_coord = node_coordinates(setup["tree"], cfg.resolution)
+    return Problem(cfg=cfg, table=table, grid=setup["grid"], node_coord=node_coord,
+                   tree=setup["tree"], calphad_values=setup["values"], X0=X0, kappa=kappa,
+                   misfit=setup["misfit"], molar_volume=setup["vm"], Lambda=setup["lam"],
+                   lvec=lvec, bk=bk, ctld=float(ctld), wavenumber_max=float(kmax), dx=float(dx),
+                   shape=shape, t_cfl=float(t_cfl), dt0=float(dt0),
+                   hessian_max=setup["hessian_max"], mobility_max=setup["mobility_max"],
+                   X_init=np.ascontiguousarray(X_init), omega_seed=table.seed,
+                   rejected_seeds=rejected)
+
+
+# ---------------------------------------------------------------------------
+# Named workloads
+# ---------------------------------------------------------------------------
+
+def config_1d_fixed():
+    """Plain FP64 1D: N=1280 (mw=80, ppw=16), X0=(0.1,0.2,0.2,0.3), κ=5e-16,
+    41^4 table at 873 K, elasticity on, fixed Δt, 10,000 steps."""
+    return SolveConfig(system_dim=1, initial_composition=(0.1, 0.2, 0.2, 0.3), mw=80, ppw=16,
+                       kappa_value=5e-16, resolution=0.025, adaptive=False,
+                       total_timesteps=10_000, steps_per_ctld=1000)
+
+
+def config_2d_adaptive():
+    """Plain FP64 2D: 512×512 (mw=32, ppw=16), X0=(0.1,0.2,0.3,0.2), κ=7.6e-15,
+    41^4 table at 873 K, elasticity on, adaptive Δt, 20,000 steps."""
+    return SolveConfig(system_dim=2, initial_composition=(0.1, 0.2, 0.3, 0.2), mw=32, ppw=16,
+                       kappa_value=7.6e-15, resolution=0.025, adaptive=True,
+                       total_timesteps=20_000, steps_per_ctld=1000)
+
+
+def config_3d_precision():
+    """Precision form: 3D 256³ (mw=16, ppw=16), 51^4 table, elasticity on,
+    5,000 adaptive steps; X0 and κ as the 2D case."""
+    return SolveConfig(system_dim=3, initial_composition=(0.1, 0.2, 0.3, 0.2), mw=16, ppw=16,
+                       kappa_value=7.6e-15, resolution=0.02, adaptive=True,
+                       total_timesteps=5_000, steps_per_ctld=1000)
