@@ -1,0 +1,342 @@
+#!/usr/bin/env python
+"""Benchmark the Cahn-Hilliard step loop on B200.
+
+Default workload (N=1): plain FP64 2D 512x512, the 41^4 synthetic table at
+873 K, elasticity on, adaptive dt -- one "step" is one explicit time step of
+the whole field.  The composition field, rates and FFT buffers of this
+workload fit in L2, so L2 is flushed (a 256 MiB write) between timed steps
+and each step is timed alone with CUDA events on the launching stream.
+
+Prints one JSON line.  ``--impl reference`` times the reference algorithm's
+CPU implementation (the oracle restatement of the Numba kernels + scipy FFT,
+all host threads) on the same workload and prints the same line with
+"impl": "reference".  Under torchrun every rank runs an independent replica
+(the path has no cross-solve exchange); value = all ranks' grid-point steps
+/ the slowest rank's time.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+if HERE not in sys.path:
+    sys.path.insert(0, HERE)
+
+# Algorithmic HBM bytes per grid-point step (FP64, elasticity on): state X
+# read+written once (64), dX/dt written+read once (64), the misfit scalar's
+# trip through the FFT pair (6 x 8).
+STEP_BYTES_FP64 = 176
+# Fused rate kernel per grid point: read X (32) and s' (8), write dX/dt (32).
+RATE_BYTES_FP64 = 72
+FALLBACK_HBM_GBS = 6650.0
+L2_FLUSH_BYTES = 256 << 20
+
+WORKLOADS = {
+    "2d": ("plain FP64 2D 512x512, 41^4 table, elastic, adaptive dt", "config_2d_adaptive"),
+    "1d": ("plain FP64 1D 1280, 41^4 table, elastic, fixed dt", "config_1d_fixed"),
+    "3d": ("plain FP64 3D 256^3, 51^4 table, elastic, adaptive dt", "config_3d_precision"),
+}
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=30)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--workload", choices=sorted(WORKLOADS), default="2d")
+    ap.add_argument("--cpu-steps", type=int, default=3, help="steps in the CPU-baseline sample")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    return ap.parse_args()
+
+
+def build_problem(name):
+    from phasefield5d_b200 import workload as W
+    return W.build_problem(getattr(W, WORKLOADS[name][1])())
+
+
+def measured_peak():
+    path = os.path.join(HERE, "MEASURED_PEAKS.json")
+    try:
+        with open(path) as f:
+            return float(json.load(f)["hbm_gbs"]), "measured"
+    except Exception:
+        return FALLBACK_HBM_GBS, "fallback"
+
+
+def committed_traffic(kernel, workload):
+    """dram bytes per launch of ``kernel`` from the committed ncu summary."""
+    try:
+        with open(os.path.join(HERE, "profiles", "traffic.json")) as f:
+            ent = json.load(f)[kernel][workload]
+        return float(ent["dram_bytes_per_launch"])
+    except Exception:
+        return None
+
+
+class ClockSampler:
+    """nvidia-smi clock/throttle samples every 200 ms while running."""
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.f = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+        try:
+            self.p = subprocess.Popen(["nvidia-smi", f"--id={index}", f"--query-gpu={self.Q}",
+                                       "--format=csv,noheader,nounits", "-lms", "200"],
+                                      stdout=self.f, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.p = None
+
+    def stop(self):
+        if self.p is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.p.terminate()
+        try:
+            self.p.wait(timeout=5)
+        except Exception:
+            self.p.kill()
+        self.f.flush()
+        rows = []
+        with open(self.f.name) as f:
+            for line in f:
+                parts = [p.strip() for p in line.split(",")]
+                if len(parts) >= 9:
+                    rows.append(parts)
+        os.unlink(self.f.name)
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no samples"]}
+        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in rows for i in range(4) if r[5 + i] == "Active"})
+        return {"sm_mhz": statistics.median(sm) if sm else None,
+                "sm_max_mhz": max(mx) if mx else None, "reasons": reasons,
+                "samples": len(rows)}
+
+
+def cpu_threads():
+    from oracle import oracle as O
+    return O.num_threads()
+
+
+def time_oracle(prob, steps, warmup):
+    """Reference algorithm on the host cores: (grid-point steps/s, seconds)."""
+    from oracle.oracle import OracleStepper
+    st = OracleStepper.from_problem(prob, fft_workers=-1)
+    for _ in range(warmup):
+        st.step()
+    t0 = time.perf_counter()
+    for _ in range(steps):
+        st.step()
+    dt = time.perf_counter() - t0
+    return prob.n_points * steps / dt, dt
+
+
+def run_reference(args, rank):
+    if rank != 0:
+        return
+    prob = build_problem(args.workload)
+    value, secs = time_oracle(prob, args.steps, args.warmup)
+    sample = f"{args.steps} steps of the full {WORKLOADS[args.workload][0]} after {args.warmup} warm-up"
+    line = {
+        "impl": "reference", "metric": "grid-point steps/s", "value": value,
+        "unit": "grid-point steps/s", "n_gpus": args.gpus, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": 1e3 * secs / args.steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": WORKLOADS[args.workload][0], "shape": list(prob.shape),
+                   "parallelism": "cpu-threads"},
+        "cpu_baseline": {"value": value, "unit": "grid-point steps/s", "cores": cpu_threads(),
+                         "kind": "port", "sample": sample},
+        "e2e": {"value": value, "unit": "grid-point steps/s", "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def run_ours(args, rank, world, local_rank):
+    import torch
+    import torch.distributed as dist
+    from phasefield5d_b200 import _lib
+    from phasefield5d_b200.stepper import Stepper
+
+    torch.cuda.set_device(local_rank)
+    dev = torch.device("cuda", local_rank)
+    prob = build_problem(args.workload)
+    P = prob.n_points
+    stream = torch.cuda.current_stream()
+    flush = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.float32, device=dev)
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    # ---- device-resident steps, L2 flushed between timed steps -------------
+    st = Stepper.from_problem(prob)
+    st.advance(1)                       # captures the one-step graph
+    for _ in range(args.warmup):
+        flush.zero_()
+        st.advance(1)
+    barrier()
+    clocks = ClockSampler(local_rank)
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+          for _ in range(args.steps)]
+    for e0, e1 in ev:
+        flush.zero_()
+        e0.record(stream)
+        st.advance(1)
+        e1.record(stream)
+    barrier()
+    clock_info = clocks.stop()
+    step_ms = [e0.elapsed_time(e1) for e0, e1 in ev]
+    total_ms = sum(step_ms)
+    state = st.state()
+    if state["halted"]:
+        raise RuntimeError(f"stepper halted during the benchmark: {state}")
+
+    # ---- back-to-back steps from the 50-step graph (L2-warm, informational)
+    st.advance(50)
+    torch.cuda.synchronize()
+    w0, w1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    w0.record(stream)
+    st.advance(200)
+    w1.record(stream)
+    torch.cuda.synchronize()
+    resident_ms = w0.elapsed_time(w1) / 200
+
+    # ---- dominant kernel (fused rate) alone, L2 flushed, same stream -------
+    probe = Stepper.from_problem(prob)
+    stage_ms = {}
+    stages = [("rate", _lib.STAGE_RATE), ("update", _lib.STAGE_UPDATE)]
+    if prob.lvec is not None:
+        stages += [("fft_fwd", _lib.STAGE_FFT_FWD), ("bmul", _lib.STAGE_BMUL),
+                   ("fft_inv", _lib.STAGE_FFT_INV)]
+    for name, sid in stages:
+        for _ in range(3):
+            probe.launch_stage(sid)
+        times = []
+        for _ in range(max(args.steps, 10)):
+            flush.zero_()
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record(stream)
+            probe.launch_stage(sid)
+            b.record(stream)
+            times.append((a, b))
+        torch.cuda.synchronize()
+        stage_ms[name] = sum(x.elapsed_time(y) for x, y in times) / len(times)
+    probe.close()
+
+    # ---- end to end through the C ABI with host buffers --------------------
+    host = torch.from_numpy(prob.X_init.copy()).pin_memory()
+    e2e_st = Stepper.from_problem(prob)
+    xdev = e2e_st.X
+    for _ in range(max(args.warmup, 1)):
+        xdev.copy_(host, non_blocking=True)
+        e2e_st.advance(1)
+        host.copy_(xdev, non_blocking=True)
+    torch.cuda.synchronize()
+    e2e_ev = []
+    for _ in range(args.steps):
+        flush.zero_()
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        xdev.copy_(host, non_blocking=True)
+        e2e_st.advance(1)
+        host.copy_(xdev, non_blocking=True)
+        b.record(stream)
+        e2e_ev.append((a, b))
+    torch.cuda.synchronize()
+    e2e_ms = sum(a.elapsed_time(b) for a, b in e2e_ev)
+    e2e_st.close()
+
+    # ---- max over ranks -----------------------------------------------------
+    t = torch.tensor([total_ms, e2e_ms, resident_ms], dtype=torch.float64, device=dev)
+    if world > 1:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    total_ms, e2e_ms, resident_ms = (float(v) for v in t.tolist())
+    if rank != 0:
+        return
+
+    value = world * P * args.steps / (total_ms * 1e-3)
+    peak, peak_kind = measured_peak()
+    rate_bytes = RATE_BYTES_FP64 * P if prob.lvec is not None else (RATE_BYTES_FP64 - 8) * P
+    achieved = rate_bytes / (stage_ms["rate"] * 1e-3) / 1e9
+    cpu = None
+    if not args.no_cpu_baseline:
+        cpu_val, _ = time_oracle(prob, args.cpu_steps, 1)
+        cpu = {"value": cpu_val, "unit": "grid-point steps/s", "cores": cpu_threads(),
+               "kind": "port",
+               "sample": f"{args.cpu_steps} steps of the full {WORKLOADS[args.workload][0]} "
+                         f"after 1 warm-up (oracle C restatement + scipy FFT)"}
+    line = {
+        "metric": "grid-point steps/s", "value": value, "unit": "grid-point steps/s",
+        "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": total_ms / args.steps, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": WORKLOADS[args.workload][0], "shape": list(prob.shape),
+                   "table_nodes_per_axis": int(prob.grid.shape[0]), "omega_seed": prob.omega_seed,
+                   "l2": "flushed (256 MiB write) between timed steps",
+                   "parallelism": f"replicas x{world}" if world > 1 else "single solve"},
+        "roofline": {"bound": "hbm", "kernel": "k_rate_march (fused chemical potential + flux "
+                                               "divergence)" if prob.dim > 1 else "k_rate_1d",
+                     "achieved": achieved, "peak": peak, "peak_kind": peak_kind, "unit": "GB/s",
+                     "frac": achieved / peak, "traffic": committed_traffic("rate", args.workload),
+                     "algorithmic_bytes_per_launch": rate_bytes,
+                     "ms_per_launch": stage_ms["rate"]},
+        "step_roofline": {"bytes_per_grid_point_step": STEP_BYTES_FP64,
+                          "achieved_gbs": STEP_BYTES_FP64 * value / world / 1e9,
+                          "frac": STEP_BYTES_FP64 * value / world / 1e9 / peak},
+        "stage_ms": stage_ms,
+        "resident_l2_warm": {"value": world * P / (resident_ms * 1e-3),
+                             "ms_per_step": resident_ms,
+                             "note": "200 back-to-back steps from 50-step graphs, no flush"},
+        "cpu_baseline": cpu,
+        "e2e": {"value": world * P * args.steps / (e2e_ms * 1e-3), "unit": "grid-point steps/s",
+                "h2d_bytes_per_step": int(host.numel() * 8),
+                "d2h_bytes_per_step": int(host.numel() * 8),
+                "path": "pinned host X -> H2D -> pf5d_stepper_advance(1) -> D2H, per step"},
+        "clocks": clock_info,
+        "gpu_launches": args.steps * (3 if prob.lvec is not None else 2),
+        "state_after": {"step": state["step"], "dt": state["dt"], "time": state["time"]},
+    }
+    print(json.dumps(line), flush=True)
+    st.close()
+
+
+def main():
+    args = parse()
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        run_reference(args, rank)
+        return
+    import torch
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        torch.cuda.set_device(local_rank)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+    try:
+        run_ours(args, rank, world, local_rank)
+    finally:
+        if world > 1:
+            import torch.distributed as dist
+            dist.barrier()
+            dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,206 @@
+/*
+ * pf5d.h -- C ABI of the B200 (sm_100a) Cahn-Hilliard step library.
+ *
+ * One shared library, libpf5d.so, built from phasefield5d_b200/csrc.  All
+ * entry points take plain pointers and sizes; device pointers are CUDA
+ * global-memory addresses on the current device, and `stream` is a
+ * cudaStream_t passed as void* (NULL = legacy default stream).  Arrays use
+ * the reference layout: C-contiguous (*spatial, S) float64 with S = 4
+ * independent components; "views" (mu = interp[..., :4], M = interp[..., 4:])
+ * are a pointer plus a point stride in elements.
+ *
+ * Every function returns a pf5d_status (0 = success).  Launch-only entry
+ * points do not synchronise; errors found on the device are reported through
+ * the device status word documented at PF5D_FLAG_*.  pf5d_last_error() gives
+ * a text for the last non-zero return on the calling thread.
+ *
+ * Reference interfaces are cited as path:line within phasefield5d.
+ */
+#ifndef PF5D_H
+#define PF5D_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Every declaration below is an exported symbol of libpf5d.so (the library
+ * is built with hidden visibility by default). */
+#if defined(__GNUC__)
+#pragma GCC visibility push(default)
+#endif
+
+/* ---------------------------------------------------------------- status */
+typedef enum {
+  PF5D_OK = 0,
+  PF5D_ERR_ARG = 1,          /* bad pointer/size/stride (reference: ValueError)        */
+  PF5D_ERR_DIM = 2,          /* unsupported spatial dimension (ValueError /
+                                NotImplementedError in the reference)                   */
+  PF5D_ERR_CUDA = 3,         /* a CUDA runtime call failed                             */
+  PF5D_ERR_CUFFT = 4,        /* a cuFFT call failed                                    */
+  PF5D_ERR_NN_DISTANCE = 5,  /* nearest table row farther than max_nn_dist
+                                (reference: RuntimeError, interpolation.py:207-208)   */
+  PF5D_ERR_OOB = 6,          /* hard out-of-bounds composition (system.py:12-53)       */
+  PF5D_ERR_CAPACITY = 7      /* request exceeds a fixed capacity of the library        */
+} pf5d_status;
+
+/* Device status word bits (OR-ed by kernels). */
+#define PF5D_FLAG_NONFINITE    0x01u  /* NaN/inf in the composition field           */
+#define PF5D_FLAG_OOB_HARD     0x02u  /* |violation| > tol_hard (1e-3)              */
+#define PF5D_FLAG_OOB_SOFT     0x04u  /* |violation| > tol_soft (1e-5)              */
+#define PF5D_FLAG_NN_FAR       0x08u  /* nearest-row distance > max_nn_dist         */
+#define PF5D_FLAG_NN_TRUNCATED 0x10u  /* nearest-row search window may have missed */
+#define PF5D_FLAG_NN_USED      0x20u  /* some point took the nearest-row fallback   */
+#define PF5D_FLAG_HALTED       0x40u  /* step loop stopped at an OOB check          */
+
+const char *pf5d_last_error(void);
+int32_t pf5d_version(void);
+
+/* ------------------------------------------------------- interpolation ----
+ * interpolator_nb (phasefield5d/solver/interpolation.py:154-211):
+ * quadrilinear interpolation of a dense (n,n,n,n,node_stride) table with the
+ * nearest-table-row fallback for points with sum(x) > 1 - 4*res - 1e-9.
+ * comp: device (npts,4); grid: device dense table, props at [0, nprops) of
+ * each node's node_stride values, NaN at nodes absent from the table;
+ * node_coord: device (n,) stored coordinate of node k on every axis;
+ * out: device, row r at out + r*out_stride; mask: device (npts,) bytes or
+ * NULL; flags: device uint32 OR-ed with PF5D_FLAG_NN_* or NULL.
+ * max_nn_dist <= 0 disables the distance check. */
+pf5d_status pf5d_interp4d(const double *comp, int64_t npts, const double *grid, int32_t n,
+                          int32_t nprops, int32_t node_stride, double resolution,
+                          const double *node_coord, double max_nn_dist, double *out,
+                          int64_t out_stride, uint8_t *mask, uint32_t *flags, void *stream);
+
+/* ----------------------------------------------------------- stencils -----
+ * calculate_laplacian (phasefield5d/solver/operators.py:10-76): periodic
+ * second-order Laplacian of a contiguous (*shape, ncomp) field. */
+pf5d_status pf5d_laplacian(int32_t dim, const int64_t *shape, int32_t ncomp, const double *c,
+                           double dx, double *out, void *stream);
+
+/* lap *= kappa; mu -= lap  (examples/simulate.py:254-255).  kappa: host (ncomp,). */
+pf5d_status pf5d_kappa_subtract(double *mu, int64_t mu_stride, double *lap, const double *kappa,
+                                int64_t npts, int32_t ncomp, void *stream);
+
+/* get_divergence_from_mu_function(dim)(X, M, mu, inv_dx, out)
+ * (phasefield5d/solver/fluxes.py:296-416, face flux 128-160). */
+pf5d_status pf5d_divergence_from_mu(int32_t dim, const int64_t *shape, int32_t ncomp,
+                                    const double *X, const double *M, int64_t m_stride,
+                                    const double *mu, int64_t mu_stride, double inv_dx,
+                                    double *out, void *stream);
+
+/* calculate_gradients_pm (phasefield5d/solver/operators.py:79-123, 126-158,
+ * 289-317): gp, gm device (dim, *shape, ncomp). */
+pf5d_status pf5d_gradients_pm(int32_t dim, const int64_t *shape, int32_t ncomp, const double *c,
+                              int64_t c_stride, double dx, double *gp, double *gm, void *stream);
+
+/* get_flux_function(dim)(X, M, gp, gm, fp, fm)
+ * (phasefield5d/solver/fluxes.py:6-125). */
+pf5d_status pf5d_fluxes_pm(int32_t dim, const int64_t *shape, int32_t ncomp, const double *X,
+                           const double *M, int64_t m_stride, const double *gp, const double *gm,
+                           double *fp, double *fm, void *stream);
+
+/* ------------------------------------------------------------ elastic -----
+ * make_elastic_updater (phasefield5d/solver/elastic.py:147-286), rank-1 path:
+ * s = (X - X0).l ; S = rfftn(s) * B(k) ; s' = irfftn(S) ; mu += s' l.
+ * bk: host real B(k) on the rfft half-grid (copied at create).  One cuFFT
+ * D2Z/Z2D plan pair per handle. */
+typedef struct pf5d_elastic pf5d_elastic;
+pf5d_status pf5d_elastic_create(int32_t dim, const int64_t *shape, const double *x0,
+                                const double *lvec, const double *bk, pf5d_elastic **out);
+pf5d_status pf5d_elastic_apply(pf5d_elastic *h, double *mu, int64_t mu_stride, const double *X,
+                               void *stream);
+pf5d_status pf5d_elastic_destroy(pf5d_elastic *h);
+
+/* --------------------------------------------------------- reductions -----
+ * abs_max (phasefield5d/solver/operators.py:161-175): max |a[i]| starting
+ * from 0.0, NaN ignored.  result: device double.  Uses a per-device block
+ * partials workspace allocated on first use. */
+pf5d_status pf5d_abs_max(const double *a, int64_t n, double *result, void *stream);
+
+/* clamp_simplex (phasefield5d/solver/operators.py:262-317), in place. */
+pf5d_status pf5d_clamp_simplex(double *X, int64_t npts, int32_t ncomp, void *stream);
+
+/* dXdt *= dt; X += dXdt  (examples/simulate.py:316-317). */
+pf5d_status pf5d_update(double *X, double *dXdt, int64_t n, double dt, void *stream);
+
+/* out_of_bounds statistics (phasefield5d/solver/system.py:12-53).  Fills
+ * host stats[5] = {n_nonfinite, max row sum, min row sum, max comp, min comp}
+ * (synchronises `stream`). */
+pf5d_status pf5d_oob_stats(const double *X, int64_t npts, int32_t ncomp, double *stats,
+                           void *stream);
+
+/* apply_adaptive_time (phasefield5d/solver/system.py:90-112) on the host;
+ * the step loop evaluates the same rule on the device. */
+double pf5d_adaptive_dt(double dt_current, double xdotmax, double ctld, double t_cfl,
+                        double lower_limit, double upper_limit, double max_change_factor);
+
+/* ---------------------------------------------------------- step loop -----
+ * The main loop body of examples/simulate.py:230-320 (saves off) as a
+ * device-resident stepper: interpolation, Laplacian, elastic term, fused
+ * flux divergence, max|dX/dt|, adaptive dt, update and clamp, with dt and
+ * time kept on the device and steps replayed from CUDA graphs.  The
+ * out_of_bounds check runs every oob_interval steps before the step, as in
+ * simulate.py:231; a hard violation halts the stepper (PF5D_FLAG_HALTED). */
+typedef struct {
+  int32_t dim;                 /* 1, 2 or 3                                   */
+  int64_t shape[3];            /* cells per axis (unused trailing = 1)        */
+  double dx;                   /* cell size [m]                               */
+  double kappa[4];             /* kappa_i * kappa_value per component         */
+  double x0[4];                /* reference composition                        */
+  int32_t elastic;             /* 1: rank-1 Khachaturyan term on             */
+  double lvec[4];              /* rank-1 factor l (Lambda = l l^T)            */
+  const double *bk;            /* host B(k) on the rfft half-grid, or NULL    */
+  const double *grid;          /* device dense table (caller owns)            */
+  int32_t table_n;             /* nodes per axis                              */
+  int32_t nprops;              /* 9                                           */
+  int32_t node_stride;         /* doubles per node (>= nprops)               */
+  double resolution;           /* table spacing                               */
+  const double *node_coord;    /* device (table_n,)                           */
+  double max_nn_dist;          /* <= 0: unchecked                             */
+  double ctld, t_cfl;          /* CTLD [s] and CFL bound [s]                  */
+  double lower_limit, upper_limit, max_change_factor;
+  int32_t adaptive;            /* 0: fixed dt = dt0                           */
+  double dt0;                  /* initial dt                                  */
+  int32_t oob_interval;        /* 100 in the reference                        */
+} pf5d_stepper_desc;
+
+typedef struct {
+  double dt, time, xdotmax;
+  int64_t step;
+  uint32_t flags;
+  uint32_t halted;
+} pf5d_step_state;
+
+typedef struct pf5d_stepper pf5d_stepper;
+
+/* X: device (*shape, 4) float64, caller-owned, advanced in place. */
+pf5d_status pf5d_stepper_create(const pf5d_stepper_desc *desc, double *X, void *stream,
+                                pf5d_stepper **out);
+/* Enqueue n steps on `stream` (no host synchronisation). */
+pf5d_status pf5d_stepper_advance(pf5d_stepper *h, int64_t nsteps, void *stream);
+/* Synchronise `stream` and copy the device step state to *out. */
+pf5d_status pf5d_stepper_state(pf5d_stepper *h, pf5d_step_state *out, void *stream);
+/* Device pointer to the last dX/dt buffer ((*shape, 4) float64). */
+double *pf5d_stepper_rate(pf5d_stepper *h);
+/* Diagnostics: launch one stage of a step by itself on `stream`
+ * (PF5D_STAGE_*), so each kernel can be timed with events.  It changes the
+ * stepper's state exactly as that stage does inside a step. */
+#define PF5D_STAGE_RATE 0        /* fused chemical potential + flux divergence */
+#define PF5D_STAGE_UPDATE 1      /* update, clamp, next misfit, OOB test       */
+#define PF5D_STAGE_FFT_FWD 2     /* cuFFT D2Z of the misfit                    */
+#define PF5D_STAGE_BMUL 3        /* B(k) multiply                              */
+#define PF5D_STAGE_FFT_INV 4     /* cuFFT Z2D                                  */
+pf5d_status pf5d_stepper_launch_stage(pf5d_stepper *h, int32_t stage, void *stream);
+/* Re-derive internal state after the caller modified X (e.g. a restart). */
+pf5d_status pf5d_stepper_reset(pf5d_stepper *h, double dt, double time, void *stream);
+pf5d_status pf5d_stepper_destroy(pf5d_stepper *h);
+
+#if defined(__GNUC__)
+#pragma GCC visibility pop
+#endif
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* PF5D_H */

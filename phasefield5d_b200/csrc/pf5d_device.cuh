@@ -1,0 +1,251 @@
+// pf5d_device.cuh -- FP64 device building blocks shared by every kernel.
+//
+// Bit-faithfulness: each routine evaluates the reference's expressions in the
+// reference's order, one IEEE rounding per operation.  Translation units that
+// include this header are compiled with -fmad=false so nvcc never contracts a
+// multiply and an add into an FMA (the reference's Numba kernels run with
+// fastmath=False, which never contracts either).  Division and square root
+// use the IEEE-rounded defaults (-prec-div=true, -prec-sqrt=true).
+#pragma once
+
+#include <cstdint>
+#include <cuda_runtime.h>
+
+#include "../../include/pf5d.h"
+
+namespace pf5d {
+
+constexpr int S = 4;    // independent components
+constexpr int NM = 5;   // mobilities (Fe first)
+constexpr int NP = 9;   // table props: mu1..mu4, M_Fe, M1..M4
+
+// Periodic neighbour indices (phasefield5d/solver/operators.py:45-46 pattern).
+__device__ __forceinline__ int64_t wrap_p(int64_t i, int64_t n) { return i + 1 < n ? i + 1 : 0; }
+__device__ __forceinline__ int64_t wrap_m(int64_t i, int64_t n) { return i - 1 >= 0 ? i - 1 : n - 1; }
+// General periodic index for halo loads (any offset, any n >= 1).
+__device__ __forceinline__ int wrap_any(int i, int n) {
+  int r = i % n;
+  return r < 0 ? r + n : r;
+}
+
+// Table view passed by value to kernels.
+struct Table {
+  const double *grid;       // dense (n,n,n,n,stride)
+  const double *coord;      // (n,) stored node coordinate per index
+  int n;                    // nodes per axis
+  int stride;               // doubles per node
+  double inv_step;          // 1.0 / resolution
+  double threshold;         // 1.0 - 4.0*resolution - 1e-9
+  double exact_d2;          // (1.99*resolution)^2: window search is exact below this
+  double max_nn_dist;       // <= 0: unchecked
+};
+
+// interpolation.py:110-121
+__device__ __forceinline__ void axis_coord(double u, int num, int &i, double &t) {
+  if (u <= 0.0) {
+    i = 0;
+    t = 0.0;
+  } else if (u >= (double)(num - 1)) {
+    i = num - 2;
+    t = 1.0;
+  } else {
+    i = (int)u;
+    t = u - (double)i;
+  }
+}
+
+// sum_d x[d] from 0.0, left to right (interpolation.py:74-79).
+__device__ __forceinline__ bool linear_region(const Table &T, const double x[S]) {
+  double s = 0.0;
+  s = s + x[0];
+  s = s + x[1];
+  s = s + x[2];
+  s = s + x[3];
+  return s <= T.threshold;
+}
+
+// Quadrilinear interpolation of NP props at x (interpolation.py:103-147).
+// Corner order c = b0 b1 b2 b3 (binary), weights ((w0*w1)*w2)*w3, per-prop
+// sum of the 16 terms left to right.  Corners are visited outermost so each
+// corner's NP props are one contiguous run of the node.
+__device__ __forceinline__ void interp_linear(const Table &T, const double x[S], double out[NP]) {
+  int i0, i1, i2, i3;
+  double t0, t1, t2, t3;
+  axis_coord(x[0] * T.inv_step, T.n, i0, t0);
+  axis_coord(x[1] * T.inv_step, T.n, i1, t1);
+  axis_coord(x[2] * T.inv_step, T.n, i2, t2);
+  axis_coord(x[3] * T.inv_step, T.n, i3, t3);
+  const double q0 = 1.0 - t0, q1 = 1.0 - t1, q2 = 1.0 - t2, q3 = 1.0 - t3;
+  const int64_t s3 = T.stride, s2 = (int64_t)T.n * s3, s1 = (int64_t)T.n * s2,
+                s0 = (int64_t)T.n * s1;
+  const double *base = T.grid + i0 * s0 + i1 * s1 + i2 * s2 + i3 * s3;
+#pragma unroll
+  for (int c = 0; c < 16; ++c) {
+    const int b0 = (c >> 3) & 1, b1 = (c >> 2) & 1, b2 = (c >> 1) & 1, b3 = c & 1;
+    const double w = (b0 ? t0 : q0) * (b1 ? t1 : q1) * (b2 ? t2 : q2) * (b3 ? t3 : q3);
+    const double *node = base + b0 * s0 + b1 * s1 + b2 * s2 + b3 * s3;
+#pragma unroll
+    for (int p = 0; p < NP; ++p) {
+      const double term = w * __ldg(node + p);
+      out[p] = (c == 0) ? term : out[p] + term;
+    }
+  }
+}
+
+// Nearest table row for a point outside the linear region
+// (interpolation.py:203-209, cKDTree over the row compositions).
+//
+// Rows sit on grid nodes, so the nearest row is the nearest present node.
+// Every node within two cells of x along each axis is inside the
+// [floor(u)-2, floor(u)+2]^4 window searched here; when the best distance is
+// below 1.99 cells the answer is therefore the exact nearest node (as long
+// as floor(u) itself is a present node, true for sum(x) < 1 + res on a full
+// simplex table).  Farther results set PF5D_FLAG_NN_TRUNCATED.  Distances
+// are accumulated as sum_d (x_d - c_d)^2 in axis order; on an exact tie the
+// first node in lexicographic order wins.
+static __device__ __noinline__ void interp_nearest(const Table T, const double *x, double *out,
+                                            unsigned *flag_bits) {
+  const int N = T.n - 1;
+  int lo[S], hi[S];
+#pragma unroll
+  for (int d = 0; d < S; ++d) {
+    double u = x[d] * T.inv_step;
+    if (!(u > -4.0)) u = -4.0;             // also maps NaN
+    if (!(u < (double)N + 4.0)) u = (double)N + 4.0;
+    const int f = (int)floor(u);
+    lo[d] = max(0, f - 2);
+    hi[d] = min(N, f + 2);
+  }
+  double best = __longlong_as_double(0x7ff0000000000000LL);   // +inf
+  int64_t best_node = -1;
+  const int64_t n = T.n;
+  for (int k0 = lo[0]; k0 <= hi[0]; ++k0) {
+    const double d0 = x[0] - T.coord[k0];
+    const double e0 = d0 * d0;
+    for (int k1 = lo[1]; k1 <= hi[1]; ++k1) {
+      const double d1 = x[1] - T.coord[k1];
+      const double e1 = e0 + d1 * d1;
+      for (int k2 = lo[2]; k2 <= hi[2]; ++k2) {
+        const double d2 = x[2] - T.coord[k2];
+        const double e2 = e1 + d2 * d2;
+        for (int k3 = lo[3]; k3 <= hi[3]; ++k3) {
+          const double d3 = x[3] - T.coord[k3];
+          const double e3 = e2 + d3 * d3;
+          if (e3 < best) {
+            const int64_t node = ((k0 * n + k1) * n + k2) * n + k3;
+            const double probe = __ldg(T.grid + node * T.stride);
+            if (probe == probe) {            // present (not NaN)
+              best = e3;
+              best_node = node;
+            }
+          }
+        }
+      }
+    }
+  }
+  unsigned f = PF5D_FLAG_NN_USED;
+  if (best_node < 0) {
+    f |= PF5D_FLAG_NN_TRUNCATED;
+    for (int p = 0; p < NP; ++p) out[p] = __longlong_as_double(0x7ff8000000000000LL);
+  } else {
+    if (!(best < T.exact_d2)) f |= PF5D_FLAG_NN_TRUNCATED;
+    if (T.max_nn_dist > 0.0 && sqrt(best) > T.max_nn_dist) f |= PF5D_FLAG_NN_FAR;
+    const double *row = T.grid + best_node * T.stride;
+    for (int p = 0; p < NP; ++p) out[p] = __ldg(row + p);
+  }
+  *flag_bits |= f;
+}
+
+// Interpolation with fallback for one point; returns true on the linear branch.
+__device__ __forceinline__ bool interp_point(const Table &T, const double x[S], double out[NP],
+                                             unsigned *flag_bits) {
+  if (linear_region(T, x)) {
+    interp_linear(T, x, out);
+    return true;
+  }
+  interp_nearest(T, x, out, flag_bits);
+  return false;
+}
+
+// _face_flux (phasefield5d/solver/fluxes.py:128-160) for the face between a
+// "centre" point c and a neighbour n, with g = the mu gradient across it.
+// J_a = w_fe*(-Xm_a)*(-<Xm,g>) + Xm_a*Mm_{1+a}*(g_a - <Xm,g>) - Xm_a*sum_k(...)
+__device__ __forceinline__ void face_flux(const double Xc[S], const double Mc[NM],
+                                          const double Xn[S], const double Mn[NM],
+                                          const double g[S], double J[S]) {
+  double xm[S], mm[NM], dk[S];
+#pragma unroll
+  for (int a = 0; a < S; ++a) xm[a] = 0.5 * (Xc[a] + Xn[a]);
+#pragma unroll
+  for (int a = 0; a < NM; ++a) mm[a] = 0.5 * (Mc[a] + Mn[a]);
+  double sum_x = 0.0;
+#pragma unroll
+  for (int a = 0; a < S; ++a) sum_x = sum_x + xm[a];
+  const double w_fe = (1.0 - sum_x) * mm[0];
+  double dot_xg = 0.0;
+#pragma unroll
+  for (int b = 0; b < S; ++b) dot_xg = dot_xg + xm[b] * g[b];
+  const double dot_fe = -dot_xg;
+#pragma unroll
+  for (int k = 0; k < S; ++k) dk[k] = g[k] - dot_xg;
+  double sum_wk = 0.0;
+#pragma unroll
+  for (int k = 0; k < S; ++k) sum_wk = sum_wk + xm[k] * mm[1 + k] * dk[k];
+#pragma unroll
+  for (int a = 0; a < S; ++a) {
+    const double wa = xm[a] * mm[1 + a];
+    J[a] = w_fe * (-xm[a]) * dot_fe + wa * dk[a] - xm[a] * sum_wk;
+  }
+}
+
+// apply_adaptive_time (phasefield5d/solver/system.py:90-112); Python's min()
+// keeps its first argument unless a later one is strictly smaller, and
+// np.clip is minimum(maximum(a, lo), hi).
+__host__ __device__ inline double adaptive_dt(double dt, double xdotmax, double ctld, double t_cfl,
+                                              double lower, double upper, double factor) {
+  double dt_raw;
+  if (xdotmax <= 0.0) {
+    dt_raw = dt;
+  } else {
+    double lo = lower / xdotmax, hi = upper / xdotmax;
+    if (lo > hi) {
+      const double t = lo;
+      lo = hi;
+      hi = t;
+    }
+    double c = dt;
+    if (c < lo) c = lo;                      // maximum(dt, lo)
+    if (c > hi) c = hi;                      // minimum(., hi)
+    dt_raw = c;
+  }
+  double m = dt * factor;
+  if (dt_raw < m) m = dt_raw;
+  const double cap = 0.005 * ctld;
+  if (cap < m) m = cap;
+  if (t_cfl < m) m = t_cfl;
+  return m;
+}
+
+// atomicMax for non-negative doubles (their bit patterns order like the values).
+__device__ __forceinline__ void atomic_max_nonneg(double *addr, double v) {
+  atomicMax(reinterpret_cast<unsigned long long *>(addr),
+            static_cast<unsigned long long>(__double_as_longlong(v)));
+}
+
+// Block-wide max of non-negative values (NaN already filtered by the caller).
+template <int NT>
+__device__ __forceinline__ double block_max(double v, double *red) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_xor_sync(0xffffffffu, v, o));
+  const int lane = threadIdx.x & 31, warp = (threadIdx.y * blockDim.x + threadIdx.x) >> 5;
+  if (lane == 0) red[warp] = v;
+  __syncthreads();
+  if (warp == 0) {
+    v = (lane < NT / 32) ? red[lane] : 0.0;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_xor_sync(0xffffffffu, v, o));
+  }
+  return v;
+}
+
+}  // namespace pf5d

@@ -1,0 +1,44 @@
+// pf5d_fft.h -- the rank-1 elastic operator's cuFFT plan pair and the
+// hand-written kernels around it (misfit contraction, B(k) multiply, rank-1
+// expansion), shared by the drop-in elastic handle and the step loop.
+#pragma once
+
+#include <cstdint>
+#include <cufft.h>
+
+#include "pf5d_host.h"
+
+namespace pf5d {
+
+// D2Z / Z2D plans over a 1D/2D/3D real field of `shape` (C order); the
+// half-spectrum has shape[:-1] x (shape[-1]/2 + 1) complex values, the layout
+// of numpy's rfftn.
+struct FFTPair {
+  cufftHandle fwd = 0, inv = 0;
+  int64_t npts = 0, nk = 0;
+  bool ready = false;
+};
+
+pf5d_status fft_create(int dim, const int64_t *shape, FFTPair *p);
+void fft_destroy(FFTPair *p);
+// s (real, npts) -> k (complex, nk); k -> s.  Both on `stream`.
+pf5d_status fft_forward(FFTPair *p, double *s, cufftDoubleComplex *k, cudaStream_t stream);
+pf5d_status fft_inverse(FFTPair *p, cufftDoubleComplex *k, double *s, cudaStream_t stream);
+
+struct Vec4 {
+  double v[4];
+};
+
+// Device-side step-state halt word the step-loop kernels honour (nullptr: none).
+pf5d_status launch_misfit(const double *X, int64_t npts, Vec4 x0, Vec4 l, double *s,
+                          const unsigned *halt, cudaStream_t stream);
+pf5d_status launch_bmul(cufftDoubleComplex *k, const double *bk, int64_t nk, const unsigned *halt,
+                        cudaStream_t stream);
+pf5d_status launch_expand_add(double *mu, int64_t mu_stride, const double *s, Vec4 l,
+                              int64_t npts, cudaStream_t stream);
+
+// Host B(k) scaled by 1/N (the inverse transform's normalisation) into a new
+// device buffer.
+pf5d_status upload_bk_scaled(const double *bk_host, int64_t nk, int64_t npts, double **bk_dev);
+
+}  // namespace pf5d

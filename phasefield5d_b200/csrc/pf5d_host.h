@@ -1,0 +1,56 @@
+// pf5d_host.h -- host-side helpers shared by the library's translation units:
+// error text, CUDA/cuFFT status checks and launch geometry.
+#pragma once
+
+#include <cstdarg>
+#include <cstdint>
+#include <cstdio>
+#include <string>
+
+#include <cuda_runtime.h>
+
+#include "../../include/pf5d.h"
+
+namespace pf5d {
+
+void set_error(const char *fmt, ...);
+
+inline cudaStream_t as_stream(void *s) { return reinterpret_cast<cudaStream_t>(s); }
+
+// Number of SMs on the current device (cached per device).
+int sm_count();
+
+// Grid size for grid-stride element kernels: a multiple of the SM count.
+inline unsigned grid_for(int64_t n, int threads, int waves = 8) {
+  const int64_t want = (n + threads - 1) / threads;
+  const int64_t cap = (int64_t)sm_count() * waves;
+  return (unsigned)(want < 1 ? 1 : (want < cap ? want : cap));
+}
+
+}  // namespace pf5d
+
+#define PF5D_CUDA(call)                                                             \
+  do {                                                                              \
+    cudaError_t e_ = (call);                                                        \
+    if (e_ != cudaSuccess) {                                                        \
+      pf5d::set_error("%s:%d %s: %s", __FILE__, __LINE__, #call, cudaGetErrorString(e_)); \
+      return PF5D_ERR_CUDA;                                                         \
+    }                                                                               \
+  } while (0)
+
+#define PF5D_LAUNCHED()                                                             \
+  do {                                                                              \
+    cudaError_t e_ = cudaGetLastError();                                            \
+    if (e_ != cudaSuccess) {                                                        \
+      pf5d::set_error("%s:%d launch: %s", __FILE__, __LINE__, cudaGetErrorString(e_)); \
+      return PF5D_ERR_CUDA;                                                         \
+    }                                                                               \
+  } while (0)
+
+#define PF5D_REQUIRE(cond, code, ...)                                               \
+  do {                                                                              \
+    if (!(cond)) {                                                                  \
+      pf5d::set_error(__VA_ARGS__);                                                 \
+      return (code);                                                                \
+    }                                                                               \
+  } while (0)

@@ -1,0 +1,157 @@
+"""Device-resident step loop (examples/simulate.py:230-320 with saves off).
+
+``Stepper`` owns the composition field on the GPU and advances it with the
+fused CUDA step of ``libpf5d.so``: dt, time and the step counter stay on the
+device, steps are replayed from CUDA graphs, and the host only reads the
+state when asked.  The out-of-bounds test runs every ``oob_interval`` steps
+before the step, exactly where the reference driver runs it, and a hard
+violation halts the stepper with the field left as the reference leaves it.
+"""
+from __future__ import annotations
+
+import ctypes
+
+import numpy as np
+
+from . import _lib
+
+
+class Stepper:
+    """FP64 stepper for one solve.
+
+    Parameters mirror the reference driver's state: dense table ``grid``
+    (n,n,n,n,9) with its ``resolution`` and per-axis ``node_coord``; initial
+    field ``X`` (*shape, 4); ``X0``; per-component ``kappa``; cell size
+    ``dx``; rank-1 elastic factor ``lvec`` and ``bk`` = B(k) on the rfft
+    half-grid (both None: elasticity off); ``ctld``, ``t_cfl``, initial
+    ``dt``; ``adaptive`` (False: dt fixed); change limits.
+    """
+
+    def __init__(self, *, grid, resolution, node_coord, X, X0, kappa, dx, lvec, bk, ctld, t_cfl,
+                 dt, adaptive=True, lower_limit=1e-5, upper_limit=1e-3, max_change_factor=2.0,
+                 oob_interval=100, max_nn_dist=None, stream=None):
+        import torch
+        self._torch = torch
+        self.L = _lib.load()
+        self.stream = stream
+        X = np.asarray(X, dtype=np.float64) if not isinstance(X, torch.Tensor) else X
+        self.shape = tuple(int(s) for s in X.shape[:-1])
+        self.dim = len(self.shape)
+        if self.dim not in (1, 2, 3):
+            raise ValueError(f"Unsupported system_dim={self.dim}. Choose 1, 2, or 3.")
+        if isinstance(grid, torch.Tensor) and grid.is_cuda:
+            self.grid = grid.to(torch.float64).contiguous()
+        else:
+            self.grid = torch.from_numpy(np.ascontiguousarray(grid, dtype=np.float64)).cuda()
+        self.node_coord = torch.from_numpy(np.ascontiguousarray(node_coord,
+                                                                dtype=np.float64)).cuda()
+        if isinstance(X, torch.Tensor):
+            self.X = X.to(device="cuda", dtype=torch.float64).contiguous().clone()
+        else:
+            self.X = torch.from_numpy(np.ascontiguousarray(X)).cuda()
+        elastic = lvec is not None and bk is not None
+        d = _lib.StepperDesc()
+        d.dim = self.dim
+        for i, s in enumerate(self.shape):
+            d.shape[i] = s
+        for i in range(self.dim, 3):
+            d.shape[i] = 1
+        d.dx = float(dx)
+        kap = np.asarray(kappa, dtype=np.float64).reshape(-1)
+        for i in range(4):
+            d.kappa[i] = float(kap[i])
+            d.x0[i] = float(X0[i])
+            d.lvec[i] = float(lvec[i]) if elastic else 0.0
+        d.elastic = 1 if elastic else 0
+        self._bk = np.ascontiguousarray(bk, dtype=np.float64) if elastic else None
+        d.bk = (self._bk.ctypes.data_as(ctypes.POINTER(ctypes.c_double)) if elastic
+                else ctypes.POINTER(ctypes.c_double)())
+        d.grid = self.grid.data_ptr()
+        d.table_n = int(self.grid.shape[0])
+        d.nprops = int(self.grid.shape[-1])
+        d.node_stride = int(self.grid.shape[-1])
+        d.resolution = float(resolution)
+        d.node_coord = self.node_coord.data_ptr()
+        d.max_nn_dist = float(max_nn_dist) if max_nn_dist is not None else -1.0
+        d.ctld = float(ctld)
+        d.t_cfl = float(t_cfl)
+        d.lower_limit = float(lower_limit)
+        d.upper_limit = float(upper_limit)
+        d.max_change_factor = float(max_change_factor)
+        d.adaptive = 1 if adaptive else 0
+        d.dt0 = float(dt)
+        d.oob_interval = int(oob_interval)
+        self.desc = d
+        h = ctypes.c_void_p()
+        _lib.check(self.L.pf5d_stepper_create(ctypes.byref(d), _lib.ptr(self.X), self._s(),
+                                              ctypes.byref(h)), "Stepper")
+        self.h = h
+        self.steps_enqueued = 0
+
+    @classmethod
+    def from_problem(cls, prob, **kw):
+        """Stepper for a ``phasefield5d_b200.workload.Problem``."""
+        return cls(grid=prob.grid, resolution=prob.cfg.resolution, node_coord=prob.node_coord,
+                   X=prob.X_init, X0=prob.X0, kappa=prob.kappa, dx=prob.dx, lvec=prob.lvec,
+                   bk=prob.bk, ctld=prob.ctld, t_cfl=prob.t_cfl, dt=prob.dt0,
+                   adaptive=prob.cfg.adaptive, lower_limit=prob.cfg.lower_limit,
+                   upper_limit=prob.cfg.upper_limit, **kw)
+
+    def _s(self):
+        return _lib.stream_handle(self.stream)
+
+    @property
+    def n_points(self):
+        return int(np.prod(self.shape))
+
+    def advance(self, n_steps):
+        """Enqueue ``n_steps`` steps on the stream; returns without waiting."""
+        _lib.check(self.L.pf5d_stepper_advance(self.h, int(n_steps), self._s()), "advance")
+        self.steps_enqueued += int(n_steps)
+
+    def state(self):
+        """Synchronise and return {dt, time, xdotmax, step, flags, halted}."""
+        st = _lib.StepState()
+        _lib.check(self.L.pf5d_stepper_state(self.h, ctypes.byref(st), self._s()), "state")
+        return dict(dt=st.dt, time=st.time, xdotmax=st.xdotmax, step=int(st.step),
+                    flags=int(st.flags), halted=bool(st.halted))
+
+    def run(self, n_steps):
+        """Advance ``n_steps`` and return the state; ``halted`` is True when an
+        out-of-bounds check stopped the loop (simulate.py:231-239)."""
+        self.advance(n_steps)
+        return self.state()
+
+    def rate(self):
+        """dX/dt of the last step as a (*shape, 4) CUDA tensor (a view)."""
+        ptr = self.L.pf5d_stepper_rate(self.h)
+        return _tensor_from_ptr(ptr, self.n_points * 4, self._torch).view(*self.shape, 4)
+
+    def launch_stage(self, stage):
+        """Diagnostics: enqueue one stage of a step (``_lib.STAGE_*``) alone."""
+        _lib.check(self.L.pf5d_stepper_launch_stage(self.h, int(stage), self._s()), "stage")
+
+    def reset(self, dt, time=0.0):
+        """Re-read X (after the caller changed it) and restart dt/time/step."""
+        _lib.check(self.L.pf5d_stepper_reset(self.h, float(dt), float(time), self._s()), "reset")
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.L.pf5d_stepper_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def _tensor_from_ptr(ptr, n, torch):
+    """Non-owning float64 CUDA tensor over ``n`` doubles at device address ptr."""
+    class _Holder:
+        pass
+    h = _Holder()
+    h.__cuda_array_interface__ = {"shape": (n,), "typestr": "<f8", "data": (int(ptr), False),
+                                  "version": 3, "strides": None}
+    return torch.as_tensor(h, device="cuda")

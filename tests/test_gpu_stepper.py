@@ -1,0 +1,212 @@
+"""GPU parity of the fused FP64 step loop.
+
+* Small 1D/2D/3D trajectories against the reference's own golden runs
+  (tests/golden/trajectories.npz).
+* The plain-FP64 workloads at full size against the CPU oracle: 1D 1280 for
+  the full 10,000 fixed-dt steps, 2D 512x512 adaptive for a prefix of
+  steps, 3D on odd shapes.
+* Properties at full size: mass conservation over 20,000 2D steps, graph
+  block boundaries invisible, out-of-bounds halts.
+
+Tolerance (plain FP64): max |X_gpu - X_ref| <= 1e-12 * max |X_ref| after N
+steps.  The only non-bitwise step is the FFT (cuFFT vs pocketfft); the
+stricter X - X0 deviation is reported in the assertion messages.
+"""
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+FIELD_RTOL = 1e-12
+
+
+@pytest.fixture(scope="module")
+def torch_cuda():
+    import torch
+    if not torch.cuda.is_available():
+        pytest.skip("no CUDA device")
+    return torch
+
+
+def _rel(got, want, X0):
+    a = float(np.max(np.abs(got - want)))
+    return a / float(np.max(np.abs(want))), a / max(float(np.max(np.abs(want - X0))), 1e-300)
+
+
+def _golden_stepper(g, name, small_table):
+    from phasefield5d_b200.solver.table import node_coordinates
+    from phasefield5d_b200.stepper import Stepper
+    sc = g[f"{name}_scalars"]
+    dx, ctld, t_cfl, dt_nom, kappa_value, adaptive, n = sc[:7]
+    adaptive = bool(adaptive)
+    dt0 = dt_nom if adaptive else min(dt_nom, 0.005 * ctld, t_cfl)
+    st = Stepper(grid=small_table["grid"], resolution=small_table["resolution"],
+                 node_coord=node_coordinates(small_table["tree"], small_table["resolution"]),
+                 X=g[f"{name}_X_init"], X0=g[f"{name}_X0"], kappa=np.full(4, kappa_value), dx=dx,
+                 lvec=g[f"{name}_lvec"], bk=g[f"{name}_bk"], ctld=ctld, t_cfl=t_cfl, dt=dt0,
+                 adaptive=adaptive, lower_limit=sc[7], upper_limit=sc[8])
+    return st, int(n)
+
+
+@pytest.mark.parametrize("name", ["1d_fixed", "1d_adapt", "2d_adapt", "3d_adapt"])
+def test_golden_trajectory(torch_cuda, small_table, traj_golden, name):
+    g = traj_golden
+    st, n = _golden_stepper(g, name, small_table)
+    state = st.run(n)
+    X = st.X.cpu().numpy()
+    want = g[f"{name}_X_final"]
+    r_field, r_dev = _rel(X, want, g[f"{name}_X0"])
+    assert state["step"] == n and not state["halted"]
+    assert r_field <= FIELD_RTOL, f"{name}: field rel {r_field:.2e} (X-X0 rel {r_dev:.2e})"
+    assert abs(state["time"] - float(g[f"{name}_time"])) <= 1e-12 * float(g[f"{name}_time"])
+    assert abs(state["dt"] - g[f"{name}_dts"][-1]) <= 1e-12 * g[f"{name}_dts"][-1]
+    st.close()
+
+
+def _problem(mk, **over):
+    from phasefield5d_b200 import workload as W
+    cfg = mk()
+    for k, v in over.items():
+        setattr(cfg, k, v)
+    return W.build_problem(cfg)
+
+
+def test_1d_full_fixed_dt_vs_oracle(torch_cuda):
+    """1D 1280 cells, fixed dt, all 10,000 steps."""
+    from oracle.oracle import OracleStepper
+    from phasefield5d_b200 import workload as W
+    from phasefield5d_b200.stepper import Stepper
+    prob = _problem(W.config_1d_fixed)
+    n = prob.cfg.total_timesteps
+    gpu = Stepper.from_problem(prob)
+    state = gpu.run(n)
+    ref = OracleStepper.from_problem(prob)
+    ref.run(n)
+    r_field, r_dev = _rel(gpu.X.cpu().numpy(), ref.X, prob.X0)
+    assert state["step"] == n
+    assert r_field <= FIELD_RTOL, f"field rel {r_field:.2e} (X-X0 rel {r_dev:.2e})"
+    assert state["time"] == pytest.approx(ref.time, rel=1e-14)
+    gpu.close()
+
+
+def test_2d_512_adaptive_prefix_vs_oracle(torch_cuda):
+    """2D 512x512 adaptive: the first 200 steps against the oracle."""
+    from oracle.oracle import OracleStepper
+    from phasefield5d_b200 import workload as W
+    from phasefield5d_b200.stepper import Stepper
+    prob = _problem(W.config_2d_adaptive)
+    n = 200
+    gpu = Stepper.from_problem(prob)
+    state = gpu.run(n)
+    ref = OracleStepper.from_problem(prob)
+    ref.run(n)
+    r_field, r_dev = _rel(gpu.X.cpu().numpy(), ref.X, prob.X0)
+    assert r_field <= FIELD_RTOL, f"field rel {r_field:.2e} (X-X0 rel {r_dev:.2e})"
+    assert state["dt"] == pytest.approx(ref.dt, rel=1e-12)
+    assert state["xdotmax"] == pytest.approx(ref.xdotmax, rel=1e-10)
+    gpu.close()
+
+
+def test_2d_512_full_run_conserves_mass(torch_cuda):
+    """All 20,000 adaptive steps on the GPU: the flux form conserves each
+    component's mean (up to rounding), no halt, finite field."""
+    from phasefield5d_b200 import workload as W
+    from phasefield5d_b200.stepper import Stepper
+    prob = _problem(W.config_2d_adaptive)
+    gpu = Stepper.from_problem(prob)
+    m0 = prob.X_init.reshape(-1, 4).mean(axis=0)
+    state = gpu.run(prob.cfg.total_timesteps)
+    X = gpu.X.cpu().numpy()
+    assert state["step"] == prob.cfg.total_timesteps and not state["halted"]
+    assert np.isfinite(X).all()
+    drift = np.max(np.abs(X.reshape(-1, 4).mean(axis=0) - m0))
+    assert drift <= 1e-13, drift
+    gpu.close()
+
+
+@pytest.mark.parametrize("shape,n", [((20, 18, 24), 12), ((10, 13, 37), 8), ((7, 33), 40),
+                                     ((131,), 60)])
+def test_odd_shapes_vs_oracle(torch_cuda, shape, n):
+    """Shapes that are not multiples of the tiles (partial tiles, wrap-around halos)."""
+    from oracle.oracle import OracleStepper
+    from phasefield5d_b200 import workload as W
+    from phasefield5d_b200.stepper import Stepper
+    cfg = W.SolveConfig(system_dim=len(shape), initial_composition=(0.1, 0.2, 0.2, 0.25),
+                        resolution=0.05, kappa_value=5e-16, mw=4, ppw=16, shape=shape,
+                        adaptive=True, n_k=2000, fluctuation=3e-2)
+    prob = W.build_problem(cfg)
+    gpu = Stepper.from_problem(prob)
+    gpu.run(n)
+    ref = OracleStepper.from_problem(prob)
+    ref.run(n)
+    r_field, r_dev = _rel(gpu.X.cpu().numpy(), ref.X, prob.X0)
+    assert r_field <= FIELD_RTOL, f"{shape}: field rel {r_field:.2e} (X-X0 rel {r_dev:.2e})"
+    gpu.close()
+
+
+def test_nearest_row_fallback_inside_step(torch_cuda):
+    """Composition straddling the linear-region threshold: part of the field
+    takes the nearest-row branch every step."""
+    from oracle.oracle import OracleStepper
+    from phasefield5d_b200 import workload as W
+    from phasefield5d_b200.stepper import Stepper
+    cfg = W.SolveConfig(system_dim=2, initial_composition=(0.1, 0.2, 0.2, 0.25), resolution=0.05,
+                        kappa_value=5e-16, mw=4, ppw=16, shape=(24, 20), adaptive=True, n_k=2000)
+    prob = W.build_problem(cfg)
+    rng = np.random.default_rng(11)
+    X = prob.X_init.copy()
+    X[..., 3] += rng.uniform(0.0, 0.1, size=X.shape[:-1])      # sums up to 0.85 > 0.8 threshold
+    prob.X_init = X
+    gpu = Stepper.from_problem(prob)
+    state = gpu.run(30)
+    ref = OracleStepper.from_problem(prob)
+    ref.run(30)
+    assert state["flags"] & 0x20            # nearest-row branch used
+    r_field, _ = _rel(gpu.X.cpu().numpy(), ref.X, prob.X0)
+    assert r_field <= FIELD_RTOL
+    gpu.close()
+
+
+def test_graph_blocks_are_invisible(torch_cuda):
+    """advance(37) + advance(83) equals advance(120) bit for bit."""
+    from phasefield5d_b200 import workload as W
+    from phasefield5d_b200.stepper import Stepper
+    cfg = W.SolveConfig(system_dim=2, initial_composition=(0.1, 0.2, 0.2, 0.25), resolution=0.05,
+                        kappa_value=5e-16, mw=4, ppw=16, shape=(40, 36), adaptive=True, n_k=2000)
+    prob = W.build_problem(cfg)
+    a = Stepper.from_problem(prob)
+    a.advance(37)
+    a.advance(83)
+    sa = a.state()
+    b = Stepper.from_problem(prob)
+    sb = b.run(120)
+    assert sa == sb
+    assert np.array_equal(a.X.cpu().numpy(), b.X.cpu().numpy())
+    a.close()
+    b.close()
+
+
+@pytest.mark.parametrize("inject", ["nan", "sum_over_one", "negative"])
+def test_out_of_bounds_halts(torch_cuda, inject):
+    """Host-made failure: a bad initial field halts the loop at the step-0
+    check (simulate.py:231) with the field untouched."""
+    from phasefield5d_b200 import workload as W
+    from phasefield5d_b200.stepper import Stepper
+    cfg = W.SolveConfig(system_dim=1, initial_composition=(0.1, 0.2, 0.2, 0.25), resolution=0.05,
+                        kappa_value=5e-16, mw=4, ppw=16, shape=(64,), adaptive=True, n_k=2000)
+    prob = W.build_problem(cfg)
+    X = prob.X_init.copy()
+    if inject == "nan":
+        X[5, 2] = np.nan
+    elif inject == "sum_over_one":
+        X[7] = [0.3, 0.3, 0.3, 0.2]
+    else:
+        X[9, 1] = -0.01
+    prob.X_init = X
+    gpu = Stepper.from_problem(prob)
+    state = gpu.run(50)
+    assert state["halted"] and state["step"] == 0 and state["time"] == 0.0
+    got = gpu.X.cpu().numpy()
+    assert np.array_equal(np.isnan(got), np.isnan(X))
+    assert np.array_equal(np.nan_to_num(got), np.nan_to_num(X))
+    gpu.close()
