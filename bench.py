@@ -44,6 +44,8 @@ WORKLOADS = {
     "2d": ("plain FP64 2D 512x512, 41^4 table, elastic, adaptive dt", "config_2d_adaptive"),
     "1d": ("plain FP64 1D 1280, 41^4 table, elastic, fixed dt", "config_1d_fixed"),
     "3d": ("plain FP64 3D 256^3, 51^4 table, elastic, adaptive dt", "config_3d_precision"),
+    "3d128": ("plain FP64 3D 128^3, 51^4 table, elastic, adaptive dt (profiling size)",
+              "config_3d_precision", (128, 128, 128)),
 }
 
 
@@ -61,7 +63,10 @@ def parse():
 
 def build_problem(name):
     from phasefield5d_b200 import workload as W
-    return W.build_problem(getattr(W, WORKLOADS[name][1])())
+    cfg = getattr(W, WORKLOADS[name][1])()
+    if len(WORKLOADS[name]) > 2:
+        cfg.shape = WORKLOADS[name][2]
+    return W.build_problem(cfg)
 
 
 def measured_peak():
@@ -84,46 +89,68 @@ def committed_traffic(kernel, workload):
 
 
 class ClockSampler:
-    """nvidia-smi clock/throttle samples every 200 ms while running."""
-    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+    """nvidia-smi clock/throttle samples every 200 ms.  ``start`` waits for a
+    first sample and ``stop`` for one more after the timed region, so the
+    samples bracket it even when the region is shorter than the period."""
+    Q = ("timestamp,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
          "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
          "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+    NAMES = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
 
     def __init__(self, index):
         self.index = index
-        self.f = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+        self.path = tempfile.NamedTemporaryFile("w", suffix=".csv", delete=False).name
+        self.p = None
         try:
             self.p = subprocess.Popen(["nvidia-smi", f"--id={index}", f"--query-gpu={self.Q}",
-                                       "--format=csv,noheader,nounits", "-lms", "200"],
-                                      stdout=self.f, stderr=subprocess.DEVNULL)
+                                       "--format=csv,noheader,nounits", "-lms", "200",
+                                       "-f", self.path], stderr=subprocess.DEVNULL)
         except Exception:
             self.p = None
+
+    def _rows(self):
+        try:
+            with open(self.path) as f:
+                return [[x.strip() for x in line.split(",")] for line in f
+                        if line.count(",") >= 8]
+        except OSError:
+            return []
+
+    def _wait_rows(self, n, timeout=3.0):
+        t0 = time.time()
+        while self.p is not None and len(self._rows()) < n and time.time() - t0 < timeout:
+            time.sleep(0.05)
+
+    def start(self):
+        self._wait_rows(1)
+        self.n0 = max(len(self._rows()) - 1, 0)
+        return self
 
     def stop(self):
         if self.p is None:
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self._wait_rows(len(self._rows()) + 1)
         self.p.terminate()
         try:
             self.p.wait(timeout=5)
         except Exception:
             self.p.kill()
-        self.f.flush()
-        rows = []
-        with open(self.f.name) as f:
-            for line in f:
-                parts = [p.strip() for p in line.split(",")]
-                if len(parts) >= 9:
-                    rows.append(parts)
-        os.unlink(self.f.name)
+        rows = self._rows()[self.n0:]
+        os.unlink(self.path)
         if not rows:
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no samples"]}
-        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
-        mx = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        reasons = sorted({names[i] for r in rows for i in range(4) if r[5 + i] == "Active"})
+
+        def num(v):
+            try:
+                return float(v)
+            except ValueError:
+                return None
+        sm = [v for v in (num(r[1]) for r in rows) if v is not None]
+        mx = [v for v in (num(r[2]) for r in rows) if v is not None]
+        reasons = sorted({self.NAMES[i] for r in rows for i in range(4) if r[5 + i] == "Active"})
         return {"sm_mhz": statistics.median(sm) if sm else None,
                 "sm_max_mhz": max(mx) if mx else None, "reasons": reasons,
-                "samples": len(rows)}
+                "samples": len(rows), "window": "samples bracketing the timed region"}
 
 
 def cpu_threads():
@@ -190,7 +217,7 @@ def run_ours(args, rank, world, local_rank):
         flush.zero_()
         st.advance(1)
     barrier()
-    clocks = ClockSampler(local_rank)
+    clocks = ClockSampler(local_rank).start()
     ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
           for _ in range(args.steps)]
     for e0, e1 in ev:

@@ -67,7 +67,10 @@ __device__ __forceinline__ bool linear_region(const Table &T, const double x[S])
 // Quadrilinear interpolation of NP props at x (interpolation.py:103-147).
 // Corner order c = b0 b1 b2 b3 (binary), weights ((w0*w1)*w2)*w3, per-prop
 // sum of the 16 terms left to right.  Corners are visited outermost so each
-// corner's NP props are one contiguous run of the node.
+// corner's NP props are one contiguous run of the node.  VEC: the node
+// stride is even and the table 16-byte aligned, so a node is read as
+// double2 pairs.
+template <bool VEC>
 __device__ __forceinline__ void interp_linear(const Table &T, const double x[S], double out[NP]) {
   int i0, i1, i2, i3;
   double t0, t1, t2, t3;
@@ -84,16 +87,30 @@ __device__ __forceinline__ void interp_linear(const Table &T, const double x[S],
     const int b0 = (c >> 3) & 1, b1 = (c >> 2) & 1, b2 = (c >> 1) & 1, b3 = c & 1;
     const double w = (b0 ? t0 : q0) * (b1 ? t1 : q1) * (b2 ? t2 : q2) * (b3 ? t3 : q3);
     const double *node = base + b0 * s0 + b1 * s1 + b2 * s2 + b3 * s3;
+    double v[NP + 1];
+    if (VEC) {
+      const double2 *n2 = reinterpret_cast<const double2 *>(node);
+#pragma unroll
+      for (int k = 0; k < (NP + 1) / 2; ++k) {
+        const double2 a = __ldg(n2 + k);
+        v[2 * k] = a.x;
+        v[2 * k + 1] = a.y;
+      }
+    } else {
+#pragma unroll
+      for (int p = 0; p < NP; ++p) v[p] = __ldg(node + p);
+    }
 #pragma unroll
     for (int p = 0; p < NP; ++p) {
-      const double term = w * __ldg(node + p);
+      const double term = w * v[p];
       out[p] = (c == 0) ? term : out[p] + term;
     }
   }
 }
 
 // Nearest table row for a point outside the linear region
-// (interpolation.py:203-209, cKDTree over the row compositions).
+// (interpolation.py:203-209, cKDTree over the row compositions); returns the
+// node index (the caller reads the row).
 //
 // Rows sit on grid nodes, so the nearest row is the nearest present node.
 // Every node within two cells of x along each axis is inside the
@@ -103,8 +120,14 @@ __device__ __forceinline__ void interp_linear(const Table &T, const double x[S],
 // simplex table).  Farther results set PF5D_FLAG_NN_TRUNCATED.  Distances
 // are accumulated as sum_d (x_d - c_d)^2 in axis order; on an exact tie the
 // first node in lexicographic order wins.
-static __device__ __noinline__ void interp_nearest(const Table T, const double *x, double *out,
-                                            unsigned *flag_bits) {
+struct NearestNode {
+  int64_t node;        // -1: nothing present in the window
+  unsigned flags;      // PF5D_FLAG_NN_*
+};
+
+static __device__ __noinline__ NearestNode nearest_node(const Table T, double x0, double x1,
+                                                        double x2, double x3) {
+  const double x[S] = {x0, x1, x2, x3};
   const int N = T.n - 1;
   int lo[S], hi[S];
 #pragma unroll
@@ -143,27 +166,27 @@ static __device__ __noinline__ void interp_nearest(const Table T, const double *
       }
     }
   }
-  unsigned f = PF5D_FLAG_NN_USED;
-  if (best_node < 0) {
-    f |= PF5D_FLAG_NN_TRUNCATED;
-    for (int p = 0; p < NP; ++p) out[p] = __longlong_as_double(0x7ff8000000000000LL);
-  } else {
-    if (!(best < T.exact_d2)) f |= PF5D_FLAG_NN_TRUNCATED;
-    if (T.max_nn_dist > 0.0 && sqrt(best) > T.max_nn_dist) f |= PF5D_FLAG_NN_FAR;
-    const double *row = T.grid + best_node * T.stride;
-    for (int p = 0; p < NP; ++p) out[p] = __ldg(row + p);
-  }
-  *flag_bits |= f;
+  NearestNode r{best_node, PF5D_FLAG_NN_USED};
+  if (best_node < 0 || !(best < T.exact_d2)) r.flags |= PF5D_FLAG_NN_TRUNCATED;
+  if (best_node >= 0 && T.max_nn_dist > 0.0 && sqrt(best) > T.max_nn_dist)
+    r.flags |= PF5D_FLAG_NN_FAR;
+  return r;
 }
 
 // Interpolation with fallback for one point; returns true on the linear branch.
+template <bool VEC = false>
 __device__ __forceinline__ bool interp_point(const Table &T, const double x[S], double out[NP],
                                              unsigned *flag_bits) {
   if (linear_region(T, x)) {
-    interp_linear(T, x, out);
+    interp_linear<VEC>(T, x, out);
     return true;
   }
-  interp_nearest(T, x, out, flag_bits);
+  const NearestNode r = nearest_node(T, x[0], x[1], x[2], x[3]);
+  *flag_bits |= r.flags;
+  const double *row = T.grid + (r.node < 0 ? 0 : r.node) * T.stride;
+#pragma unroll
+  for (int p = 0; p < NP; ++p)
+    out[p] = r.node < 0 ? __longlong_as_double(0x7ff8000000000000LL) : __ldg(row + p);
   return false;
 }
 

@@ -46,7 +46,7 @@ struct StepState {
 };
 
 struct RateParams {
-  int nz, ny, nx;              // axis 0 (march), axis 1 (3D only, else 1), last axis
+  int nz, ny, nx;              // 3D: (n0, n1, n2); 2D: (1, n0, n1); 1D: (1, 1, n0)
   const double *X;
   const double *sp;            // s' (already scaled by 1/N) or nullptr
   double *dX;
@@ -63,11 +63,12 @@ struct RateParams {
 // ------------------------------------------------------------------------
 
 // chemical potential and mobility at one point (examples/simulate.py:242-258).
+template <bool VEC>
 __device__ __forceinline__ void chem_point(const RateParams &P, const double x[S],
                                            const double lap[S], double spv, double mu[S],
                                            double M[NM], unsigned *flags) {
   double v[NP];
-  interp_point(P.T, x, v, flags);
+  interp_point<VEC>(P.T, x, v, flags);
 #pragma unroll
   for (int c = 0; c < S; ++c) {
     const double lk = lap[c] * P.kappa.v[c];
@@ -112,128 +113,231 @@ __device__ __forceinline__ void finish_rate(const RateParams &P, double m, doubl
   }
 }
 
-// ------------------------------------------------------------------------
-// 2D / 3D marching kernel
-// ------------------------------------------------------------------------
-// Plane = TY x TX tile of (axis 1, last axis) for DIM 3, a TX row segment of
-// the last axis for DIM 2 (TY = 1).  X ring: 3 planes with a 2-cell halo
-// (HY x HX).  mu/M ring: 2 planes with a 1-cell halo (MY x MX), 9 values per
-// point (mu 0..3, M 4..8).  Face buffers hold the tile's +x / +y fluxes and
-// the tile-boundary -x / -y fluxes.
-template <int DIM, int TX, int TY>
-struct MarchGeom {
-  static constexpr int HX = TX + 4, HY = DIM == 3 ? TY + 4 : 1, PX = HX * HY;
-  static constexpr int MX = TX + 2, MY = DIM == 3 ? TY + 2 : 1, PM = MX * MY;
+// Shared-memory geometry of one plane tile: TY rows (axis "y") x TX columns
+// (the contiguous axis "x").  X is staged with a 2-cell halo (HY x HX), mu/M
+// with a 1-cell halo (MY x MX, corners unused).  x-faces: TY x (TX+1),
+// face (y, f) lies between columns f-1 and f; y-faces: (TY+1) x TX, face
+// (f, x) lies between rows f-1 and f.
+template <int TX, int TY>
+struct PlaneGeom {
+  static constexpr int HX = TX + 4, HY = TY + 4, PX = HX * HY;
+  static constexpr int MX = TX + 2, MY = TY + 2, PM = MX * MY;
   static constexpr int NT = TX * TY;
-  static constexpr int FXN = TY * (TX + 1), FYN = DIM == 3 ? (TY + 1) * TX : 0;
-  static constexpr size_t smem_doubles =
-      3 * S * PX + 2 * NP * PM + S * FXN + S * FYN + (NT + 31) / 32;
-  static constexpr size_t smem_bytes = smem_doubles * sizeof(double);
+  static constexpr int NFX = TY * (TX + 1), NFY = (TY + 1) * TX;
 };
 
-template <int DIM, int TX, int TY>
-__global__ void __launch_bounds__(TX * TY, DIM == 3 ? 2 : 4)
-    k_rate_march(RateParams P, int zc) {
-  using G = MarchGeom<DIM, TX, TY>;
+// Flux through the face between (X plane XL, pos pl ; mu/M plane ML, pos ql)
+// and (XH, ph ; MH, qh), lower -> upper along one axis.
+template <int PX, int PM>
+__device__ __forceinline__ void face_between(const double *XL, const double *ML, int pl, int ql,
+                                             const double *XH, const double *MH, int ph, int qh,
+                                             double inv_dx, double J[S]) {
+  double Xc[S], Xn[S], Mc[NM], Mn[NM], g[S];
+#pragma unroll
+  for (int c = 0; c < S; ++c) {
+    Xc[c] = XL[c * PX + pl];
+    Xn[c] = XH[c * PX + ph];
+    g[c] = (MH[c * PM + qh] - ML[c * PM + ql]) * inv_dx;
+  }
+#pragma unroll
+  for (int c = 0; c < NM; ++c) {
+    Mc[c] = ML[(S + c) * PM + ql];
+    Mn[c] = MH[(S + c) * PM + qh];
+  }
+  face_flux(Xc, Mc, Xn, Mn, g, J);
+}
+
+// All x- and y-faces of one plane tile into Fx / Fy (flat loop: every
+// thread takes faces in turn).
+template <int TX, int TY>
+__device__ __forceinline__ void plane_faces(const double *Xp, const double *Mp, double *Fx,
+                                            double *Fy, double inv_dx, int tid) {
+  using G = PlaneGeom<TX, TY>;
+  for (int f = tid; f < G::NFX + G::NFY; f += G::NT) {
+    double J[S];
+    if (f < G::NFX) {
+      const int fy = f / (TX + 1), fx = f - fy * (TX + 1);
+      const int pl = (fy + 2) * G::HX + (fx + 1), ql = (fy + 1) * G::MX + fx;
+      face_between<G::PX, G::PM>(Xp, Mp, pl, ql, Xp, Mp, pl + 1, ql + 1, inv_dx, J);
+#pragma unroll
+      for (int c = 0; c < S; ++c) Fx[c * G::NFX + f] = J[c];
+    } else {
+      const int f2 = f - G::NFX;
+      const int fy = f2 / TX, fx = f2 - fy * TX;
+      const int pl = (fy + 1) * G::HX + (fx + 2), ql = fy * G::MX + (fx + 1);
+      face_between<G::PX, G::PM>(Xp, Mp, pl, ql, Xp, Mp, pl + G::HX, ql + G::MX, inv_dx, J);
+#pragma unroll
+      for (int c = 0; c < S; ++c) Fy[c * G::NFY + f2] = J[c];
+    }
+  }
+}
+
+// Stage one X plane (tile + 2-cell halo) into SoA shared memory.
+template <int TX, int TY>
+__device__ __forceinline__ void load_plane(const double *__restrict__ X, int64_t plane_off,
+                                           const int *wx, const int *wy, int nx, double *dst,
+                                           int tid) {
+  using G = PlaneGeom<TX, TY>;
+  for (int pos = tid; pos < G::PX; pos += G::NT) {
+    const int hy = pos / G::HX, hx = pos - hy * G::HX;
+    const int64_t g = plane_off + (int64_t)wy[hy] * nx + wx[hx];
+    const double2 a = __ldg(reinterpret_cast<const double2 *>(X + 4 * g));
+    const double2 b = __ldg(reinterpret_cast<const double2 *>(X + 4 * g) + 1);
+    dst[0 * G::PX + pos] = a.x;
+    dst[1 * G::PX + pos] = a.y;
+    dst[2 * G::PX + pos] = b.x;
+    dst[3 * G::PX + pos] = b.y;
+  }
+}
+
+// ------------------------------------------------------------------------
+// 2D kernel: one plane tile per block, one point per thread.
+// ------------------------------------------------------------------------
+// Axis 0 of the (n0, n1) field is the tile's y, axis 1 its x.  Laplacian
+// (operators.py:49-60) and divergence (fluxes.py:349) keep the reference's
+// axis order: axis-0 terms first.
+template <int TX, int TY, bool VEC>
+__global__ void __launch_bounds__(TX * TY, 2) k_rate_tile2d(RateParams P) {
+  using G = PlaneGeom<TX, TY>;
   if (P.st->halt) return;
   extern __shared__ double sm[];
-  double *Xs = sm;                                  // [3][S][PX]
-  double *Ms = Xs + 3 * S * G::PX;                  // [2][NP][PM]
-  double *Fx = Ms + 2 * NP * G::PM;                 // [S][TY][TX+1]
-  double *Fy = Fx + S * G::FXN;                     // [S][TY+1][TX]
-  double *red = Fy + S * G::FYN;
-
+  double *Xs = sm;                       // [S][PX]
+  double *Ms = Xs + S * G::PX;           // [NP][PM]
+  double *Fx = Ms + NP * G::PM;          // [S][NFX]
+  double *Fy = Fx + S * G::NFX;          // [S][NFY]
+  double *red = Fy + S * G::NFY;         // [NT/32]
+  int *wx = reinterpret_cast<int *>(red + G::NT / 32);   // [HX]
+  int *wy = wx + G::HX;                                  // [HY]
   const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * TX + tx;
-  const int x0 = blockIdx.x * TX, y0 = (DIM == 3) ? blockIdx.y * TY : 0;
-  const int zb = blockIdx.z * zc;
-  const int ze = min(zb + zc, P.nz);
+  const int x0 = blockIdx.x * TX, y0 = blockIdx.y * TY;
   unsigned flags = 0;
 
+  for (int i = tid; i < G::HX + G::HY; i += G::NT) {
+    if (i < G::HX) wx[i] = wrap_any(x0 + i - 2, P.nx);
+    else wy[i - G::HX] = wrap_any(y0 + (i - G::HX) - 2, P.ny);
+  }
+  __syncthreads();
+  load_plane<TX, TY>(P.X, 0, wx, wy, P.nx, Xs, tid);
+  __syncthreads();
+  for (int pos = tid; pos < G::PM; pos += G::NT) {
+    const int my = pos / G::MX, mx = pos - my * G::MX;
+    if ((mx == 0 || mx == G::MX - 1) && (my == 0 || my == G::MY - 1)) continue;
+    const int px = (my + 1) * G::HX + (mx + 1);
+    double x[S], lap[S];
+#pragma unroll
+    for (int c = 0; c < S; ++c) {
+      const double *q = Xs + c * G::PX;
+      x[c] = q[px];
+      lap[c] = (q[px + G::HX] + q[px - G::HX] + q[px + 1] + q[px - 1] - 4.0 * x[c]) * P.inv_dx2;
+    }
+    const double spv = P.sp ? __ldg(P.sp + (int64_t)wy[my + 1] * P.nx + wx[mx + 1]) : 0.0;
+    double mu[S], M[NM];
+    chem_point<VEC>(P, x, lap, spv, mu, M, &flags);
+#pragma unroll
+    for (int c = 0; c < S; ++c) Ms[c * G::PM + pos] = mu[c];
+#pragma unroll
+    for (int c = 0; c < NM; ++c) Ms[(S + c) * G::PM + pos] = M[c];
+  }
+  __syncthreads();
+  plane_faces<TX, TY>(Xs, Ms, Fx, Fy, P.inv_dx, tid);
+  __syncthreads();
+  double vmax = 0.0;
+  if (x0 + tx < P.nx && y0 + ty < P.ny) {
+    double out[S];
+#pragma unroll
+    for (int c = 0; c < S; ++c) {
+      double a = Fy[c * G::NFY + (ty + 1) * TX + tx] - Fy[c * G::NFY + ty * TX + tx];
+      a = a + Fx[c * G::NFX + ty * (TX + 1) + tx + 1];
+      a = a - Fx[c * G::NFX + ty * (TX + 1) + tx];
+      out[c] = a * P.inv_dx;
+      const double v = fabs(out[c]);
+      if (v > vmax) vmax = v;
+    }
+    const int64_t g = (int64_t)(y0 + ty) * P.nx + (x0 + tx);
+    double2 *o = reinterpret_cast<double2 *>(P.dX + 4 * g);
+    o[0] = make_double2(out[0], out[1]);
+    o[1] = make_double2(out[2], out[3]);
+  }
+  if (flags) atomicOr(&P.st->flags, flags);
+  finish_rate(P, vmax, red);
+}
+
+template <int TX, int TY>
+constexpr size_t tile2d_smem() {
+  using G = PlaneGeom<TX, TY>;
+  return (S * G::PX + NP * G::PM + S * G::NFX + S * G::NFY + G::NT / 32) * sizeof(double) +
+         (G::HX + G::HY) * sizeof(int);
+}
+
+// ------------------------------------------------------------------------
+// 3D kernel: plane tile marching along axis 0
+// ------------------------------------------------------------------------
+// Each block owns a TY x TX tile of (axis 1, axis 2) and a chunk of axis-0
+// planes.  Rings in shared memory: 3 X planes (2-cell halo), 2 mu/M planes
+// (1-cell halo).  Per output plane z: stage X(z+2), evaluate mu/M(z+1),
+// compute the plane's x/y faces (flat loop) and each point's +z face, and
+// form the divergence with the -z face kept in registers from plane z-1.
+// Laplacian order (operators.py:68-76): +z, -z, +y, -y, +x, -x.
+template <int TX, int TY, bool VEC>
+__global__ void __launch_bounds__(TX * TY, 2) k_rate_march3d(RateParams P, int zc) {
+  using G = PlaneGeom<TX, TY>;
+  if (P.st->halt) return;
+  extern __shared__ double sm[];
+  double *Xs = sm;                       // [3][S][PX]
+  double *Ms = Xs + 3 * S * G::PX;       // [2][NP][PM]
+  double *Fx = Ms + 2 * NP * G::PM;      // [S][NFX]
+  double *Fy = Fx + S * G::NFX;          // [S][NFY]
+  double *red = Fy + S * G::NFY;         // [NT/32]
+  int *wx = reinterpret_cast<int *>(red + G::NT / 32);
+  int *wy = wx + G::HX;
+  const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * TX + tx;
+  const int x0 = blockIdx.x * TX, y0 = blockIdx.y * TY;
+  const int zb = blockIdx.z * zc;
+  const int ze = min(zb + zc, P.nz);
+  const int64_t plane = (int64_t)P.ny * P.nx;
+  unsigned flags = 0;
+
+  for (int i = tid; i < G::HX + G::HY; i += G::NT) {
+    if (i < G::HX) wx[i] = wrap_any(x0 + i - 2, P.nx);
+    else wy[i - G::HX] = wrap_any(y0 + (i - G::HX) - 2, P.ny);
+  }
   auto xplane = [&](int z) { return Xs + ((z - zb + 3) % 3) * S * G::PX; };
   auto mplane = [&](int z) { return Ms + ((z - zb + 2) & 1) * NP * G::PM; };
-
   auto load_x = [&](int z) {
-    double *dst = xplane(z);
-    const int zw = wrap_any(z, P.nz);
-    for (int pos = tid; pos < G::PX; pos += G::NT) {
-      const int hx = pos % G::HX, hy = pos / G::HX;
-      const int gx = wrap_any(x0 + hx - 2, P.nx);
-      const int gy = (DIM == 3) ? wrap_any(y0 + hy - 2, P.ny) : 0;
-      const int64_t g = ((int64_t)zw * P.ny + gy) * P.nx + gx;
-      const double2 a = __ldg(reinterpret_cast<const double2 *>(P.X + 4 * g));
-      const double2 b = __ldg(reinterpret_cast<const double2 *>(P.X + 4 * g) + 1);
-      dst[0 * G::PX + pos] = a.x;
-      dst[1 * G::PX + pos] = a.y;
-      dst[2 * G::PX + pos] = b.x;
-      dst[3 * G::PX + pos] = b.y;
-    }
+    load_plane<TX, TY>(P.X, (int64_t)wrap_any(z, P.nz) * plane, wx, wy, P.nx, xplane(z), tid);
   };
-
-  // mu/M of plane z at muM positions; interior_only: tile positions only.
   auto compute_mu = [&](int z, bool interior_only) {
-    const double *Xm = xplane(z - 1), *X0p = xplane(z), *Xp = xplane(z + 1);
+    const double *Xm = xplane(z - 1), *Xc = xplane(z), *Xp = xplane(z + 1);
     double *dst = mplane(z);
-    const int zw = wrap_any(z, P.nz);
+    const int64_t zoff = (int64_t)wrap_any(z, P.nz) * plane;
     for (int pos = tid; pos < G::PM; pos += G::NT) {
-      const int mx = pos % G::MX, my = pos / G::MX;
-      const bool edge_x = (mx == 0 || mx == G::MX - 1);
-      const bool edge_y = (DIM == 3) && (my == 0 || my == G::MY - 1);
-      if (interior_only ? (edge_x || edge_y) : (edge_x && edge_y)) continue;
-      const int px = (DIM == 3) ? (my + 1) * G::HX + (mx + 1) : (mx + 1);
+      const int my = pos / G::MX, mx = pos - my * G::MX;
+      const bool ex = (mx == 0 || mx == G::MX - 1), ey = (my == 0 || my == G::MY - 1);
+      if (interior_only ? (ex || ey) : (ex && ey)) continue;
+      const int px = (my + 1) * G::HX + (mx + 1);
       double x[S], lap[S];
 #pragma unroll
       for (int c = 0; c < S; ++c) {
-        const double *q = X0p + c * G::PX;
+        const double *q = Xc + c * G::PX;
         x[c] = q[px];
-        double a = Xp[c * G::PX + px] + Xm[c * G::PX + px];
-        if (DIM == 3) {
-          a = a + q[px + G::HX];
-          a = a + q[px - G::HX];
-        }
-        a = a + q[px + 1];
-        a = a + q[px - 1];
-        lap[c] = (a - (DIM == 3 ? 6.0 : 4.0) * x[c]) * P.inv_dx2;
+        lap[c] = (Xp[c * G::PX + px] + Xm[c * G::PX + px] + q[px + G::HX] + q[px - G::HX] +
+                  q[px + 1] + q[px - 1] - 6.0 * x[c]) * P.inv_dx2;
       }
-      double spv = 0.0;
-      if (P.sp) {
-        const int gx = wrap_any(x0 + mx - 1, P.nx);
-        const int gy = (DIM == 3) ? wrap_any(y0 + my - 1, P.ny) : 0;
-        spv = __ldg(P.sp + ((int64_t)zw * P.ny + gy) * P.nx + gx);
-      }
+      const double spv =
+          P.sp ? __ldg(P.sp + zoff + (int64_t)wy[my + 1] * P.nx + wx[mx + 1]) : 0.0;
       double mu[S], M[NM];
-      chem_point(P, x, lap, spv, mu, M, &flags);
+      chem_point<VEC>(P, x, lap, spv, mu, M, &flags);
 #pragma unroll
       for (int c = 0; c < S; ++c) dst[c * G::PM + pos] = mu[c];
 #pragma unroll
       for (int c = 0; c < NM; ++c) dst[(S + c) * G::PM + pos] = M[c];
     }
   };
+  const int pX = (ty + 2) * G::HX + (tx + 2);
+  const int pM = (ty + 1) * G::MX + (tx + 1);
+  const bool in_tile = (x0 + tx < P.nx) && (y0 + ty < P.ny);
 
-  // flux through the face between (plane zl, X pos pl, muM pos ql) and (zh, ph, qh).
-  auto face = [&](int zl, int pl, int ql, int zh, int ph, int qh, double J[S]) {
-    const double *XL = xplane(zl), *XH = xplane(zh);
-    const double *ML = mplane(zl), *MH = mplane(zh);
-    double Xc[S], Xn[S], Mc[NM], Mn[NM], g[S];
-#pragma unroll
-    for (int c = 0; c < S; ++c) {
-      Xc[c] = XL[c * G::PX + pl];
-      Xn[c] = XH[c * G::PX + ph];
-      g[c] = (MH[c * G::PM + qh] - ML[c * G::PM + ql]) * P.inv_dx;
-    }
-#pragma unroll
-    for (int c = 0; c < NM; ++c) {
-      Mc[c] = ML[(S + c) * G::PM + ql];
-      Mn[c] = MH[(S + c) * G::PM + qh];
-    }
-    face_flux(Xc, Mc, Xn, Mn, g, J);
-  };
-
-  const int pX = (DIM == 3) ? (ty + 2) * G::HX + (tx + 2) : (tx + 2);
-  const int pM = (DIM == 3) ? (ty + 1) * G::MX + (tx + 1) : (tx + 1);
-  const bool in_tile = (x0 + tx < P.nx) && (DIM == 2 || y0 + ty < P.ny);
-
-  // Prologue: X planes zb-2..zb+1, mu of zb-1 (tile) and zb (tile + halo),
-  // then the -axis0 face of plane zb.
+  __syncthreads();
   load_x(zb - 2);
   load_x(zb - 1);
   load_x(zb);
@@ -245,8 +349,8 @@ __global__ void __launch_bounds__(TX * TY, DIM == 3 ? 2 : 4)
   compute_mu(zb, false);
   __syncthreads();
   double Jm[S];
-  face(zb - 1, pX, pM, zb, pX, pM, Jm);
-
+  face_between<G::PX, G::PM>(xplane(zb - 1), mplane(zb - 1), pX, pM, xplane(zb), mplane(zb), pX,
+                             pM, P.inv_dx, Jm);
   double vmax = 0.0;
   for (int z = zb; z < ze; ++z) {
     __syncthreads();
@@ -254,49 +358,25 @@ __global__ void __launch_bounds__(TX * TY, DIM == 3 ? 2 : 4)
     __syncthreads();
     compute_mu(z + 1, false);
     __syncthreads();
-    double Jz[S], J[S];
-    face(z, pX, pM, z + 1, pX, pM, Jz);                          // +axis0
-    face(z, pX, pM, z, pX + 1, pM + 1, J);                       // +x
-#pragma unroll
-    for (int c = 0; c < S; ++c) Fx[c * G::FXN + ty * (TX + 1) + tx + 1] = J[c];
-    if (DIM == 3) {
-      face(z, pX, pM, z, pX + G::HX, pM + G::MX, J);             // +y
-#pragma unroll
-      for (int c = 0; c < S; ++c) Fy[c * G::FYN + (ty + 1) * TX + tx] = J[c];
-    }
-    // tile-boundary faces: -x of column 0 (threads 0..TY-1), -y of row 0.
-    if (tid < TY) {
-      const int r = tid;
-      const int bx = (DIM == 3) ? (r + 2) * G::HX + 2 : 2;
-      const int bm = (DIM == 3) ? (r + 1) * G::MX + 1 : 1;
-      face(z, bx - 1, bm - 1, z, bx, bm, J);
-#pragma unroll
-      for (int c = 0; c < S; ++c) Fx[c * G::FXN + r * (TX + 1)] = J[c];
-    }
-    if (DIM == 3 && tid >= 32 && tid < 32 + TX) {
-      const int col = tid - 32;
-      const int bx = 2 * G::HX + col + 2, bm = G::MX + col + 1;
-      face(z, bx - G::HX, bm - G::MX, z, bx, bm, J);
-#pragma unroll
-      for (int c = 0; c < S; ++c) Fy[c * G::FYN + col] = J[c];
-    }
+    double Jz[S];
+    face_between<G::PX, G::PM>(xplane(z), mplane(z), pX, pM, xplane(z + 1), mplane(z + 1), pX,
+                               pM, P.inv_dx, Jz);
+    plane_faces<TX, TY>(xplane(z), mplane(z), Fx, Fy, P.inv_dx, tid);
     __syncthreads();
     if (in_tile) {
       double out[S];
 #pragma unroll
       for (int c = 0; c < S; ++c) {
         double a = Jz[c] - Jm[c];
-        if (DIM == 3) {
-          a = a + Fy[c * G::FYN + (ty + 1) * TX + tx];
-          a = a - Fy[c * G::FYN + ty * TX + tx];
-        }
-        a = a + Fx[c * G::FXN + ty * (TX + 1) + tx + 1];
-        a = a - Fx[c * G::FXN + ty * (TX + 1) + tx];
+        a = a + Fy[c * G::NFY + (ty + 1) * TX + tx];
+        a = a - Fy[c * G::NFY + ty * TX + tx];
+        a = a + Fx[c * G::NFX + ty * (TX + 1) + tx + 1];
+        a = a - Fx[c * G::NFX + ty * (TX + 1) + tx];
         out[c] = a * P.inv_dx;
         const double v = fabs(out[c]);
         if (v > vmax) vmax = v;
       }
-      const int64_t g = ((int64_t)z * P.ny + (y0 + ty)) * P.nx + (x0 + tx);
+      const int64_t g = (int64_t)z * plane + (int64_t)(y0 + ty) * P.nx + (x0 + tx);
       double2 *o = reinterpret_cast<double2 *>(P.dX + 4 * g);
       o[0] = make_double2(out[0], out[1]);
       o[1] = make_double2(out[2], out[3]);
@@ -308,10 +388,18 @@ __global__ void __launch_bounds__(TX * TY, DIM == 3 ? 2 : 4)
   finish_rate(P, vmax, red);
 }
 
+template <int TX, int TY>
+constexpr size_t march3d_smem() {
+  using G = PlaneGeom<TX, TY>;
+  return (3 * S * G::PX + 2 * NP * G::PM + S * G::NFX + S * G::NFY + G::NT / 32) *
+             sizeof(double) +
+         (G::HX + G::HY) * sizeof(int);
+}
+
 // ------------------------------------------------------------------------
 // 1D kernel: a tile of TX points with halos, no marching.
 // ------------------------------------------------------------------------
-template <int TX>
+template <int TX, bool VEC>
 __global__ void __launch_bounds__(TX) k_rate_1d(RateParams P) {
   if (P.st->halt) return;
   constexpr int HX = TX + 4, MX = TX + 2;
@@ -343,36 +431,30 @@ __global__ void __launch_bounds__(TX) k_rate_1d(RateParams P) {
     }
     const double spv = P.sp ? __ldg(P.sp + wrap_any(x0 + pos - 1, n)) : 0.0;
     double mu[S], M[NM];
-    chem_point(P, x, lap, spv, mu, M, &flags);
+    chem_point<VEC>(P, x, lap, spv, mu, M, &flags);
 #pragma unroll
     for (int c = 0; c < S; ++c) Ms[c][pos] = mu[c];
 #pragma unroll
     for (int c = 0; c < NM; ++c) Ms[S + c][pos] = M[c];
   }
   __syncthreads();
-  auto face = [&](int ml, double J[S]) {   // face between muM pos ml and ml+1
-    double Xc[S], Xn[S], Mc[NM], Mn[NM], g[S];
+  // face f lies between mu/M positions f and f+1 (X positions f+1, f+2)
+  for (int f = tx; f < TX + 1; f += TX) {
+    double Xc[S], Xn[S], Mc[NM], Mn[NM], g[S], J[S];
 #pragma unroll
     for (int c = 0; c < S; ++c) {
-      Xc[c] = Xs[c][ml + 1];
-      Xn[c] = Xs[c][ml + 2];
-      g[c] = (Ms[c][ml + 1] - Ms[c][ml]) * P.inv_dx;
+      Xc[c] = Xs[c][f + 1];
+      Xn[c] = Xs[c][f + 2];
+      g[c] = (Ms[c][f + 1] - Ms[c][f]) * P.inv_dx;
     }
 #pragma unroll
     for (int c = 0; c < NM; ++c) {
-      Mc[c] = Ms[S + c][ml];
-      Mn[c] = Ms[S + c][ml + 1];
+      Mc[c] = Ms[S + c][f];
+      Mn[c] = Ms[S + c][f + 1];
     }
     face_flux(Xc, Mc, Xn, Mn, g, J);
-  };
-  double J[S];
-  face(tx + 1, J);
 #pragma unroll
-  for (int c = 0; c < S; ++c) Fx[c][tx + 1] = J[c];
-  if (tx == 0) {
-    face(0, J);
-#pragma unroll
-    for (int c = 0; c < S; ++c) Fx[c][0] = J[c];
+    for (int c = 0; c < S; ++c) Fx[c][f] = J[c];
   }
   __syncthreads();
   double vmax = 0.0;
@@ -498,63 +580,72 @@ struct pf5d_stepper {
   dim3 rate_grid, rate_block;
   size_t rate_smem = 0;
   int zc = 1;
+  bool vec = false;
 };
 
 namespace {
 
-constexpr int kTX3 = 32, kTY3 = 8;   // 3D plane tile
-constexpr int kTX2 = 64;             // 2D row segment
+constexpr int kTX = 32, kTY = 8;     // 2D / 3D plane tile
 constexpr int kTX1 = 128;            // 1D tile
 constexpr int kGraphSteps = 50;      // steps per captured graph
+
+template <typename K>
+pf5d_status allow_smem(K kernel, size_t bytes) {
+  PF5D_CUDA(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes));
+  return PF5D_OK;
+}
 
 pf5d_status configure_rate(pf5d_stepper *h) {
   const int dim = h->d.dim;
   const int nsm = sm_count();
+  const RateParams &P = h->rp;
+  h->vec = (P.T.stride % 2 == 0) && (((uintptr_t)P.T.grid & 15) == 0);
+  pf5d_status st = PF5D_OK;
   if (dim == 1) {
     h->rate_block = dim3(kTX1);
-    h->rate_grid = dim3((unsigned)((h->rp.nx + kTX1 - 1) / kTX1));
+    h->rate_grid = dim3((unsigned)((P.nx + kTX1 - 1) / kTX1));
     h->rate_smem = 0;
     return PF5D_OK;
   }
-  int tiles;
+  h->rate_block = dim3(kTX, kTY);
+  const unsigned gx = (unsigned)((P.nx + kTX - 1) / kTX), gy = (unsigned)((P.ny + kTY - 1) / kTY);
   if (dim == 2) {
-    using G = MarchGeom<2, kTX2, 1>;
-    h->rate_block = dim3(kTX2, 1);
-    tiles = (h->rp.nx + kTX2 - 1) / kTX2;
-    h->rate_smem = G::smem_bytes;
-    PF5D_CUDA(cudaFuncSetAttribute(k_rate_march<2, kTX2, 1>,
-                                   cudaFuncAttributeMaxDynamicSharedMemorySize, (int)G::smem_bytes));
-  } else {
-    using G = MarchGeom<3, kTX3, kTY3>;
-    h->rate_block = dim3(kTX3, kTY3);
-    tiles = ((h->rp.nx + kTX3 - 1) / kTX3) * ((h->rp.ny + kTY3 - 1) / kTY3);
-    h->rate_smem = G::smem_bytes;
-    PF5D_CUDA(cudaFuncSetAttribute(k_rate_march<3, kTX3, kTY3>,
-                                   cudaFuncAttributeMaxDynamicSharedMemorySize, (int)G::smem_bytes));
+    h->rate_smem = tile2d_smem<kTX, kTY>();
+    h->rate_grid = dim3(gx, gy, 1);
+    st = h->vec ? allow_smem(k_rate_tile2d<kTX, kTY, true>, h->rate_smem)
+                : allow_smem(k_rate_tile2d<kTX, kTY, false>, h->rate_smem);
+    return st;
   }
-  // Chunk length along axis 0: aim for ~8 blocks per SM, at least 4 planes.
+  h->rate_smem = march3d_smem<kTX, kTY>();
+  st = h->vec ? allow_smem(k_rate_march3d<kTX, kTY, true>, h->rate_smem)
+              : allow_smem(k_rate_march3d<kTX, kTY, false>, h->rate_smem);
+  if (st != PF5D_OK) return st;
+  // Chunk of axis-0 planes per block: ~8 blocks per SM, at least 4 planes.
+  const int64_t tiles = (int64_t)gx * gy;
   const int64_t target = (int64_t)nsm * 8;
-  int64_t zc = ((int64_t)tiles * h->rp.nz + target - 1) / target;
-  zc = std::max<int64_t>(dim == 2 ? 8 : 4, std::min<int64_t>(zc, 64));
-  zc = std::min<int64_t>(zc, h->rp.nz);
+  int64_t zc = (tiles * P.nz + target - 1) / target;
+  zc = std::max<int64_t>(4, std::min<int64_t>(zc, 64));
+  zc = std::min<int64_t>(zc, P.nz);
   h->zc = (int)zc;
-  const unsigned nzb = (unsigned)((h->rp.nz + zc - 1) / zc);
-  if (dim == 2)
-    h->rate_grid = dim3((unsigned)tiles, 1, nzb);
-  else
-    h->rate_grid = dim3((unsigned)((h->rp.nx + kTX3 - 1) / kTX3),
-                        (unsigned)((h->rp.ny + kTY3 - 1) / kTY3), nzb);
+  h->rate_grid = dim3(gx, gy, (unsigned)((P.nz + zc - 1) / zc));
   return PF5D_OK;
 }
 
 pf5d_status launch_rate(pf5d_stepper *h, cudaStream_t s) {
+  const dim3 g = h->rate_grid, b = h->rate_block;
+  const size_t sm = h->rate_smem;
   switch (h->d.dim) {
-    case 1: k_rate_1d<kTX1><<<h->rate_grid, h->rate_block, 0, s>>>(h->rp); break;
+    case 1:
+      if (h->vec) k_rate_1d<kTX1, true><<<g, b, 0, s>>>(h->rp);
+      else k_rate_1d<kTX1, false><<<g, b, 0, s>>>(h->rp);
+      break;
     case 2:
-      k_rate_march<2, kTX2, 1><<<h->rate_grid, h->rate_block, h->rate_smem, s>>>(h->rp, h->zc);
+      if (h->vec) k_rate_tile2d<kTX, kTY, true><<<g, b, sm, s>>>(h->rp);
+      else k_rate_tile2d<kTX, kTY, false><<<g, b, sm, s>>>(h->rp);
       break;
     default:
-      k_rate_march<3, kTX3, kTY3><<<h->rate_grid, h->rate_block, h->rate_smem, s>>>(h->rp, h->zc);
+      if (h->vec) k_rate_march3d<kTX, kTY, true><<<g, b, sm, s>>>(h->rp, h->zc);
+      else k_rate_march3d<kTX, kTY, false><<<g, b, sm, s>>>(h->rp, h->zc);
   }
   PF5D_LAUNCHED();
   return PF5D_OK;
@@ -652,7 +743,7 @@ pf5d_status pf5d_stepper_create(const pf5d_stepper_desc *desc, double *X, void *
   if (desc->dim == 1) {
     P.nz = 1; P.ny = 1; P.nx = (int)h->shape[0];
   } else if (desc->dim == 2) {
-    P.nz = (int)h->shape[0]; P.ny = 1; P.nx = (int)h->shape[1];
+    P.nz = 1; P.ny = (int)h->shape[0]; P.nx = (int)h->shape[1];
   } else {
     P.nz = (int)h->shape[0]; P.ny = (int)h->shape[1]; P.nx = (int)h->shape[2];
   }

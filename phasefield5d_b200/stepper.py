@@ -39,10 +39,7 @@ class Stepper:
         self.dim = len(self.shape)
         if self.dim not in (1, 2, 3):
             raise ValueError(f"Unsupported system_dim={self.dim}. Choose 1, 2, or 3.")
-        if isinstance(grid, torch.Tensor) and grid.is_cuda:
-            self.grid = grid.to(torch.float64).contiguous()
-        else:
-            self.grid = torch.from_numpy(np.ascontiguousarray(grid, dtype=np.float64)).cuda()
+        self.grid = device_table(grid, torch)
         self.node_coord = torch.from_numpy(np.ascontiguousarray(node_coord,
                                                                 dtype=np.float64)).cuda()
         if isinstance(X, torch.Tensor):
@@ -68,7 +65,7 @@ class Stepper:
                 else ctypes.POINTER(ctypes.c_double)())
         d.grid = self.grid.data_ptr()
         d.table_n = int(self.grid.shape[0])
-        d.nprops = int(self.grid.shape[-1])
+        d.nprops = 9
         d.node_stride = int(self.grid.shape[-1])
         d.resolution = float(resolution)
         d.node_coord = self.node_coord.data_ptr()
@@ -145,6 +142,26 @@ class Stepper:
             self.close()
         except Exception:
             pass
+
+
+NODE_STRIDE = 10
+
+
+def device_table(grid, torch):
+    """Dense (n,n,n,n,9) table as a device tensor padded to 10 doubles per node
+    (80-byte nodes: every node starts on a 16-byte boundary, so the fused
+    kernels read each node as five double2 loads)."""
+    if isinstance(grid, torch.Tensor):
+        g = grid.to(device="cuda", dtype=torch.float64)
+    else:
+        g = torch.from_numpy(np.ascontiguousarray(grid, dtype=np.float64)).cuda()
+    if g.shape[-1] == NODE_STRIDE:
+        return g.contiguous()
+    if g.shape[-1] != 9:
+        raise ValueError(f"table must have 9 props per node (got {g.shape[-1]})")
+    out = torch.zeros((*g.shape[:-1], NODE_STRIDE), dtype=torch.float64, device="cuda")
+    out[..., :9] = g
+    return out
 
 
 def _tensor_from_ptr(ptr, n, torch):
