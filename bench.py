@@ -326,6 +326,7 @@ def run_ours(args, rank, world, local_rank):
                           "achieved_gbs": STEP_BYTES_FP64 * value / world / 1e9,
                           "frac": STEP_BYTES_FP64 * value / world / 1e9 / peak},
         "stage_ms": stage_ms,
+        "rate_variant": {"index": st.variant, "tuned_ms": st.tuned_ms},
         "resident_l2_warm": {"value": world * P / (resident_ms * 1e-3),
                              "ms_per_step": resident_ms,
                              "note": "200 back-to-back steps from 50-step graphs, no flush"},

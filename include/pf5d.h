@@ -192,6 +192,13 @@ double *pf5d_stepper_rate(pf5d_stepper *h);
 #define PF5D_STAGE_BMUL 3        /* B(k) multiply                              */
 #define PF5D_STAGE_FFT_INV 4     /* cuFFT Z2D                                  */
 pf5d_status pf5d_stepper_launch_stage(pf5d_stepper *h, int32_t stage, void *stream);
+/* Autotuner: time every rate-kernel variant (plane tile shape x resident
+ * blocks per SM) on this solve and keep the fastest; the step state is
+ * preserved.  *variant / *best_ms (either may be NULL) report the choice. */
+pf5d_status pf5d_stepper_autotune(pf5d_stepper *h, int32_t *variant, float *best_ms,
+                                  void *stream);
+/* Select a rate-kernel variant explicitly (index from a previous autotune). */
+pf5d_status pf5d_stepper_set_variant(pf5d_stepper *h, int32_t variant);
 /* Re-derive internal state after the caller modified X (e.g. a restart). */
 pf5d_status pf5d_stepper_reset(pf5d_stepper *h, double dt, double time, void *stream);
 pf5d_status pf5d_stepper_destroy(pf5d_stepper *h);

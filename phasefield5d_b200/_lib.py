@@ -83,6 +83,9 @@ _SIGS = {
     "pf5d_stepper_state": (_i32, [_vp, ctypes.POINTER(StepState), _vp]),
     "pf5d_stepper_rate": (_vp, [_vp]),
     "pf5d_stepper_launch_stage": (_i32, [_vp, _i32, _vp]),
+    "pf5d_stepper_autotune": (_i32, [_vp, ctypes.POINTER(_i32), ctypes.POINTER(ctypes.c_float),
+                                     _vp]),
+    "pf5d_stepper_set_variant": (_i32, [_vp, _i32]),
     "pf5d_stepper_reset": (_i32, [_vp, _f64, _f64, _vp]),
     "pf5d_stepper_destroy": (_i32, [_vp]),
 }

@@ -196,8 +196,8 @@ __device__ __forceinline__ void load_plane(const double *__restrict__ X, int64_t
 // Axis 0 of the (n0, n1) field is the tile's y, axis 1 its x.  Laplacian
 // (operators.py:49-60) and divergence (fluxes.py:349) keep the reference's
 // axis order: axis-0 terms first.
-template <int TX, int TY, bool VEC>
-__global__ void __launch_bounds__(TX * TY, 2) k_rate_tile2d(RateParams P) {
+template <int TX, int TY, int MINB, bool VEC>
+__global__ void __launch_bounds__(TX * TY, MINB) k_rate_tile2d(RateParams P) {
   using G = PlaneGeom<TX, TY>;
   if (P.st->halt) return;
   extern __shared__ double sm[];
@@ -278,8 +278,8 @@ constexpr size_t tile2d_smem() {
 // compute the plane's x/y faces (flat loop) and each point's +z face, and
 // form the divergence with the -z face kept in registers from plane z-1.
 // Laplacian order (operators.py:68-76): +z, -z, +y, -y, +x, -x.
-template <int TX, int TY, bool VEC>
-__global__ void __launch_bounds__(TX * TY, 2) k_rate_march3d(RateParams P, int zc) {
+template <int TX, int TY, int MINB, bool VEC>
+__global__ void __launch_bounds__(TX * TY, MINB) k_rate_march3d(RateParams P, int zc) {
   using G = PlaneGeom<TX, TY>;
   if (P.st->halt) return;
   extern __shared__ double sm[];
@@ -581,48 +581,92 @@ struct pf5d_stepper {
   size_t rate_smem = 0;
   int zc = 1;
   bool vec = false;
+  int variant = 0;
 };
 
 namespace {
 
-constexpr int kTX = 32, kTY = 8;     // 2D / 3D plane tile
 constexpr int kTX1 = 128;            // 1D tile
 constexpr int kGraphSteps = 50;      // steps per captured graph
 
-template <typename K>
-pf5d_status allow_smem(K kernel, size_t bytes) {
-  PF5D_CUDA(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes));
-  return PF5D_OK;
+// Rate-kernel variants the autotuner chooses from: plane tile (TX x TY
+// threads) and the minimum resident blocks per SM (which caps registers).
+struct RateVariant {
+  int tx, ty, minb;
+  size_t smem2d, smem3d;
+  void (*set_attrs)(bool vec);
+  void (*launch2d)(bool vec, dim3 g, dim3 b, size_t sm, cudaStream_t s, const RateParams &P);
+  void (*launch3d)(bool vec, dim3 g, dim3 b, size_t sm, cudaStream_t s, const RateParams &P,
+                   int zc);
+};
+
+template <int TX, int TY, int MINB>
+RateVariant make_variant() {
+  RateVariant v;
+  v.tx = TX;
+  v.ty = TY;
+  v.minb = MINB;
+  v.smem2d = tile2d_smem<TX, TY>();
+  v.smem3d = march3d_smem<TX, TY>();
+  v.set_attrs = [](bool vec) {
+    const int s2 = (int)tile2d_smem<TX, TY>(), s3 = (int)march3d_smem<TX, TY>();
+    const auto a = cudaFuncAttributeMaxDynamicSharedMemorySize;
+    if (vec) {
+      cudaFuncSetAttribute(k_rate_tile2d<TX, TY, MINB, true>, a, s2);
+      cudaFuncSetAttribute(k_rate_march3d<TX, TY, MINB, true>, a, s3);
+    } else {
+      cudaFuncSetAttribute(k_rate_tile2d<TX, TY, MINB, false>, a, s2);
+      cudaFuncSetAttribute(k_rate_march3d<TX, TY, MINB, false>, a, s3);
+    }
+  };
+  v.launch2d = [](bool vec, dim3 g, dim3 b, size_t sm, cudaStream_t s, const RateParams &P) {
+    if (vec) k_rate_tile2d<TX, TY, MINB, true><<<g, b, sm, s>>>(P);
+    else k_rate_tile2d<TX, TY, MINB, false><<<g, b, sm, s>>>(P);
+  };
+  v.launch3d = [](bool vec, dim3 g, dim3 b, size_t sm, cudaStream_t s, const RateParams &P,
+                  int zc) {
+    if (vec) k_rate_march3d<TX, TY, MINB, true><<<g, b, sm, s>>>(P, zc);
+    else k_rate_march3d<TX, TY, MINB, false><<<g, b, sm, s>>>(P, zc);
+  };
+  return v;
 }
 
-pf5d_status configure_rate(pf5d_stepper *h) {
+const std::vector<RateVariant> &rate_variants() {
+  static const std::vector<RateVariant> v = {
+      make_variant<32, 8, 2>(), make_variant<32, 8, 3>(), make_variant<32, 4, 4>(),
+      make_variant<16, 8, 4>(), make_variant<64, 4, 2>(), make_variant<32, 4, 6>()};
+  return v;
+}
+
+pf5d_status configure_rate(pf5d_stepper *h, int variant) {
   const int dim = h->d.dim;
   const int nsm = sm_count();
   const RateParams &P = h->rp;
   h->vec = (P.T.stride % 2 == 0) && (((uintptr_t)P.T.grid & 15) == 0);
-  pf5d_status st = PF5D_OK;
   if (dim == 1) {
     h->rate_block = dim3(kTX1);
     h->rate_grid = dim3((unsigned)((P.nx + kTX1 - 1) / kTX1));
     h->rate_smem = 0;
     return PF5D_OK;
   }
-  h->rate_block = dim3(kTX, kTY);
-  const unsigned gx = (unsigned)((P.nx + kTX - 1) / kTX), gy = (unsigned)((P.ny + kTY - 1) / kTY);
+  const auto &vars = rate_variants();
+  PF5D_REQUIRE(variant >= 0 && variant < (int)vars.size(), PF5D_ERR_ARG, "bad variant %d",
+               variant);
+  const RateVariant &v = vars[variant];
+  h->variant = variant;
+  v.set_attrs(h->vec);
+  PF5D_LAUNCHED();
+  h->rate_block = dim3(v.tx, v.ty);
+  const unsigned gx = (unsigned)((P.nx + v.tx - 1) / v.tx), gy = (unsigned)((P.ny + v.ty - 1) / v.ty);
   if (dim == 2) {
-    h->rate_smem = tile2d_smem<kTX, kTY>();
+    h->rate_smem = v.smem2d;
     h->rate_grid = dim3(gx, gy, 1);
-    st = h->vec ? allow_smem(k_rate_tile2d<kTX, kTY, true>, h->rate_smem)
-                : allow_smem(k_rate_tile2d<kTX, kTY, false>, h->rate_smem);
-    return st;
+    return PF5D_OK;
   }
-  h->rate_smem = march3d_smem<kTX, kTY>();
-  st = h->vec ? allow_smem(k_rate_march3d<kTX, kTY, true>, h->rate_smem)
-              : allow_smem(k_rate_march3d<kTX, kTY, false>, h->rate_smem);
-  if (st != PF5D_OK) return st;
-  // Chunk of axis-0 planes per block: ~8 blocks per SM, at least 4 planes.
+  h->rate_smem = v.smem3d;
+  // Chunk of axis-0 planes per block: ~8 resident-block waves, >= 4 planes.
   const int64_t tiles = (int64_t)gx * gy;
-  const int64_t target = (int64_t)nsm * 8;
+  const int64_t target = (int64_t)nsm * v.minb * 4;
   int64_t zc = (tiles * P.nz + target - 1) / target;
   zc = std::max<int64_t>(4, std::min<int64_t>(zc, 64));
   zc = std::min<int64_t>(zc, P.nz);
@@ -640,14 +684,60 @@ pf5d_status launch_rate(pf5d_stepper *h, cudaStream_t s) {
       else k_rate_1d<kTX1, false><<<g, b, 0, s>>>(h->rp);
       break;
     case 2:
-      if (h->vec) k_rate_tile2d<kTX, kTY, true><<<g, b, sm, s>>>(h->rp);
-      else k_rate_tile2d<kTX, kTY, false><<<g, b, sm, s>>>(h->rp);
+      rate_variants()[h->variant].launch2d(h->vec, g, b, sm, s, h->rp);
       break;
     default:
-      if (h->vec) k_rate_march3d<kTX, kTY, true><<<g, b, sm, s>>>(h->rp, h->zc);
-      else k_rate_march3d<kTX, kTY, false><<<g, b, sm, s>>>(h->rp, h->zc);
+      rate_variants()[h->variant].launch3d(h->vec, g, b, sm, s, h->rp, h->zc);
   }
   PF5D_LAUNCHED();
+  return PF5D_OK;
+}
+
+// Time every rate-kernel variant on this solve (events on `s`, a few reps
+// each) and keep the fastest.  The step state is saved and restored, so
+// tuning leaves the solve where it was; any captured graphs are dropped.
+pf5d_status autotune_rate(pf5d_stepper *h, cudaStream_t s, float *best_ms) {
+  if (h->d.dim == 1) {
+    if (best_ms) *best_ms = 0.f;
+    return PF5D_OK;
+  }
+  StepState saved;
+  PF5D_CUDA(cudaMemcpyAsync(&saved, h->st, sizeof(saved), cudaMemcpyDeviceToHost, s));
+  PF5D_CUDA(cudaStreamSynchronize(s));
+  cudaEvent_t e0, e1;
+  PF5D_CUDA(cudaEventCreate(&e0));
+  PF5D_CUDA(cudaEventCreate(&e1));
+  int best = h->variant;
+  float best_t = 1e30f;
+  const int reps = 5;
+  for (int v = 0; v < (int)rate_variants().size(); ++v) {
+    pf5d_status st = configure_rate(h, v);
+    if (st != PF5D_OK) continue;
+    if (launch_rate(h, s) != PF5D_OK) {           // warm-up (e.g. too much smem)
+      cudaGetLastError();
+      continue;
+    }
+    PF5D_CUDA(cudaEventRecord(e0, s));
+    for (int r = 0; r < reps; ++r)
+      if ((st = launch_rate(h, s)) != PF5D_OK) break;
+    PF5D_CUDA(cudaEventRecord(e1, s));
+    PF5D_CUDA(cudaEventSynchronize(e1));
+    float ms = 0.f;
+    PF5D_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+    if (st == PF5D_OK && ms / reps < best_t) {
+      best_t = ms / reps;
+      best = v;
+    }
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  pf5d_status st = configure_rate(h, best);
+  if (st != PF5D_OK) return st;
+  for (auto &kv : h->graphs) cudaGraphExecDestroy(kv.second);
+  h->graphs.clear();
+  PF5D_CUDA(cudaMemcpyAsync(h->st, &saved, sizeof(saved), cudaMemcpyHostToDevice, s));
+  PF5D_CUDA(cudaStreamSynchronize(s));
+  if (best_ms) *best_ms = best_t;
   return PF5D_OK;
 }
 
@@ -782,7 +872,7 @@ pf5d_status pf5d_stepper_create(const pf5d_stepper_desc *desc, double *X, void *
   }
   U.s = desc->elastic ? h->s : nullptr;
   U.oob_interval = desc->oob_interval;
-  if ((st = configure_rate(h)) != PF5D_OK) return fail(st);
+  if ((st = configure_rate(h, 0)) != PF5D_OK) return fail(st);
   if ((st = pf5d_stepper_reset(h, desc->dt0, 0.0, stream)) != PF5D_OK) return fail(st);
   (void)s;
   *out = h;
@@ -843,6 +933,23 @@ pf5d_status pf5d_stepper_state(pf5d_stepper *h, pf5d_step_state *out, void *stre
 }
 
 double *pf5d_stepper_rate(pf5d_stepper *h) { return h ? h->dX : nullptr; }
+
+pf5d_status pf5d_stepper_autotune(pf5d_stepper *h, int32_t *variant, float *best_ms,
+                                  void *stream) {
+  PF5D_REQUIRE(h, PF5D_ERR_ARG, "null stepper");
+  pf5d_status st = autotune_rate(h, as_stream(stream), best_ms);
+  if (variant) *variant = h->variant;
+  return st;
+}
+
+pf5d_status pf5d_stepper_set_variant(pf5d_stepper *h, int32_t variant) {
+  PF5D_REQUIRE(h, PF5D_ERR_ARG, "null stepper");
+  pf5d_status st = configure_rate(h, variant);
+  if (st != PF5D_OK) return st;
+  for (auto &kv : h->graphs) cudaGraphExecDestroy(kv.second);
+  h->graphs.clear();
+  return PF5D_OK;
+}
 
 pf5d_status pf5d_stepper_launch_stage(pf5d_stepper *h, int32_t stage, void *stream) {
   PF5D_REQUIRE(h, PF5D_ERR_ARG, "null stepper");

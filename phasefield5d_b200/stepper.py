@@ -29,7 +29,7 @@ class Stepper:
 
     def __init__(self, *, grid, resolution, node_coord, X, X0, kappa, dx, lvec, bk, ctld, t_cfl,
                  dt, adaptive=True, lower_limit=1e-5, upper_limit=1e-3, max_change_factor=2.0,
-                 oob_interval=100, max_nn_dist=None, stream=None):
+                 oob_interval=100, max_nn_dist=None, stream=None, autotune=True):
         import torch
         self._torch = torch
         self.L = _lib.load()
@@ -84,6 +84,7 @@ class Stepper:
                                               ctypes.byref(h)), "Stepper")
         self.h = h
         self.steps_enqueued = 0
+        self.variant, self.tuned_ms = (self.autotune() if autotune else (0, None))
 
     @classmethod
     def from_problem(cls, prob, **kw):
@@ -123,6 +124,18 @@ class Stepper:
         """dX/dt of the last step as a (*shape, 4) CUDA tensor (a view)."""
         ptr = self.L.pf5d_stepper_rate(self.h)
         return _tensor_from_ptr(ptr, self.n_points * 4, self._torch).view(*self.shape, 4)
+
+    def autotune(self):
+        """Pick the fastest rate-kernel variant for this solve (in-library
+        autotuner); returns (variant index, ms per rate launch)."""
+        v = ctypes.c_int32()
+        ms = ctypes.c_float()
+        _lib.check(self.L.pf5d_stepper_autotune(self.h, ctypes.byref(v), ctypes.byref(ms),
+                                                self._s()), "autotune")
+        return int(v.value), float(ms.value)
+
+    def set_variant(self, variant):
+        _lib.check(self.L.pf5d_stepper_set_variant(self.h, int(variant)), "set_variant")
 
     def launch_stage(self, stage):
         """Diagnostics: enqueue one stage of a step (``_lib.STAGE_*``) alone."""

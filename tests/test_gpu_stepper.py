@@ -210,3 +210,25 @@ def test_out_of_bounds_halts(torch_cuda, inject):
     assert np.array_equal(np.isnan(got), np.isnan(X))
     assert np.array_equal(np.nan_to_num(got), np.nan_to_num(X))
     gpu.close()
+
+
+def test_rate_variants_bitwise_identical(torch_cuda):
+    """Every autotuner variant (tile shape x occupancy) computes each point
+    the same way, so trajectories are bit-identical across variants."""
+    from phasefield5d_b200 import workload as W
+    from phasefield5d_b200.stepper import Stepper
+    for dim, shape in [(2, (40, 70)), (3, (12, 20, 36))]:
+        cfg = W.SolveConfig(system_dim=dim, initial_composition=(0.1, 0.2, 0.2, 0.25),
+                            resolution=0.05, kappa_value=5e-16, mw=4, ppw=16, shape=shape,
+                            adaptive=True, n_k=2000, fluctuation=2e-2)
+        prob = W.build_problem(cfg)
+        ref = None
+        for v in range(6):
+            st = Stepper.from_problem(prob, autotune=False)
+            st.set_variant(v)
+            st.run(7)
+            X = st.X.cpu().numpy()
+            st.close()
+            if ref is None:
+                ref = X
+            assert np.array_equal(X, ref), (dim, v)
