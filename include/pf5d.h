@@ -118,6 +118,18 @@ pf5d_status pf5d_elastic_destroy(pf5d_elastic *h);
  * partials workspace allocated on first use. */
 pf5d_status pf5d_abs_max(const double *a, int64_t n, double *result, void *stream);
 
+/* No counterpart in the reference.  The same reduction as pf5d_abs_max for
+ * callers that cannot allow a library to allocate device memory (a host
+ * whose own pool owns the GPU's memory, or a loop that must not risk the
+ * synchronisation cudaMalloc/cudaFree can cause).  Its scratch is a fixed
+ * 256 KiB __device__ array held by every GPU that loads the library, so the
+ * call allocates nothing; n is limited to 67,108,864 elements (larger n is
+ * rejected with PF5D_ERR_CAPACITY).  The first call on a device looks up
+ * that array's device address (cudaGetSymbolAddress); make that first call
+ * before any stream capture.  Calls share the array: calls whose kernels
+ * overlap on the GPU race. */
+pf5d_status pf5d_abs_max_noalloc(const double *a, int64_t n, double *result, void *stream);
+
 /* clamp_simplex (phasefield5d/solver/operators.py:262-317), in place. */
 pf5d_status pf5d_clamp_simplex(double *X, int64_t npts, int32_t ncomp, void *stream);
 

@@ -74,6 +74,7 @@ _SIGS = {
     "pf5d_elastic_apply": (_i32, [_vp, _vp, _i64, _vp, _vp]),
     "pf5d_elastic_destroy": (_i32, [_vp]),
     "pf5d_abs_max": (_i32, [_vp, _i64, _vp, _vp]),
+    "pf5d_abs_max_noalloc": (_i32, [_vp, _i64, _vp, _vp]),
     "pf5d_clamp_simplex": (_i32, [_vp, _i64, _i32, _vp]),
     "pf5d_update": (_i32, [_vp, _vp, _i64, _f64, _vp]),
     "pf5d_oob_stats": (_i32, [_vp, _i64, _i32, _f64p, _vp]),

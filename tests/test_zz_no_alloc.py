@@ -1,0 +1,67 @@
+"""pf5d_abs_max_noalloc: the max-|a| reduction for callers that cannot let
+the library allocate device memory (their own pool owns the GPU, or the loop
+must never pay for cudaMalloc/cudaFree).  It must give exactly what
+pf5d_abs_max gives -- a maximum is exact, so the tolerance is zero, as in
+the other abs_max tests -- on consecutive calls that share its static
+scratch, and it must refuse inputs larger than that scratch covers.
+
+Kept in its own file, collected last, so a run that stops at the first
+failure has already run every other test.
+"""
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def cuda():
+    import torch
+    if not torch.cuda.is_available():
+        pytest.skip("no CUDA device")
+    from phasefield5d_b200 import _lib
+    return torch, _lib, _lib.load()
+
+
+def _both(cuda, a):
+    torch, _lib, L = cuda
+    res = torch.full((2,), -1.0, dtype=torch.float64, device="cuda")
+    s = _lib.stream_handle()
+    _lib.check(L.pf5d_abs_max(_lib.ptr(a), a.numel(), ctypes_ptr(res, 0), s))
+    _lib.check(L.pf5d_abs_max_noalloc(_lib.ptr(a), a.numel(), ctypes_ptr(res, 1), s))
+    torch.cuda.synchronize()
+    return res.cpu().numpy()
+
+
+def ctypes_ptr(t, i):
+    import ctypes
+    return ctypes.c_void_p(t.data_ptr() + i * t.element_size())
+
+
+def test_noalloc_matches_abs_max_on_two_calls(cuda):
+    torch = cuda[0]
+    rng = np.random.default_rng(42)
+    big = rng.normal(size=3_000_017) * 3.0
+    big[12345] = -97.25                      # the maximum, negative sign
+    big[777] = np.nan                        # ignored by both
+    small = rng.normal(size=10_001)          # second call: smaller input, smaller max
+    for host in (big, small):
+        a = torch.from_numpy(host).cuda()
+        ref, got = _both(cuda, a)
+        assert got == ref
+        assert ref == np.nanmax(np.abs(host))
+
+
+def test_noalloc_empty_and_limit(cuda):
+    torch, _lib, L = cuda
+    a = torch.zeros(0, dtype=torch.float64, device="cuda")
+    ref, got = _both(cuda, a)
+    assert got == ref == 0.0
+    # The size check runs before anything is launched, so a one-element
+    # buffer is enough to see the refusal.
+    one = torch.zeros(1, dtype=torch.float64, device="cuda")
+    res = torch.zeros(1, dtype=torch.float64, device="cuda")
+    too_many = 32768 * 2048 + 1
+    with pytest.raises(RuntimeError, match="at most"):
+        _lib.check(L.pf5d_abs_max_noalloc(_lib.ptr(one), too_many, _lib.ptr(res),
+                                          _lib.stream_handle()))
