@@ -37,6 +37,11 @@ if HERE not in sys.path:
 STEP_BYTES_FP64 = 176
 # Fused rate kernel per grid point: read X (32) and s' (8), write dX/dt (32).
 RATE_BYTES_FP64 = 72
+# FP32-compensated form: X - X0 as FP32 hi+lo read+written (64), dX/dt
+# FP32 written+read (32), the FP32 misfit scalar through the FFT pair (24).
+STEP_BYTES_FP32C = 120
+# Its rate kernel: read D hi (16) and s' (4), write dX/dt (16).
+RATE_BYTES_FP32C = 36
 FALLBACK_HBM_GBS = 6650.0
 L2_FLUSH_BYTES = 256 << 20
 
@@ -56,6 +61,10 @@ def parse():
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--workload", choices=sorted(WORKLOADS), default="2d")
+    ap.add_argument("--precision", choices=["fp64", "fp32c"], default="fp64",
+                    help="plain FP64 (bit-faithful) or FP32-compensated form")
+    ap.add_argument("--accuracy-steps", type=int, default=2000,
+                    help="steps of the FP32c-vs-FP64 accuracy report")
     ap.add_argument("--cpu-steps", type=int, default=3, help="steps in the CPU-baseline sample")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     return ap.parse_args()
@@ -210,8 +219,9 @@ def run_ours(args, rank, world, local_rank):
             dist.barrier()
         torch.cuda.synchronize()
 
+    fp32c = args.precision == "fp32c"
     # ---- device-resident steps, L2 flushed between timed steps -------------
-    st = Stepper.from_problem(prob)
+    st = Stepper.from_problem(prob, precision=args.precision)
     st.advance(1)                       # captures the one-step graph
     for _ in range(args.warmup):
         flush.zero_()
@@ -244,7 +254,7 @@ def run_ours(args, rank, world, local_rank):
     resident_ms = w0.elapsed_time(w1) / 200
 
     # ---- dominant kernel (fused rate) alone, L2 flushed, same stream -------
-    probe = Stepper.from_problem(prob)
+    probe = Stepper.from_problem(prob, precision=args.precision)
     stage_ms = {}
     stages = [("rate", _lib.STAGE_RATE), ("update", _lib.STAGE_UPDATE)]
     if prob.lvec is not None:
@@ -267,21 +277,29 @@ def run_ours(args, rank, world, local_rank):
 
     # ---- end to end through the C ABI with host buffers --------------------
     host = torch.from_numpy(prob.X_init.copy()).pin_memory()
-    e2e_st = Stepper.from_problem(prob)
+    e2e_st = Stepper.from_problem(prob, precision=args.precision)
     xdev = e2e_st.X
-    for _ in range(max(args.warmup, 1)):
+
+    def e2e_step():
         xdev.copy_(host, non_blocking=True)
+        if fp32c:
+            e2e_st.reset(e2e_st.state_dt, e2e_st.state_time)   # re-seed hi/lo from X
         e2e_st.advance(1)
-        host.copy_(xdev, non_blocking=True)
+        if fp32c:
+            host.copy_(e2e_st.field(), non_blocking=True)
+        else:
+            host.copy_(xdev, non_blocking=True)
+
+    e2e_st.state_dt, e2e_st.state_time = prob.dt0, 0.0
+    for _ in range(max(args.warmup, 1)):
+        e2e_step()
     torch.cuda.synchronize()
     e2e_ev = []
     for _ in range(args.steps):
         flush.zero_()
         a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         a.record(stream)
-        xdev.copy_(host, non_blocking=True)
-        e2e_st.advance(1)
-        host.copy_(xdev, non_blocking=True)
+        e2e_step()
         b.record(stream)
         e2e_ev.append((a, b))
     torch.cuda.synchronize()
@@ -298,7 +316,9 @@ def run_ours(args, rank, world, local_rank):
 
     value = world * P * args.steps / (total_ms * 1e-3)
     peak, peak_kind = measured_peak()
-    rate_bytes = RATE_BYTES_FP64 * P if prob.lvec is not None else (RATE_BYTES_FP64 - 8) * P
+    per_rate = RATE_BYTES_FP32C if fp32c else RATE_BYTES_FP64
+    per_step = STEP_BYTES_FP32C if fp32c else STEP_BYTES_FP64
+    rate_bytes = per_rate * P if prob.lvec is not None else (per_rate - (4 if fp32c else 8)) * P
     achieved = rate_bytes / (stage_ms["rate"] * 1e-3) / 1e9
     cpu = None
     if not args.no_cpu_baseline:
@@ -311,8 +331,10 @@ def run_ours(args, rank, world, local_rank):
         "metric": "grid-point steps/s", "value": value, "unit": "grid-point steps/s",
         "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": total_ms / args.steps, "higher_is_better": True, "scaling": "weak",
-        "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "vs_baseline": None, "dtype": "f32+f64 (compensated)" if fp32c else "f64",
+        "data": "synthetic",
         "config": {"workload": WORKLOADS[args.workload][0], "shape": list(prob.shape),
+                   "precision": args.precision,
                    "table_nodes_per_axis": int(prob.grid.shape[0]), "omega_seed": prob.omega_seed,
                    "l2": "flushed (256 MiB write) between timed steps",
                    "parallelism": f"replicas x{world}" if world > 1 else "single solve"},
@@ -322,9 +344,9 @@ def run_ours(args, rank, world, local_rank):
                      "frac": achieved / peak, "traffic": committed_traffic("rate", args.workload),
                      "algorithmic_bytes_per_launch": rate_bytes,
                      "ms_per_launch": stage_ms["rate"]},
-        "step_roofline": {"bytes_per_grid_point_step": STEP_BYTES_FP64,
-                          "achieved_gbs": STEP_BYTES_FP64 * value / world / 1e9,
-                          "frac": STEP_BYTES_FP64 * value / world / 1e9 / peak},
+        "step_roofline": {"bytes_per_grid_point_step": per_step,
+                          "achieved_gbs": per_step * value / world / 1e9,
+                          "frac": per_step * value / world / 1e9 / peak},
         "stage_ms": stage_ms,
         "rate_variant": {"index": st.variant, "tuned_ms": st.tuned_ms},
         "resident_l2_warm": {"value": world * P / (resident_ms * 1e-3),
@@ -339,6 +361,9 @@ def run_ours(args, rank, world, local_rank):
         "gpu_launches": args.steps * (3 if prob.lvec is not None else 2),
         "state_after": {"step": state["step"], "dt": state["dt"], "time": state["time"]},
     }
+    if fp32c and args.accuracy_steps > 0:
+        from phasefield5d_b200.precision import compare_forms
+        line["accuracy_vs_fp64"] = compare_forms(prob, args.accuracy_steps)
     print(json.dumps(line), flush=True)
     st.close()
 

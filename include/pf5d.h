@@ -175,7 +175,20 @@ typedef struct {
   int32_t adaptive;            /* 0: fixed dt = dt0                           */
   double dt0;                  /* initial dt                                  */
   int32_t oob_interval;        /* 100 in the reference                        */
+  int32_t precision;           /* PF5D_PRECISION_FP64 or _FP32C                */
+  const float *grid32;         /* FP32C: device table, node_stride32 floats per
+                                  node: mu - mu0 (4), M (5), pad               */
+  int32_t node_stride32;       /* 12                                          */
+  double mu0[4];               /* FP32C: mu at X0 subtracted from the table   */
 } pf5d_stepper_desc;
+
+/* Precision forms of the stepper.  FP64: bit-faithful to the reference
+ * (apart from FFT rounding); X is advanced in place.  FP32C: D = X - X0 as
+ * an FP32 hi/lo pair with a compensated update, FP32 stencils, table and
+ * FFT, FP64 closure / sums / dt / mass; X only seeds the state (read it back
+ * with pf5d_stepper_field). */
+#define PF5D_PRECISION_FP64 0
+#define PF5D_PRECISION_FP32C 1
 
 typedef struct {
   double dt, time, xdotmax;
@@ -193,8 +206,14 @@ pf5d_status pf5d_stepper_create(const pf5d_stepper_desc *desc, double *X, void *
 pf5d_status pf5d_stepper_advance(pf5d_stepper *h, int64_t nsteps, void *stream);
 /* Synchronise `stream` and copy the device step state to *out. */
 pf5d_status pf5d_stepper_state(pf5d_stepper *h, pf5d_step_state *out, void *stream);
-/* Device pointer to the last dX/dt buffer ((*shape, 4) float64). */
+/* Device pointer to the last dX/dt buffer ((*shape, 4); float64 for FP64,
+ * float32 for FP32C). */
 double *pf5d_stepper_rate(pf5d_stepper *h);
+/* Write the current field X ((*shape, 4) float64, device) to X_out. */
+pf5d_status pf5d_stepper_field(pf5d_stepper *h, double *X_out, void *stream);
+/* FP64 mean composition per component (host mean_out[4]); synchronises.
+ * The mass-drift report is its change over a run. */
+pf5d_status pf5d_stepper_mass(pf5d_stepper *h, double *mean_out, void *stream);
 /* Diagnostics: launch one stage of a step by itself on `stream`
  * (PF5D_STAGE_*), so each kernel can be timed with events.  It changes the
  * stepper's state exactly as that stage does inside a step. */

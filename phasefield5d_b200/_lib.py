@@ -31,6 +31,7 @@ FLAG_NN_USED = 0x20
 FLAG_HALTED = 0x40
 
 STAGE_RATE, STAGE_UPDATE, STAGE_FFT_FWD, STAGE_BMUL, STAGE_FFT_INV = 0, 1, 2, 3, 4
+PRECISION_FP64, PRECISION_FP32C = 0, 1
 
 _vp = ctypes.c_void_p
 _i32 = ctypes.c_int32
@@ -49,7 +50,8 @@ class StepperDesc(ctypes.Structure):
         ("resolution", _f64), ("node_coord", _vp), ("max_nn_dist", _f64),
         ("ctld", _f64), ("t_cfl", _f64), ("lower_limit", _f64), ("upper_limit", _f64),
         ("max_change_factor", _f64), ("adaptive", _i32), ("dt0", _f64),
-        ("oob_interval", _i32),
+        ("oob_interval", _i32), ("precision", _i32), ("grid32", _vp), ("node_stride32", _i32),
+        ("mu0", _f64 * 4),
     ]
 
 
@@ -83,6 +85,8 @@ _SIGS = {
     "pf5d_stepper_advance": (_i32, [_vp, _i64, _vp]),
     "pf5d_stepper_state": (_i32, [_vp, ctypes.POINTER(StepState), _vp]),
     "pf5d_stepper_rate": (_vp, [_vp]),
+    "pf5d_stepper_field": (_i32, [_vp, _vp, _vp]),
+    "pf5d_stepper_mass": (_i32, [_vp, _f64p, _vp]),
     "pf5d_stepper_launch_stage": (_i32, [_vp, _i32, _vp]),
     "pf5d_stepper_autotune": (_i32, [_vp, ctypes.POINTER(_i32), ctypes.POINTER(ctypes.c_float),
                                      _vp]),

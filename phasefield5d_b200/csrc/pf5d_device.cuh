@@ -125,14 +125,22 @@ struct NearestNode {
   unsigned flags;      // PF5D_FLAG_NN_*
 };
 
-static __device__ __noinline__ NearestNode nearest_node(const Table T, double x0, double x1,
-                                                        double x2, double x3) {
+// The search needs only the node coordinates and a presence probe (the
+// table's first prop is NaN at absent nodes), so it serves FP64 and FP32
+// tables alike: `grid` points at the first prop of node 0, `stride` is in
+// elements of type E.
+template <typename E>
+static __device__ __noinline__ NearestNode nearest_node_g(const E *grid, int stride,
+                                                          const double *coord, int n_axis,
+                                                          double inv_step, double exact_d2,
+                                                          double max_nn_dist, double x0,
+                                                          double x1, double x2, double x3) {
   const double x[S] = {x0, x1, x2, x3};
-  const int N = T.n - 1;
+  const int N = n_axis - 1;
   int lo[S], hi[S];
 #pragma unroll
   for (int d = 0; d < S; ++d) {
-    double u = x[d] * T.inv_step;
+    double u = x[d] * inv_step;
     if (!(u > -4.0)) u = -4.0;             // also maps NaN
     if (!(u < (double)N + 4.0)) u = (double)N + 4.0;
     const int f = (int)floor(u);
@@ -141,22 +149,22 @@ static __device__ __noinline__ NearestNode nearest_node(const Table T, double x0
   }
   double best = __longlong_as_double(0x7ff0000000000000LL);   // +inf
   int64_t best_node = -1;
-  const int64_t n = T.n;
+  const int64_t n = n_axis;
   for (int k0 = lo[0]; k0 <= hi[0]; ++k0) {
-    const double d0 = x[0] - T.coord[k0];
+    const double d0 = x[0] - coord[k0];
     const double e0 = d0 * d0;
     for (int k1 = lo[1]; k1 <= hi[1]; ++k1) {
-      const double d1 = x[1] - T.coord[k1];
+      const double d1 = x[1] - coord[k1];
       const double e1 = e0 + d1 * d1;
       for (int k2 = lo[2]; k2 <= hi[2]; ++k2) {
-        const double d2 = x[2] - T.coord[k2];
+        const double d2 = x[2] - coord[k2];
         const double e2 = e1 + d2 * d2;
         for (int k3 = lo[3]; k3 <= hi[3]; ++k3) {
-          const double d3 = x[3] - T.coord[k3];
+          const double d3 = x[3] - coord[k3];
           const double e3 = e2 + d3 * d3;
           if (e3 < best) {
             const int64_t node = ((k0 * n + k1) * n + k2) * n + k3;
-            const double probe = __ldg(T.grid + node * T.stride);
+            const E probe = __ldg(grid + node * stride);
             if (probe == probe) {            // present (not NaN)
               best = e3;
               best_node = node;
@@ -167,10 +175,16 @@ static __device__ __noinline__ NearestNode nearest_node(const Table T, double x0
     }
   }
   NearestNode r{best_node, PF5D_FLAG_NN_USED};
-  if (best_node < 0 || !(best < T.exact_d2)) r.flags |= PF5D_FLAG_NN_TRUNCATED;
-  if (best_node >= 0 && T.max_nn_dist > 0.0 && sqrt(best) > T.max_nn_dist)
+  if (best_node < 0 || !(best < exact_d2)) r.flags |= PF5D_FLAG_NN_TRUNCATED;
+  if (best_node >= 0 && max_nn_dist > 0.0 && sqrt(best) > max_nn_dist)
     r.flags |= PF5D_FLAG_NN_FAR;
   return r;
+}
+
+__device__ __forceinline__ NearestNode nearest_node(const Table &T, double x0, double x1,
+                                                    double x2, double x3) {
+  return nearest_node_g<double>(T.grid, T.stride, T.coord, T.n, T.inv_step, T.exact_d2,
+                                T.max_nn_dist, x0, x1, x2, x3);
 }
 
 // Interpolation with fallback for one point; returns true on the linear branch.

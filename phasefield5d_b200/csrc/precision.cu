@@ -1,0 +1,1138 @@
+// precision.cu -- FP32-compensated form of the step loop (the "precision
+// form").  Same dataflow and tiling as the FP64 stepper (stepper.cu):
+//   cuFFT R2C of the misfit -> B(k)/N multiply -> cuFFT C2R -> fused rate
+//   kernel (FP32 interpolation, Laplacian, mu, one flux per face,
+//   divergence, max|dX/dt| and the FP64 dt controller in the last block)
+//   -> compensated update + clamp + next misfit + out-of-bounds test,
+// replayed from CUDA graphs.
+//
+// Numerics:
+//   * the field is D = X - X0 as an FP32 pair (hi, lo); the update adds
+//     dt*dX/dt with TwoSum and renormalises, so rounding does not
+//     accumulate over thousands of steps;
+//   * the table stores mu - mu(X0) (and M) in FP32, so mu gradients are
+//     differences of small numbers;
+//   * cell fractions come from a host FP64 split of X0/res into integer and
+//     fraction plus the FP32 deviation D/res;
+//   * FP64: closure X_Fe = 1 - sum X (face flux), linear-region and simplex
+//     sums, dt controller, mass/mean reductions.  The k = 0 elastic mode is
+//     exactly zero because B(0) = 0.
+// Compiled with FMA contraction allowed; the TwoSum update uses explicit
+// round-to-nearest intrinsics so it is never contracted.
+#include <algorithm>
+#include <cstring>
+#include <map>
+#include <vector>
+
+#include <cufft.h>
+
+#include "pf5d_device.cuh"
+#include "pf5d_fp32c.h"
+#include "pf5d_host.h"
+#include "pf5d_tiles.cuh"
+
+namespace pf5d {
+
+struct StepState32 {
+  double dt;
+  double time;
+  double xdotmax;
+  double xacc;
+  unsigned blocks_done;
+  unsigned flags;
+  unsigned halt;
+  unsigned pad;
+  long long step;
+};
+
+constexpr int kStride32 = 12;   // floats per FP32 table node (9 props + 3 pad = 48 bytes)
+
+struct Table32 {
+  const float *grid;
+  const double *coord;
+  int n;
+  int stride;
+  double inv_step, threshold, exact_d2, max_nn_dist;
+  float inv_step_f;
+  int ib[S];          // floor(X0_d / res)
+  float fb[S];        // X0_d / res - floor(X0_d / res)
+  double x0[S];
+  double sum_x0;
+};
+
+struct Rate32 {
+  int nz, ny, nx;
+  const float4 *D;     // hi part of X - X0
+  const float *sp;     // s' scaled by 1/N, or nullptr
+  float4 *dX;
+  Table32 T;
+  float kappa[S], lvec[S], x0f[S];
+  double c_fe;         // 1 - sum X0
+  float inv_dx, inv_dx2;
+  double ctld, t_cfl, lower, upper, factor;
+  int adaptive;
+  StepState32 *st;
+};
+
+// ------------------------------------------------------------------------
+// Device numerics
+// ------------------------------------------------------------------------
+
+__device__ __forceinline__ void interp32(const Rate32 &P, const float d[S], float out[NP],
+                                         unsigned *flags) {
+  const Table32 &T = P.T;
+  const double sd = (((double)d[0] + (double)d[1]) + (double)d[2]) + (double)d[3];
+  if (T.sum_x0 + sd <= T.threshold) {
+    int ii[S];
+    float tt[S];
+#pragma unroll
+    for (int a = 0; a < S; ++a) {
+      const float v = fmaf(d[a], T.inv_step_f, T.fb[a]);
+      const float k = floorf(v);
+      int i = T.ib[a] + (int)k;
+      float t = v - k;
+      if (i < 0) {
+        i = 0;
+        t = 0.f;
+      } else if (i > T.n - 2) {
+        i = T.n - 2;
+        t = 1.f;
+      }
+      ii[a] = i;
+      tt[a] = t;
+    }
+    const float q0 = 1.f - tt[0], q1 = 1.f - tt[1], q2 = 1.f - tt[2], q3 = 1.f - tt[3];
+    const int64_t s3 = T.stride, s2 = (int64_t)T.n * s3, s1 = (int64_t)T.n * s2,
+                  s0 = (int64_t)T.n * s1;
+    const float *base = T.grid + ii[0] * s0 + ii[1] * s1 + ii[2] * s2 + ii[3] * s3;
+#pragma unroll
+    for (int c = 0; c < 16; ++c) {
+      const int b0 = (c >> 3) & 1, b1 = (c >> 2) & 1, b2 = (c >> 1) & 1, b3 = c & 1;
+      const float w = (b0 ? tt[0] : q0) * (b1 ? tt[1] : q1) * (b2 ? tt[2] : q2) * (b3 ? tt[3] : q3);
+      const float4 *node = reinterpret_cast<const float4 *>(base + b0 * s0 + b1 * s1 + b2 * s2 +
+                                                             b3 * s3);
+      const float4 a = __ldg(node), b = __ldg(node + 1), e = __ldg(node + 2);
+      const float v[NP] = {a.x, a.y, a.z, a.w, b.x, b.y, b.z, b.w, e.x};
+#pragma unroll
+      for (int p = 0; p < NP; ++p) out[p] = (c == 0) ? w * v[p] : fmaf(w, v[p], out[p]);
+    }
+    return;
+  }
+  const NearestNode r = nearest_node_g<float>(T.grid, T.stride, T.coord, T.n, T.inv_step,
+                                              T.exact_d2, T.max_nn_dist, T.x0[0] + (double)d[0],
+                                              T.x0[1] + (double)d[1], T.x0[2] + (double)d[2],
+                                              T.x0[3] + (double)d[3]);
+  *flags |= r.flags;
+  const float *row = T.grid + (r.node < 0 ? 0 : r.node) * T.stride;
+#pragma unroll
+  for (int p = 0; p < NP; ++p) out[p] = r.node < 0 ? __int_as_float(0x7fc00000) : __ldg(row + p);
+}
+
+// mu (relative to mu(X0)) and M at one point.
+__device__ __forceinline__ void chem32(const Rate32 &P, const float d[S], const float lap[S],
+                                       float spv, float mu[S], float M[NM], unsigned *flags) {
+  float v[NP];
+  interp32(P, d, v, flags);
+#pragma unroll
+  for (int c = 0; c < S; ++c) {
+    float m = fmaf(-lap[c], P.kappa[c], v[c]);
+    if (P.sp) m = fmaf(spv, P.lvec[c], m);
+    mu[c] = m;
+  }
+#pragma unroll
+  for (int c = 0; c < NM; ++c) M[c] = v[S + c];
+}
+
+// Face flux (phasefield5d/solver/fluxes.py:128-160) in FP32 with the FP64
+// closure X_Fe = (1 - sum X0) - sum Dmid.
+__device__ __forceinline__ void face_flux32(const Rate32 &P, const float Dc[S], const float Mc[NM],
+                                            const float Dn[S], const float Mn[NM],
+                                            const float g[S], float J[S]) {
+  float dm[S], xm[S], mm[NM], dk[S];
+#pragma unroll
+  for (int a = 0; a < S; ++a) {
+    dm[a] = 0.5f * (Dc[a] + Dn[a]);
+    xm[a] = P.x0f[a] + dm[a];
+  }
+#pragma unroll
+  for (int a = 0; a < NM; ++a) mm[a] = 0.5f * (Mc[a] + Mn[a]);
+  const double x_fe = P.c_fe - (((double)dm[0] + (double)dm[1]) + (double)dm[2] + (double)dm[3]);
+  const float w_fe = (float)x_fe * mm[0];
+  float dot = 0.f;
+#pragma unroll
+  for (int b = 0; b < S; ++b) dot = fmaf(xm[b], g[b], dot);
+#pragma unroll
+  for (int k = 0; k < S; ++k) dk[k] = g[k] - dot;
+  float swk = 0.f;
+#pragma unroll
+  for (int k = 0; k < S; ++k) swk = fmaf(xm[k] * mm[1 + k], dk[k], swk);
+#pragma unroll
+  for (int a = 0; a < S; ++a) J[a] = w_fe * xm[a] * dot + xm[a] * mm[1 + a] * dk[a] - xm[a] * swk;
+}
+
+__device__ __forceinline__ void finish_rate32(const Rate32 &P, float m32, double *red) {
+  double m = (double)m32;
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
+  const int tid = threadIdx.y * blockDim.x + threadIdx.x;
+  const int nw = (blockDim.x * blockDim.y + 31) >> 5;
+  __syncthreads();
+  if ((tid & 31) == 0) red[tid >> 5] = m;
+  __syncthreads();
+  if (tid == 0) {
+    for (int w = 1; w < nw; ++w) m = fmax(m, red[w]);
+    StepState32 *st = P.st;
+    atomic_max_nonneg(&st->xacc, m);
+    __threadfence();
+    const unsigned total = gridDim.x * gridDim.y * gridDim.z;
+    if (atomicAdd(&st->blocks_done, 1u) == total - 1) {
+      __threadfence();
+      const double xmax = __longlong_as_double(
+          (long long)atomicAdd(reinterpret_cast<unsigned long long *>(&st->xacc), 0ULL));
+      double dt = st->dt;
+      if (P.adaptive) dt = adaptive_dt(dt, xmax, P.ctld, P.t_cfl, P.lower, P.upper, P.factor);
+      st->dt = dt;
+      st->time = st->time + dt;
+      st->xdotmax = xmax;
+      st->step = st->step + 1;
+      st->xacc = 0.0;
+      st->blocks_done = 0;
+    }
+  }
+}
+
+template <int PX, int PM>
+__device__ __forceinline__ void face32_between(const Rate32 &P, const float *XL, const float *ML,
+                                               int pl, int ql, const float *XH, const float *MH,
+                                               int ph, int qh, float J[S]) {
+  float Dc[S], Dn[S], Mc[NM], Mn[NM], g[S];
+#pragma unroll
+  for (int c = 0; c < S; ++c) {
+    Dc[c] = XL[c * PX + pl];
+    Dn[c] = XH[c * PX + ph];
+    g[c] = (MH[c * PM + qh] - ML[c * PM + ql]) * P.inv_dx;
+  }
+#pragma unroll
+  for (int c = 0; c < NM; ++c) {
+    Mc[c] = ML[(S + c) * PM + ql];
+    Mn[c] = MH[(S + c) * PM + qh];
+  }
+  face_flux32(P, Dc, Mc, Dn, Mn, g, J);
+}
+
+template <int TX, int TY>
+__device__ __forceinline__ void plane_faces32(const Rate32 &P, const float *Xp, const float *Mp,
+                                              float *Fx, float *Fy, int tid) {
+  using G = PlaneGeom<TX, TY>;
+  for (int f = tid; f < G::NFX + G::NFY; f += G::NT) {
+    float J[S];
+    if (f < G::NFX) {
+      const int fy = f / (TX + 1), fx = f - fy * (TX + 1);
+      const int pl = (fy + 2) * G::HX + (fx + 1), ql = (fy + 1) * G::MX + fx;
+      face32_between<G::PX, G::PM>(P, Xp, Mp, pl, ql, Xp, Mp, pl + 1, ql + 1, J);
+#pragma unroll
+      for (int c = 0; c < S; ++c) Fx[c * G::NFX + f] = J[c];
+    } else {
+      const int f2 = f - G::NFX;
+      const int fy = f2 / TX, fx = f2 - fy * TX;
+      const int pl = (fy + 1) * G::HX + (fx + 2), ql = fy * G::MX + (fx + 1);
+      face32_between<G::PX, G::PM>(P, Xp, Mp, pl, ql, Xp, Mp, pl + G::HX, ql + G::MX, J);
+#pragma unroll
+      for (int c = 0; c < S; ++c) Fy[c * G::NFY + f2] = J[c];
+    }
+  }
+}
+
+template <int TX, int TY>
+__device__ __forceinline__ void load_plane32(const float4 *__restrict__ D, int64_t plane_off,
+                                             const int *wx, const int *wy, int nx, float *dst,
+                                             int tid) {
+  using G = PlaneGeom<TX, TY>;
+  for (int pos = tid; pos < G::PX; pos += G::NT) {
+    const int hy = pos / G::HX, hx = pos - hy * G::HX;
+    const float4 v = __ldg(D + plane_off + (int64_t)wy[hy] * nx + wx[hx]);
+    dst[0 * G::PX + pos] = v.x;
+    dst[1 * G::PX + pos] = v.y;
+    dst[2 * G::PX + pos] = v.z;
+    dst[3 * G::PX + pos] = v.w;
+  }
+}
+
+__device__ __forceinline__ void store_rate(float4 *dX, int64_t g, const float out[S], float &vmax) {
+#pragma unroll
+  for (int c = 0; c < S; ++c) vmax = fmaxf(vmax, fabsf(out[c]));
+  dX[g] = make_float4(out[0], out[1], out[2], out[3]);
+}
+
+// ------------------------------------------------------------------------
+// Rate kernels (same tiling as the FP64 kernels)
+// ------------------------------------------------------------------------
+template <int TX, int TY, int MINB>
+__global__ void __launch_bounds__(TX * TY, MINB) k32_rate_tile2d(Rate32 P) {
+  using G = PlaneGeom<TX, TY>;
+  if (P.st->halt) return;
+  extern __shared__ double sm64[];
+  double *red = sm64;                                    // [NT/32]
+  float *Xs = reinterpret_cast<float *>(red + G::NT / 32);   // [S][PX]
+  float *Ms = Xs + S * G::PX;                            // [NP][PM]
+  float *Fx = Ms + NP * G::PM;                           // [S][NFX]
+  float *Fy = Fx + S * G::NFX;                           // [S][NFY]
+  int *wx = reinterpret_cast<int *>(Fy + S * G::NFY);
+  int *wy = wx + G::HX;
+  const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * TX + tx;
+  const int x0 = blockIdx.x * TX, y0 = blockIdx.y * TY;
+  unsigned flags = 0;
+  for (int i = tid; i < G::HX + G::HY; i += G::NT) {
+    if (i < G::HX) wx[i] = wrap_any(x0 + i - 2, P.nx);
+    else wy[i - G::HX] = wrap_any(y0 + (i - G::HX) - 2, P.ny);
+  }
+  __syncthreads();
+  load_plane32<TX, TY>(P.D, 0, wx, wy, P.nx, Xs, tid);
+  __syncthreads();
+  for (int pos = tid; pos < G::PM; pos += G::NT) {
+    const int my = pos / G::MX, mx = pos - my * G::MX;
+    if ((mx == 0 || mx == G::MX - 1) && (my == 0 || my == G::MY - 1)) continue;
+    const int px = (my + 1) * G::HX + (mx + 1);
+    float d[S], lap[S];
+#pragma unroll
+    for (int c = 0; c < S; ++c) {
+      const float *q = Xs + c * G::PX;
+      d[c] = q[px];
+      lap[c] = (q[px + G::HX] + q[px - G::HX] + q[px + 1] + q[px - 1] - 4.f * d[c]) * P.inv_dx2;
+    }
+    const float spv = P.sp ? __ldg(P.sp + (int64_t)wy[my + 1] * P.nx + wx[mx + 1]) : 0.f;
+    float mu[S], M[NM];
+    chem32(P, d, lap, spv, mu, M, &flags);
+#pragma unroll
+    for (int c = 0; c < S; ++c) Ms[c * G::PM + pos] = mu[c];
+#pragma unroll
+    for (int c = 0; c < NM; ++c) Ms[(S + c) * G::PM + pos] = M[c];
+  }
+  __syncthreads();
+  plane_faces32<TX, TY>(P, Xs, Ms, Fx, Fy, tid);
+  __syncthreads();
+  float vmax = 0.f;
+  if (x0 + tx < P.nx && y0 + ty < P.ny) {
+    float out[S];
+#pragma unroll
+    for (int c = 0; c < S; ++c) {
+      const float a = (Fy[c * G::NFY + (ty + 1) * TX + tx] - Fy[c * G::NFY + ty * TX + tx]) +
+                      (Fx[c * G::NFX + ty * (TX + 1) + tx + 1] - Fx[c * G::NFX + ty * (TX + 1) + tx]);
+      out[c] = a * P.inv_dx;
+    }
+    store_rate(P.dX, (int64_t)(y0 + ty) * P.nx + (x0 + tx), out, vmax);
+  }
+  if (flags) atomicOr(&P.st->flags, flags);
+  finish_rate32(P, vmax, red);
+}
+
+template <int TX, int TY>
+constexpr size_t tile2d32_smem() {
+  using G = PlaneGeom<TX, TY>;
+  return (G::NT / 32) * sizeof(double) +
+         (S * G::PX + NP * G::PM + S * G::NFX + S * G::NFY) * sizeof(float) +
+         (G::HX + G::HY) * sizeof(int);
+}
+
+template <int TX, int TY, int MINB>
+__global__ void __launch_bounds__(TX * TY, MINB) k32_rate_march3d(Rate32 P, int zc) {
+  using G = PlaneGeom<TX, TY>;
+  if (P.st->halt) return;
+  extern __shared__ double sm64[];
+  double *red = sm64;
+  float *Xs = reinterpret_cast<float *>(red + G::NT / 32);   // [3][S][PX]
+  float *Ms = Xs + 3 * S * G::PX;                        // [2][NP][PM]
+  float *Fx = Ms + 2 * NP * G::PM;
+  float *Fy = Fx + S * G::NFX;
+  int *wx = reinterpret_cast<int *>(Fy + S * G::NFY);
+  int *wy = wx + G::HX;
+  const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * TX + tx;
+  const int x0 = blockIdx.x * TX, y0 = blockIdx.y * TY;
+  const int zb = blockIdx.z * zc;
+  const int ze = min(zb + zc, P.nz);
+  const int64_t plane = (int64_t)P.ny * P.nx;
+  unsigned flags = 0;
+  for (int i = tid; i < G::HX + G::HY; i += G::NT) {
+    if (i < G::HX) wx[i] = wrap_any(x0 + i - 2, P.nx);
+    else wy[i - G::HX] = wrap_any(y0 + (i - G::HX) - 2, P.ny);
+  }
+  auto xplane = [&](int z) { return Xs + ((z - zb + 3) % 3) * S * G::PX; };
+  auto mplane = [&](int z) { return Ms + ((z - zb + 2) & 1) * NP * G::PM; };
+  auto load_x = [&](int z) {
+    load_plane32<TX, TY>(P.D, (int64_t)wrap_any(z, P.nz) * plane, wx, wy, P.nx, xplane(z), tid);
+  };
+  auto compute_mu = [&](int z, bool interior_only) {
+    const float *Xm = xplane(z - 1), *Xc = xplane(z), *Xp = xplane(z + 1);
+    float *dst = mplane(z);
+    const int64_t zoff = (int64_t)wrap_any(z, P.nz) * plane;
+    for (int pos = tid; pos < G::PM; pos += G::NT) {
+      const int my = pos / G::MX, mx = pos - my * G::MX;
+      const bool ex = (mx == 0 || mx == G::MX - 1), ey = (my == 0 || my == G::MY - 1);
+      if (interior_only ? (ex || ey) : (ex && ey)) continue;
+      const int px = (my + 1) * G::HX + (mx + 1);
+      float d[S], lap[S];
+#pragma unroll
+      for (int c = 0; c < S; ++c) {
+        const float *q = Xc + c * G::PX;
+        d[c] = q[px];
+        lap[c] = (Xp[c * G::PX + px] + Xm[c * G::PX + px] + q[px + G::HX] + q[px - G::HX] +
+                  q[px + 1] + q[px - 1] - 6.f * d[c]) * P.inv_dx2;
+      }
+      const float spv =
+          P.sp ? __ldg(P.sp + zoff + (int64_t)wy[my + 1] * P.nx + wx[mx + 1]) : 0.f;
+      float mu[S], M[NM];
+      chem32(P, d, lap, spv, mu, M, &flags);
+#pragma unroll
+      for (int c = 0; c < S; ++c) dst[c * G::PM + pos] = mu[c];
+#pragma unroll
+      for (int c = 0; c < NM; ++c) dst[(S + c) * G::PM + pos] = M[c];
+    }
+  };
+  const int pX = (ty + 2) * G::HX + (tx + 2);
+  const int pM = (ty + 1) * G::MX + (tx + 1);
+  const bool in_tile = (x0 + tx < P.nx) && (y0 + ty < P.ny);
+  __syncthreads();
+  load_x(zb - 2);
+  load_x(zb - 1);
+  load_x(zb);
+  __syncthreads();
+  compute_mu(zb - 1, true);
+  __syncthreads();
+  load_x(zb + 1);
+  __syncthreads();
+  compute_mu(zb, false);
+  __syncthreads();
+  float Jm[S];
+  face32_between<G::PX, G::PM>(P, xplane(zb - 1), mplane(zb - 1), pX, pM, xplane(zb), mplane(zb),
+                               pX, pM, Jm);
+  float vmax = 0.f;
+  for (int z = zb; z < ze; ++z) {
+    __syncthreads();
+    load_x(z + 2);
+    __syncthreads();
+    compute_mu(z + 1, false);
+    __syncthreads();
+    float Jz[S];
+    face32_between<G::PX, G::PM>(P, xplane(z), mplane(z), pX, pM, xplane(z + 1), mplane(z + 1),
+                                 pX, pM, Jz);
+    plane_faces32<TX, TY>(P, xplane(z), mplane(z), Fx, Fy, tid);
+    __syncthreads();
+    if (in_tile) {
+      float out[S];
+#pragma unroll
+      for (int c = 0; c < S; ++c) {
+        const float a = (Jz[c] - Jm[c]) +
+                        (Fy[c * G::NFY + (ty + 1) * TX + tx] - Fy[c * G::NFY + ty * TX + tx]) +
+                        (Fx[c * G::NFX + ty * (TX + 1) + tx + 1] - Fx[c * G::NFX + ty * (TX + 1) + tx]);
+        out[c] = a * P.inv_dx;
+      }
+      store_rate(P.dX, (int64_t)z * plane + (int64_t)(y0 + ty) * P.nx + (x0 + tx), out, vmax);
+    }
+#pragma unroll
+    for (int c = 0; c < S; ++c) Jm[c] = Jz[c];
+  }
+  if (flags) atomicOr(&P.st->flags, flags);
+  finish_rate32(P, vmax, red);
+}
+
+template <int TX, int TY>
+constexpr size_t march3d32_smem() {
+  using G = PlaneGeom<TX, TY>;
+  return (G::NT / 32) * sizeof(double) +
+         (3 * S * G::PX + 2 * NP * G::PM + S * G::NFX + S * G::NFY) * sizeof(float) +
+         (G::HX + G::HY) * sizeof(int);
+}
+
+template <int TX>
+__global__ void __launch_bounds__(TX) k32_rate_1d(Rate32 P) {
+  if (P.st->halt) return;
+  constexpr int HX = TX + 4, MX = TX + 2;
+  __shared__ float Xs[S][HX];
+  __shared__ float Ms[NP][MX];
+  __shared__ float Fx[S][TX + 1];
+  __shared__ double red[(TX + 31) / 32];
+  const int tx = threadIdx.x;
+  const int x0 = blockIdx.x * TX;
+  const int n = P.nx;
+  unsigned flags = 0;
+  for (int pos = tx; pos < HX; pos += TX) {
+    const float4 v = __ldg(P.D + wrap_any(x0 + pos - 2, n));
+    Xs[0][pos] = v.x;
+    Xs[1][pos] = v.y;
+    Xs[2][pos] = v.z;
+    Xs[3][pos] = v.w;
+  }
+  __syncthreads();
+  for (int pos = tx; pos < MX; pos += TX) {
+    const int px = pos + 1;
+    float d[S], lap[S];
+#pragma unroll
+    for (int c = 0; c < S; ++c) {
+      d[c] = Xs[c][px];
+      lap[c] = (Xs[c][px + 1] + Xs[c][px - 1] - 2.f * d[c]) * P.inv_dx2;
+    }
+    const float spv = P.sp ? __ldg(P.sp + wrap_any(x0 + pos - 1, n)) : 0.f;
+    float mu[S], M[NM];
+    chem32(P, d, lap, spv, mu, M, &flags);
+#pragma unroll
+    for (int c = 0; c < S; ++c) Ms[c][pos] = mu[c];
+#pragma unroll
+    for (int c = 0; c < NM; ++c) Ms[S + c][pos] = M[c];
+  }
+  __syncthreads();
+  for (int f = tx; f < TX + 1; f += TX) {
+    float Dc[S], Dn[S], Mc[NM], Mn[NM], g[S], J[S];
+#pragma unroll
+    for (int c = 0; c < S; ++c) {
+      Dc[c] = Xs[c][f + 1];
+      Dn[c] = Xs[c][f + 2];
+      g[c] = (Ms[c][f + 1] - Ms[c][f]) * P.inv_dx;
+    }
+#pragma unroll
+    for (int c = 0; c < NM; ++c) {
+      Mc[c] = Ms[S + c][f];
+      Mn[c] = Ms[S + c][f + 1];
+    }
+    face_flux32(P, Dc, Mc, Dn, Mn, g, J);
+#pragma unroll
+    for (int c = 0; c < S; ++c) Fx[c][f] = J[c];
+  }
+  __syncthreads();
+  float vmax = 0.f;
+  if (x0 + tx < n) {
+    float out[S];
+#pragma unroll
+    for (int c = 0; c < S; ++c) out[c] = (Fx[c][tx + 1] - Fx[c][tx]) * P.inv_dx;
+    store_rate(P.dX, x0 + tx, out, vmax);
+  }
+  if (flags) atomicOr(&P.st->flags, flags);
+  finish_rate32(P, vmax, red);
+}
+
+// ------------------------------------------------------------------------
+// Compensated update, clamp, next misfit, out-of-bounds test
+// ------------------------------------------------------------------------
+struct Update32 {
+  float4 *hi, *lo;
+  const float4 *dX;
+  int64_t npts;
+  StepState32 *st;
+  double x0[S];
+  double sum_x0;
+  float lvec[S];
+  float *s;          // next misfit or nullptr
+  int oob_interval;
+};
+
+// (h, l) += inc with TwoSum and renormalisation; explicit _rn intrinsics keep
+// every operation separately rounded.
+__device__ __forceinline__ void comp_add(float &h, float &l, float inc) {
+  const float s = __fadd_rn(h, inc);
+  const float bb = __fsub_rn(s, h);
+  const float err = __fadd_rn(__fsub_rn(h, __fsub_rn(s, bb)), __fsub_rn(inc, bb));
+  const float lo = __fadd_rn(l, err);
+  const float hn = __fadd_rn(s, lo);
+  l = __fsub_rn(lo, __fsub_rn(hn, s));
+  h = hn;
+}
+
+__device__ __forceinline__ unsigned oob_flags_x(const double x[S]) {
+  unsigned f = 0;
+  double sum = 0.0;
+#pragma unroll
+  for (int c = 0; c < S; ++c) {
+    if (!isfinite(x[c])) f |= PF5D_FLAG_NONFINITE;
+    sum = sum + x[c];
+    if (x[c] < 0.0 - 1e-3 || x[c] > 1.0 + 1e-3) f |= PF5D_FLAG_OOB_HARD;
+    if (x[c] < 0.0 - 1e-5 || x[c] > 1.0 + 1e-5) f |= PF5D_FLAG_OOB_SOFT;
+  }
+  if (sum > 1.0 + 1e-3 || sum < 0.0 - 1e-3) f |= PF5D_FLAG_OOB_HARD;
+  if (sum > 1.0 + 1e-5 || sum < 0.0 - 1e-5) f |= PF5D_FLAG_OOB_SOFT;
+  return f;
+}
+
+__device__ __forceinline__ void raise32(StepState32 *st, unsigned f) {
+  if (!f) return;
+  atomicOr(&st->flags, f);
+  if (f & (PF5D_FLAG_NONFINITE | PF5D_FLAG_OOB_HARD)) atomicExch(&st->halt, 1u);
+}
+
+__global__ void k32_update(Update32 U) {
+  StepState32 *st = U.st;
+  if (st->halt) return;
+  const float dtf = (float)st->dt;
+  const bool check = U.oob_interval > 0 && (st->step % U.oob_interval) == 0;
+  unsigned f = 0;
+  for (int64_t p = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; p < U.npts;
+       p += (int64_t)gridDim.x * blockDim.x) {
+    const float4 H = U.hi[p], L = U.lo[p], R = U.dX[p];
+    float h[S] = {H.x, H.y, H.z, H.w}, l[S] = {L.x, L.y, L.z, L.w};
+    const float r[S] = {R.x, R.y, R.z, R.w};
+#pragma unroll
+    for (int c = 0; c < S; ++c) comp_add(h[c], l[c], __fmul_rn(dtf, r[c]));
+    double dd[S], dsum = 0.0;
+#pragma unroll
+    for (int c = 0; c < S; ++c) {
+      dd[c] = (double)h[c] + (double)l[c];
+      dsum = dsum + dd[c];
+    }
+    const double total = U.sum_x0 + dsum;
+    if (total > 1.0) {                 // clamp_simplex on X = X0 + D, in FP64
+      const double inv = 1.0 / total;
+#pragma unroll
+      for (int c = 0; c < S; ++c) {
+        const double dn = (U.x0[c] + dd[c]) * inv - U.x0[c];
+        h[c] = (float)dn;
+        l[c] = (float)(dn - (double)h[c]);
+        dd[c] = (double)h[c] + (double)l[c];
+      }
+    }
+    U.hi[p] = make_float4(h[0], h[1], h[2], h[3]);
+    U.lo[p] = make_float4(l[0], l[1], l[2], l[3]);
+    if (U.s) {
+      float acc = 0.f;
+#pragma unroll
+      for (int c = 0; c < S; ++c) acc = fmaf(h[c] + l[c], U.lvec[c], acc);
+      U.s[p] = acc;
+    }
+    if (check) {
+      double x[S];
+#pragma unroll
+      for (int c = 0; c < S; ++c) x[c] = U.x0[c] + dd[c];
+      f |= oob_flags_x(x);
+    }
+  }
+  raise32(st, f);
+}
+
+__global__ void k32_split(const double *__restrict__ X, int64_t npts, Update32 U) {
+  unsigned f = 0;
+  for (int64_t p = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; p < npts;
+       p += (int64_t)gridDim.x * blockDim.x) {
+    float h[S], l[S];
+    double x[S];
+#pragma unroll
+    for (int c = 0; c < S; ++c) {
+      x[c] = X[4 * p + c];
+      const double d = x[c] - U.x0[c];
+      h[c] = (float)d;
+      l[c] = (float)(d - (double)h[c]);
+    }
+    U.hi[p] = make_float4(h[0], h[1], h[2], h[3]);
+    U.lo[p] = make_float4(l[0], l[1], l[2], l[3]);
+    if (U.s) {
+      float acc = 0.f;
+#pragma unroll
+      for (int c = 0; c < S; ++c) acc = fmaf(h[c] + l[c], U.lvec[c], acc);
+      U.s[p] = acc;
+    }
+    if (U.oob_interval > 0) f |= oob_flags_x(x);
+  }
+  raise32(U.st, f);
+}
+
+__global__ void k32_join(const float4 *__restrict__ hi, const float4 *__restrict__ lo,
+                         int64_t npts, Update32 U, double *__restrict__ X) {
+  for (int64_t p = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; p < npts;
+       p += (int64_t)gridDim.x * blockDim.x) {
+    const float4 H = hi[p], L = lo[p];
+    const float h[S] = {H.x, H.y, H.z, H.w}, l[S] = {L.x, L.y, L.z, L.w};
+#pragma unroll
+    for (int c = 0; c < S; ++c) X[4 * p + c] = U.x0[c] + ((double)h[c] + (double)l[c]);
+  }
+}
+
+constexpr int kMassBlocks = 512;
+
+// FP64 per-component sums of X = X0 + hi + lo; two passes, deterministic.
+__global__ void k32_mass_partial(const float4 *__restrict__ hi, const float4 *__restrict__ lo,
+                                 int64_t npts, double *partial) {
+  __shared__ double red[S][8];
+  double acc[S] = {0.0, 0.0, 0.0, 0.0};
+  for (int64_t p = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; p < npts;
+       p += (int64_t)gridDim.x * blockDim.x) {
+    const float4 H = hi[p], L = lo[p];
+    acc[0] += (double)H.x + (double)L.x;
+    acc[1] += (double)H.y + (double)L.y;
+    acc[2] += (double)H.z + (double)L.z;
+    acc[3] += (double)H.w + (double)L.w;
+  }
+#pragma unroll
+  for (int c = 0; c < S; ++c) {
+    double v = acc[c];
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    if ((threadIdx.x & 31) == 0) red[c][threadIdx.x >> 5] = v;
+  }
+  __syncthreads();
+  if (threadIdx.x < S) {
+    double v = 0.0;
+    for (int w = 0; w < (int)(blockDim.x >> 5); ++w) v += red[threadIdx.x][w];
+    partial[blockIdx.x * S + threadIdx.x] = v;
+  }
+}
+
+__global__ void k32_mass_final(const double *partial, int nparts, double *out) {
+  if (threadIdx.x < S) {
+    double v = 0.0;
+    for (int b = 0; b < nparts; ++b) v += partial[b * S + threadIdx.x];
+    out[threadIdx.x] = v;
+  }
+}
+
+__global__ void k32_bmul(cufftComplex *__restrict__ k, const float *__restrict__ bk, int64_t nk,
+                         const unsigned *halt) {
+  if (halt && *halt) return;
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < nk;
+       i += (int64_t)gridDim.x * blockDim.x) {
+    const float b = bk[i];
+    cufftComplex v = k[i];
+    v.x *= b;
+    v.y *= b;
+    k[i] = v;
+  }
+}
+
+// ------------------------------------------------------------------------
+// Host side
+// ------------------------------------------------------------------------
+constexpr int kTX1_32 = 128;
+constexpr int kGraphSteps32 = 50;
+
+struct Variant32 {
+  int tx, ty, minb;
+  size_t smem2d, smem3d;
+  void (*set_attrs)();
+  void (*launch2d)(dim3, dim3, size_t, cudaStream_t, const Rate32 &);
+  void (*launch3d)(dim3, dim3, size_t, cudaStream_t, const Rate32 &, int);
+};
+
+template <int TX, int TY, int MINB>
+Variant32 make_variant32() {
+  Variant32 v;
+  v.tx = TX;
+  v.ty = TY;
+  v.minb = MINB;
+  v.smem2d = tile2d32_smem<TX, TY>();
+  v.smem3d = march3d32_smem<TX, TY>();
+  v.set_attrs = []() {
+    const auto a = cudaFuncAttributeMaxDynamicSharedMemorySize;
+    cudaFuncSetAttribute(k32_rate_tile2d<TX, TY, MINB>, a, (int)tile2d32_smem<TX, TY>());
+    cudaFuncSetAttribute(k32_rate_march3d<TX, TY, MINB>, a, (int)march3d32_smem<TX, TY>());
+  };
+  v.launch2d = [](dim3 g, dim3 b, size_t sm, cudaStream_t s, const Rate32 &P) {
+    k32_rate_tile2d<TX, TY, MINB><<<g, b, sm, s>>>(P);
+  };
+  v.launch3d = [](dim3 g, dim3 b, size_t sm, cudaStream_t s, const Rate32 &P, int zc) {
+    k32_rate_march3d<TX, TY, MINB><<<g, b, sm, s>>>(P, zc);
+  };
+  return v;
+}
+
+const std::vector<Variant32> &variants32() {
+  static const std::vector<Variant32> v = {
+      make_variant32<32, 8, 2>(), make_variant32<32, 8, 3>(), make_variant32<32, 8, 4>(),
+      make_variant32<32, 4, 6>(), make_variant32<64, 4, 3>(), make_variant32<32, 16, 2>()};
+  return v;
+}
+
+struct Stepper32 {
+  pf5d_stepper_desc d{};
+  int64_t shape[3] = {1, 1, 1};
+  int64_t npts = 0, nk = 0;
+  float4 *hi = nullptr, *lo = nullptr, *dX = nullptr;
+  float *s = nullptr, *bk = nullptr;
+  cufftComplex *k = nullptr;
+  cufftHandle fwd = 0, inv = 0;
+  bool plans = false;
+  double *mass_ws = nullptr;
+  StepState32 *st = nullptr;
+  Rate32 rp{};
+  Update32 up{};
+  cudaStream_t cap = nullptr;
+  std::map<int64_t, cudaGraphExec_t> graphs;
+  dim3 grid, block;
+  size_t smem = 0;
+  int zc = 1;
+  int variant = 0;
+};
+
+#define PF5D_CUFFT32(call)                                                         \
+  do {                                                                             \
+    cufftResult r_ = (call);                                                       \
+    if (r_ != CUFFT_SUCCESS) {                                                     \
+      set_error("%s:%d %s: cufft error %d", __FILE__, __LINE__, #call, (int)r_);   \
+      return PF5D_ERR_CUFFT;                                                       \
+    }                                                                              \
+  } while (0)
+
+static pf5d_status configure32(Stepper32 *h, int variant) {
+  const Rate32 &P = h->rp;
+  if (h->d.dim == 1) {
+    h->block = dim3(kTX1_32);
+    h->grid = dim3((unsigned)((P.nx + kTX1_32 - 1) / kTX1_32));
+    h->smem = 0;
+    return PF5D_OK;
+  }
+  const auto &vars = variants32();
+  PF5D_REQUIRE(variant >= 0 && variant < (int)vars.size(), PF5D_ERR_ARG, "bad variant %d",
+               variant);
+  const Variant32 &v = vars[variant];
+  h->variant = variant;
+  v.set_attrs();
+  PF5D_LAUNCHED();
+  h->block = dim3(v.tx, v.ty);
+  const unsigned gx = (unsigned)((P.nx + v.tx - 1) / v.tx), gy = (unsigned)((P.ny + v.ty - 1) / v.ty);
+  if (h->d.dim == 2) {
+    h->smem = v.smem2d;
+    h->grid = dim3(gx, gy, 1);
+    return PF5D_OK;
+  }
+  h->smem = v.smem3d;
+  const int64_t tiles = (int64_t)gx * gy;
+  const int64_t target = (int64_t)sm_count() * v.minb * 4;
+  int64_t zc = (tiles * P.nz + target - 1) / target;
+  zc = std::max<int64_t>(4, std::min<int64_t>(zc, 64));
+  zc = std::min<int64_t>(zc, P.nz);
+  h->zc = (int)zc;
+  h->grid = dim3(gx, gy, (unsigned)((P.nz + zc - 1) / zc));
+  return PF5D_OK;
+}
+
+static pf5d_status launch_rate32(Stepper32 *h, cudaStream_t s) {
+  switch (h->d.dim) {
+    case 1: k32_rate_1d<kTX1_32><<<h->grid, h->block, 0, s>>>(h->rp); break;
+    case 2: variants32()[h->variant].launch2d(h->grid, h->block, h->smem, s, h->rp); break;
+    default: variants32()[h->variant].launch3d(h->grid, h->block, h->smem, s, h->rp, h->zc);
+  }
+  PF5D_LAUNCHED();
+  return PF5D_OK;
+}
+
+static pf5d_status enqueue32(Stepper32 *h, cudaStream_t s) {
+  if (h->d.elastic) {
+    PF5D_CUFFT32(cufftSetStream(h->fwd, s));
+    PF5D_CUFFT32(cufftExecR2C(h->fwd, h->s, h->k));
+    k32_bmul<<<grid_for(h->nk, 256), 256, 0, s>>>(h->k, h->bk, h->nk, &h->st->halt);
+    PF5D_LAUNCHED();
+    PF5D_CUFFT32(cufftSetStream(h->inv, s));
+    PF5D_CUFFT32(cufftExecC2R(h->inv, h->k, h->s));
+  }
+  pf5d_status st = launch_rate32(h, s);
+  if (st != PF5D_OK) return st;
+  k32_update<<<grid_for(h->npts, 256, 4), 256, 0, s>>>(h->up);
+  PF5D_LAUNCHED();
+  return PF5D_OK;
+}
+
+static pf5d_status graph32(Stepper32 *h, int64_t n, cudaGraphExec_t *out) {
+  auto it = h->graphs.find(n);
+  if (it != h->graphs.end()) {
+    *out = it->second;
+    return PF5D_OK;
+  }
+  cudaGraph_t g = nullptr;
+  PF5D_CUDA(cudaStreamBeginCapture(h->cap, cudaStreamCaptureModeThreadLocal));
+  pf5d_status st = PF5D_OK;
+  for (int64_t i = 0; i < n && st == PF5D_OK; ++i) st = enqueue32(h, h->cap);
+  cudaError_t e = cudaStreamEndCapture(h->cap, &g);
+  if (st != PF5D_OK) {
+    if (g) cudaGraphDestroy(g);
+    return st;
+  }
+  PF5D_REQUIRE(e == cudaSuccess, PF5D_ERR_CUDA, "graph capture: %s", cudaGetErrorString(e));
+  cudaGraphExec_t exec = nullptr;
+  e = cudaGraphInstantiate(&exec, g, 0);
+  cudaGraphDestroy(g);
+  PF5D_REQUIRE(e == cudaSuccess, PF5D_ERR_CUDA, "graph instantiate: %s", cudaGetErrorString(e));
+  h->graphs[n] = exec;
+  *out = exec;
+  return PF5D_OK;
+}
+
+static void drop_graphs(Stepper32 *h) {
+  for (auto &kv : h->graphs) cudaGraphExecDestroy(kv.second);
+  h->graphs.clear();
+}
+
+pf5d_status s32_create(const pf5d_stepper_desc *desc, const double *X_init, void *stream,
+                       Stepper32 **out) {
+  PF5D_REQUIRE(desc && X_init && out && desc->grid32, PF5D_ERR_ARG, "null argument");
+  PF5D_REQUIRE(desc->node_stride32 == kStride32 && (((uintptr_t)desc->grid32) & 15) == 0,
+               PF5D_ERR_ARG, "FP32 table needs %d floats per node, 16-byte aligned", kStride32);
+  auto *h = new Stepper32();
+  h->d = *desc;
+  h->d.bk = nullptr;
+  int64_t npts = 1;
+  for (int d = 0; d < desc->dim; ++d) {
+    h->shape[d] = desc->shape[d];
+    npts *= desc->shape[d];
+  }
+  h->npts = npts;
+  auto fail = [&](pf5d_status code) {
+    s32_destroy(h);
+    return code;
+  };
+  if (cudaMalloc(&h->hi, npts * sizeof(float4)) != cudaSuccess ||
+      cudaMalloc(&h->lo, npts * sizeof(float4)) != cudaSuccess ||
+      cudaMalloc(&h->dX, npts * sizeof(float4)) != cudaSuccess ||
+      cudaMalloc(&h->st, sizeof(StepState32)) != cudaSuccess ||
+      cudaMalloc(&h->mass_ws, (kMassBlocks * S + S) * sizeof(double)) != cudaSuccess ||
+      cudaStreamCreateWithFlags(&h->cap, cudaStreamNonBlocking) != cudaSuccess) {
+    set_error("device allocation failed");
+    return fail(PF5D_ERR_CUDA);
+  }
+  if (desc->elastic) {
+    long long n[3];
+    for (int d = 0; d < desc->dim; ++d) n[d] = desc->shape[d];
+    h->nk = npts / desc->shape[desc->dim - 1] * (desc->shape[desc->dim - 1] / 2 + 1);
+    size_t ws = 0;
+    if (cufftCreate(&h->fwd) != CUFFT_SUCCESS || cufftCreate(&h->inv) != CUFFT_SUCCESS ||
+        cufftMakePlanMany64(h->fwd, desc->dim, n, nullptr, 1, 0, nullptr, 1, 0, CUFFT_R2C, 1,
+                            &ws) != CUFFT_SUCCESS ||
+        cufftMakePlanMany64(h->inv, desc->dim, n, nullptr, 1, 0, nullptr, 1, 0, CUFFT_C2R, 1,
+                            &ws) != CUFFT_SUCCESS) {
+      set_error("cuFFT plan creation failed");
+      return fail(PF5D_ERR_CUFFT);
+    }
+    h->plans = true;
+    std::vector<float> b(h->nk);
+    const double inv_n = 1.0 / (double)npts;
+    for (int64_t i = 0; i < h->nk; ++i) b[i] = (float)(desc->bk[i] * inv_n);
+    if (cudaMalloc(&h->s, npts * sizeof(float)) != cudaSuccess ||
+        cudaMalloc(&h->k, h->nk * sizeof(cufftComplex)) != cudaSuccess ||
+        cudaMalloc(&h->bk, h->nk * sizeof(float)) != cudaSuccess ||
+        cudaMemcpy(h->bk, b.data(), h->nk * sizeof(float), cudaMemcpyHostToDevice) != cudaSuccess) {
+      set_error("device allocation failed");
+      return fail(PF5D_ERR_CUDA);
+    }
+  }
+  Rate32 &P = h->rp;
+  if (desc->dim == 1) {
+    P.nz = 1; P.ny = 1; P.nx = (int)h->shape[0];
+  } else if (desc->dim == 2) {
+    P.nz = 1; P.ny = (int)h->shape[0]; P.nx = (int)h->shape[1];
+  } else {
+    P.nz = (int)h->shape[0]; P.ny = (int)h->shape[1]; P.nx = (int)h->shape[2];
+  }
+  P.D = h->hi;
+  P.sp = desc->elastic ? h->s : nullptr;
+  P.dX = h->dX;
+  Table32 &T = P.T;
+  T.grid = desc->grid32;
+  T.coord = desc->node_coord;
+  T.n = desc->table_n;
+  T.stride = kStride32;
+  T.inv_step = 1.0 / desc->resolution;
+  T.inv_step_f = (float)T.inv_step;
+  T.threshold = 1.0 - 4.0 * desc->resolution - 1e-9;
+  T.exact_d2 = (1.99 * desc->resolution) * (1.99 * desc->resolution);
+  T.max_nn_dist = desc->max_nn_dist;
+  double sx = 0.0;
+  for (int c = 0; c < S; ++c) {
+    const double u = desc->x0[c] * T.inv_step;
+    const double fl = floor(u);
+    T.ib[c] = (int)fl;
+    T.fb[c] = (float)(u - fl);
+    T.x0[c] = desc->x0[c];
+    sx = sx + desc->x0[c];
+    P.kappa[c] = (float)desc->kappa[c];
+    P.lvec[c] = (float)desc->lvec[c];
+    P.x0f[c] = (float)desc->x0[c];
+  }
+  T.sum_x0 = sx;
+  P.c_fe = 1.0 - sx;
+  P.inv_dx = (float)(1.0 / desc->dx);
+  P.inv_dx2 = (float)(1.0 / (desc->dx * desc->dx));
+  P.ctld = desc->ctld;
+  P.t_cfl = desc->t_cfl;
+  P.lower = desc->lower_limit;
+  P.upper = desc->upper_limit;
+  P.factor = desc->max_change_factor;
+  P.adaptive = desc->adaptive;
+  P.st = h->st;
+  Update32 &U = h->up;
+  U.hi = h->hi;
+  U.lo = h->lo;
+  U.dX = h->dX;
+  U.npts = npts;
+  U.st = h->st;
+  for (int c = 0; c < S; ++c) {
+    U.x0[c] = desc->x0[c];
+    U.lvec[c] = (float)desc->lvec[c];
+  }
+  U.sum_x0 = sx;
+  U.s = desc->elastic ? h->s : nullptr;
+  U.oob_interval = desc->oob_interval;
+  pf5d_status st = configure32(h, 0);
+  if (st != PF5D_OK) return fail(st);
+  if ((st = s32_reset(h, X_init, desc->dt0, 0.0, stream)) != PF5D_OK) return fail(st);
+  *out = h;
+  return PF5D_OK;
+}
+
+pf5d_status s32_reset(Stepper32 *h, const double *X, double dt, double time, void *stream) {
+  cudaStream_t s = as_stream(stream);
+  StepState32 init{};
+  init.dt = dt;
+  init.time = time;
+  PF5D_CUDA(cudaMemcpyAsync(h->st, &init, sizeof(init), cudaMemcpyHostToDevice, s));
+  if (X) {
+    k32_split<<<grid_for(h->npts, 256, 4), 256, 0, s>>>(X, h->npts, h->up);
+    PF5D_LAUNCHED();
+  }
+  PF5D_CUDA(cudaStreamSynchronize(s));
+  return PF5D_OK;
+}
+
+pf5d_status s32_advance(Stepper32 *h, int64_t nsteps, void *stream) {
+  cudaStream_t s = as_stream(stream);
+  while (nsteps > 0) {
+    const int64_t n = nsteps < kGraphSteps32 ? nsteps : kGraphSteps32;
+    cudaGraphExec_t g = nullptr;
+    pf5d_status st = graph32(h, n, &g);
+    if (st != PF5D_OK) return st;
+    PF5D_CUDA(cudaGraphLaunch(g, s));
+    nsteps -= n;
+  }
+  return PF5D_OK;
+}
+
+pf5d_status s32_state(Stepper32 *h, pf5d_step_state *out, void *stream) {
+  StepState32 hs;
+  cudaStream_t s = as_stream(stream);
+  PF5D_CUDA(cudaMemcpyAsync(&hs, h->st, sizeof(hs), cudaMemcpyDeviceToHost, s));
+  PF5D_CUDA(cudaStreamSynchronize(s));
+  out->dt = hs.dt;
+  out->time = hs.time;
+  out->xdotmax = hs.xdotmax;
+  out->step = hs.step;
+  out->flags = hs.flags | (hs.halt ? PF5D_FLAG_HALTED : 0u);
+  out->halted = hs.halt;
+  return PF5D_OK;
+}
+
+pf5d_status s32_field(Stepper32 *h, double *X_out, void *stream) {
+  cudaStream_t s = as_stream(stream);
+  k32_join<<<grid_for(h->npts, 256, 4), 256, 0, s>>>(h->hi, h->lo, h->npts, h->up, X_out);
+  PF5D_LAUNCHED();
+  return PF5D_OK;
+}
+
+pf5d_status s32_mass(Stepper32 *h, double *mean_out, void *stream) {
+  cudaStream_t s = as_stream(stream);
+  const unsigned nb = std::min<unsigned>(kMassBlocks, grid_for(h->npts, 256, 4));
+  k32_mass_partial<<<nb, 256, 0, s>>>(h->hi, h->lo, h->npts, h->mass_ws);
+  PF5D_LAUNCHED();
+  k32_mass_final<<<1, 32, 0, s>>>(h->mass_ws, (int)nb, h->mass_ws + kMassBlocks * S);
+  PF5D_LAUNCHED();
+  double sums[S];
+  PF5D_CUDA(cudaMemcpyAsync(sums, h->mass_ws + kMassBlocks * S, sizeof(sums),
+                            cudaMemcpyDeviceToHost, s));
+  PF5D_CUDA(cudaStreamSynchronize(s));
+  for (int c = 0; c < S; ++c) mean_out[c] = h->d.x0[c] + sums[c] / (double)h->npts;
+  return PF5D_OK;
+}
+
+pf5d_status s32_set_variant(Stepper32 *h, int32_t variant) {
+  pf5d_status st = configure32(h, variant);
+  if (st == PF5D_OK) drop_graphs(h);
+  return st;
+}
+
+pf5d_status s32_autotune(Stepper32 *h, int32_t *variant, float *best_ms, void *stream) {
+  cudaStream_t s = as_stream(stream);
+  if (h->d.dim == 1) {
+    if (variant) *variant = 0;
+    if (best_ms) *best_ms = 0.f;
+    return PF5D_OK;
+  }
+  StepState32 saved;
+  PF5D_CUDA(cudaMemcpyAsync(&saved, h->st, sizeof(saved), cudaMemcpyDeviceToHost, s));
+  PF5D_CUDA(cudaStreamSynchronize(s));
+  cudaEvent_t e0, e1;
+  PF5D_CUDA(cudaEventCreate(&e0));
+  PF5D_CUDA(cudaEventCreate(&e1));
+  int best = h->variant;
+  float best_t = 1e30f;
+  for (int v = 0; v < (int)variants32().size(); ++v) {
+    if (configure32(h, v) != PF5D_OK) continue;
+    if (launch_rate32(h, s) != PF5D_OK) {
+      cudaGetLastError();
+      continue;
+    }
+    PF5D_CUDA(cudaEventRecord(e0, s));
+    pf5d_status st = PF5D_OK;
+    for (int r = 0; r < 5 && st == PF5D_OK; ++r) st = launch_rate32(h, s);
+    PF5D_CUDA(cudaEventRecord(e1, s));
+    PF5D_CUDA(cudaEventSynchronize(e1));
+    float ms = 0.f;
+    PF5D_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+    if (st == PF5D_OK && ms / 5 < best_t) {
+      best_t = ms / 5;
+      best = v;
+    }
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  pf5d_status st = configure32(h, best);
+  if (st != PF5D_OK) return st;
+  drop_graphs(h);
+  PF5D_CUDA(cudaMemcpyAsync(h->st, &saved, sizeof(saved), cudaMemcpyHostToDevice, s));
+  PF5D_CUDA(cudaStreamSynchronize(s));
+  if (variant) *variant = best;
+  if (best_ms) *best_ms = best_t;
+  return PF5D_OK;
+}
+
+pf5d_status s32_launch_stage(Stepper32 *h, int32_t stage, void *stream) {
+  cudaStream_t s = as_stream(stream);
+  switch (stage) {
+    case PF5D_STAGE_RATE:
+      return launch_rate32(h, s);
+    case PF5D_STAGE_UPDATE:
+      k32_update<<<grid_for(h->npts, 256, 4), 256, 0, s>>>(h->up);
+      PF5D_LAUNCHED();
+      return PF5D_OK;
+    case PF5D_STAGE_FFT_FWD:
+      PF5D_REQUIRE(h->d.elastic, PF5D_ERR_ARG, "elasticity is off");
+      PF5D_CUFFT32(cufftSetStream(h->fwd, s));
+      PF5D_CUFFT32(cufftExecR2C(h->fwd, h->s, h->k));
+      return PF5D_OK;
+    case PF5D_STAGE_BMUL:
+      PF5D_REQUIRE(h->d.elastic, PF5D_ERR_ARG, "elasticity is off");
+      k32_bmul<<<grid_for(h->nk, 256), 256, 0, s>>>(h->k, h->bk, h->nk, &h->st->halt);
+      PF5D_LAUNCHED();
+      return PF5D_OK;
+    case PF5D_STAGE_FFT_INV:
+      PF5D_REQUIRE(h->d.elastic, PF5D_ERR_ARG, "elasticity is off");
+      PF5D_CUFFT32(cufftSetStream(h->inv, s));
+      PF5D_CUFFT32(cufftExecC2R(h->inv, h->k, h->s));
+      return PF5D_OK;
+    default:
+      set_error("unknown stage %d", stage);
+      return PF5D_ERR_ARG;
+  }
+}
+
+float *s32_rate(Stepper32 *h) { return reinterpret_cast<float *>(h->dX); }
+
+void s32_destroy(Stepper32 *h) {
+  if (!h) return;
+  drop_graphs(h);
+  if (h->plans) {
+    cufftDestroy(h->fwd);
+    cufftDestroy(h->inv);
+  }
+  cudaFree(h->hi);
+  cudaFree(h->lo);
+  cudaFree(h->dX);
+  cudaFree(h->s);
+  cudaFree(h->bk);
+  cudaFree(h->k);
+  cudaFree(h->st);
+  cudaFree(h->mass_ws);
+  if (h->cap) cudaStreamDestroy(h->cap);
+  delete h;
+}
+
+}  // namespace pf5d

@@ -30,6 +30,8 @@
 
 #include "pf5d_device.cuh"
 #include "pf5d_fft.h"
+#include "pf5d_fp32c.h"
+#include "pf5d_tiles.cuh"
 
 namespace pf5d {
 
@@ -112,19 +114,6 @@ __device__ __forceinline__ void finish_rate(const RateParams &P, double m, doubl
     }
   }
 }
-
-// Shared-memory geometry of one plane tile: TY rows (axis "y") x TX columns
-// (the contiguous axis "x").  X is staged with a 2-cell halo (HY x HX), mu/M
-// with a 1-cell halo (MY x MX, corners unused).  x-faces: TY x (TX+1),
-// face (y, f) lies between columns f-1 and f; y-faces: (TY+1) x TX, face
-// (f, x) lies between rows f-1 and f.
-template <int TX, int TY>
-struct PlaneGeom {
-  static constexpr int HX = TX + 4, HY = TY + 4, PX = HX * HY;
-  static constexpr int MX = TX + 2, MY = TY + 2, PM = MX * MY;
-  static constexpr int NT = TX * TY;
-  static constexpr int NFX = TY * (TX + 1), NFY = (TY + 1) * TX;
-};
 
 // Flux through the face between (X plane XL, pos pl ; mu/M plane ML, pos ql)
 // and (XH, ph ; MH, qh), lower -> upper along one axis.
@@ -558,6 +547,38 @@ __global__ void k_check_state(const double *X, int64_t npts, StepState *st) {
   raise_flags(st, f);
 }
 
+constexpr int kMeanBlocks = 512;
+
+// FP64 per-component sums of X, two passes (deterministic order).
+__global__ void k_mean_partial(const double *__restrict__ X, int64_t npts, double *partial) {
+  __shared__ double red[S][8];
+  double acc[S] = {0.0, 0.0, 0.0, 0.0};
+  for (int64_t p = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; p < npts;
+       p += (int64_t)gridDim.x * blockDim.x)
+#pragma unroll
+    for (int c = 0; c < S; ++c) acc[c] += X[4 * p + c];
+#pragma unroll
+  for (int c = 0; c < S; ++c) {
+    double v = acc[c];
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    if ((threadIdx.x & 31) == 0) red[c][threadIdx.x >> 5] = v;
+  }
+  __syncthreads();
+  if (threadIdx.x < S) {
+    double v = 0.0;
+    for (int w = 0; w < (int)(blockDim.x >> 5); ++w) v += red[threadIdx.x][w];
+    partial[blockIdx.x * S + threadIdx.x] = v;
+  }
+}
+
+__global__ void k_mean_final(const double *partial, int nparts, double *out) {
+  if (threadIdx.x < S) {
+    double v = 0.0;
+    for (int b = 0; b < nparts; ++b) v += partial[b * S + threadIdx.x];
+    out[threadIdx.x] = v;
+  }
+}
+
 }  // namespace pf5d
 
 using namespace pf5d;
@@ -582,6 +603,8 @@ struct pf5d_stepper {
   int zc = 1;
   bool vec = false;
   int variant = 0;
+  Stepper32 *s32 = nullptr;      // FP32C form (all calls delegate)
+  double *mass_ws = nullptr;     // FP64 mean reduction workspace
 };
 
 namespace {
@@ -788,6 +811,25 @@ pf5d_status pf5d_stepper_create(const pf5d_stepper_desc *desc, double *X, void *
   PF5D_REQUIRE(desc && X && out, PF5D_ERR_ARG, "null argument");
   PF5D_REQUIRE(desc->dim >= 1 && desc->dim <= 3, PF5D_ERR_DIM,
                "Unsupported system_dim=%d. Choose 1, 2, or 3.", desc->dim);
+  PF5D_REQUIRE(desc->precision == PF5D_PRECISION_FP64 || desc->precision == PF5D_PRECISION_FP32C,
+               PF5D_ERR_ARG, "unknown precision %d", desc->precision);
+  for (int d = 0; d < desc->dim; ++d)
+    PF5D_REQUIRE(desc->shape[d] > 0 && desc->shape[d] <= (1LL << 30), PF5D_ERR_ARG, "bad shape");
+  PF5D_REQUIRE(!desc->elastic || desc->bk, PF5D_ERR_ARG, "elastic term needs B(k)");
+  if (desc->precision == PF5D_PRECISION_FP32C) {
+    PF5D_REQUIRE(desc->node_coord && desc->table_n >= 2, PF5D_ERR_ARG, "bad table description");
+    auto *h = new pf5d_stepper();
+    h->d = *desc;
+    h->d.bk = nullptr;
+    h->X = X;
+    pf5d_status st = s32_create(desc, X, stream, &h->s32);
+    if (st != PF5D_OK) {
+      delete h;
+      return st;
+    }
+    *out = h;
+    return PF5D_OK;
+  }
   PF5D_REQUIRE(desc->grid && desc->node_coord && desc->nprops == NP &&
                    desc->node_stride >= NP && desc->table_n >= 2,
                PF5D_ERR_ARG, "bad table description");
@@ -881,6 +923,7 @@ pf5d_status pf5d_stepper_create(const pf5d_stepper_desc *desc, double *X, void *
 
 pf5d_status pf5d_stepper_reset(pf5d_stepper *h, double dt, double time, void *stream) {
   PF5D_REQUIRE(h, PF5D_ERR_ARG, "null stepper");
+  if (h->s32) return s32_reset(h->s32, h->X, dt, time, stream);
   cudaStream_t s = as_stream(stream);
   StepState init{};
   init.dt = dt;
@@ -905,6 +948,7 @@ pf5d_status pf5d_stepper_reset(pf5d_stepper *h, double dt, double time, void *st
 
 pf5d_status pf5d_stepper_advance(pf5d_stepper *h, int64_t nsteps, void *stream) {
   PF5D_REQUIRE(h && nsteps >= 0, PF5D_ERR_ARG, "bad arguments");
+  if (h->s32) return s32_advance(h->s32, nsteps, stream);
   cudaStream_t s = as_stream(stream);
   while (nsteps > 0) {
     const int64_t n = nsteps < kGraphSteps ? nsteps : kGraphSteps;
@@ -919,6 +963,7 @@ pf5d_status pf5d_stepper_advance(pf5d_stepper *h, int64_t nsteps, void *stream) 
 
 pf5d_status pf5d_stepper_state(pf5d_stepper *h, pf5d_step_state *out, void *stream) {
   PF5D_REQUIRE(h && out, PF5D_ERR_ARG, "bad arguments");
+  if (h->s32) return s32_state(h->s32, out, stream);
   StepState hs;
   cudaStream_t s = as_stream(stream);
   PF5D_CUDA(cudaMemcpyAsync(&hs, h->st, sizeof(hs), cudaMemcpyDeviceToHost, s));
@@ -932,11 +977,43 @@ pf5d_status pf5d_stepper_state(pf5d_stepper *h, pf5d_step_state *out, void *stre
   return PF5D_OK;
 }
 
-double *pf5d_stepper_rate(pf5d_stepper *h) { return h ? h->dX : nullptr; }
+double *pf5d_stepper_rate(pf5d_stepper *h) {
+  if (!h) return nullptr;
+  if (h->s32) return reinterpret_cast<double *>(s32_rate(h->s32));
+  return h->dX;
+}
+
+pf5d_status pf5d_stepper_field(pf5d_stepper *h, double *X_out, void *stream) {
+  PF5D_REQUIRE(h && X_out, PF5D_ERR_ARG, "bad arguments");
+  if (h->s32) return s32_field(h->s32, X_out, stream);
+  if (X_out != h->X)
+    PF5D_CUDA(cudaMemcpyAsync(X_out, h->X, h->npts * 4 * sizeof(double), cudaMemcpyDeviceToDevice,
+                              as_stream(stream)));
+  return PF5D_OK;
+}
+
+pf5d_status pf5d_stepper_mass(pf5d_stepper *h, double *mean_out, void *stream) {
+  PF5D_REQUIRE(h && mean_out, PF5D_ERR_ARG, "bad arguments");
+  if (h->s32) return s32_mass(h->s32, mean_out, stream);
+  cudaStream_t s = as_stream(stream);
+  if (!h->mass_ws) PF5D_CUDA(cudaMalloc(&h->mass_ws, (kMeanBlocks * S + S) * sizeof(double)));
+  const unsigned nb = std::min<unsigned>(kMeanBlocks, grid_for(h->npts, 256, 4));
+  k_mean_partial<<<nb, 256, 0, s>>>(h->X, h->npts, h->mass_ws);
+  PF5D_LAUNCHED();
+  k_mean_final<<<1, 32, 0, s>>>(h->mass_ws, (int)nb, h->mass_ws + kMeanBlocks * S);
+  PF5D_LAUNCHED();
+  double sums[S];
+  PF5D_CUDA(cudaMemcpyAsync(sums, h->mass_ws + kMeanBlocks * S, sizeof(sums),
+                            cudaMemcpyDeviceToHost, s));
+  PF5D_CUDA(cudaStreamSynchronize(s));
+  for (int c = 0; c < S; ++c) mean_out[c] = sums[c] / (double)h->npts;
+  return PF5D_OK;
+}
 
 pf5d_status pf5d_stepper_autotune(pf5d_stepper *h, int32_t *variant, float *best_ms,
                                   void *stream) {
   PF5D_REQUIRE(h, PF5D_ERR_ARG, "null stepper");
+  if (h->s32) return s32_autotune(h->s32, variant, best_ms, stream);
   pf5d_status st = autotune_rate(h, as_stream(stream), best_ms);
   if (variant) *variant = h->variant;
   return st;
@@ -944,6 +1021,7 @@ pf5d_status pf5d_stepper_autotune(pf5d_stepper *h, int32_t *variant, float *best
 
 pf5d_status pf5d_stepper_set_variant(pf5d_stepper *h, int32_t variant) {
   PF5D_REQUIRE(h, PF5D_ERR_ARG, "null stepper");
+  if (h->s32) return s32_set_variant(h->s32, variant);
   pf5d_status st = configure_rate(h, variant);
   if (st != PF5D_OK) return st;
   for (auto &kv : h->graphs) cudaGraphExecDestroy(kv.second);
@@ -953,6 +1031,7 @@ pf5d_status pf5d_stepper_set_variant(pf5d_stepper *h, int32_t variant) {
 
 pf5d_status pf5d_stepper_launch_stage(pf5d_stepper *h, int32_t stage, void *stream) {
   PF5D_REQUIRE(h, PF5D_ERR_ARG, "null stepper");
+  if (h->s32) return s32_launch_stage(h->s32, stage, stream);
   cudaStream_t s = as_stream(stream);
   switch (stage) {
     case PF5D_STAGE_RATE:
@@ -978,6 +1057,8 @@ pf5d_status pf5d_stepper_launch_stage(pf5d_stepper *h, int32_t stage, void *stre
 
 pf5d_status pf5d_stepper_destroy(pf5d_stepper *h) {
   if (!h) return PF5D_OK;
+  if (h->s32) s32_destroy(h->s32);
+  cudaFree(h->mass_ws);
   for (auto &kv : h->graphs) cudaGraphExecDestroy(kv.second);
   fft_destroy(&h->fft);
   cudaFree(h->dX);

@@ -17,7 +17,11 @@ from . import _lib
 
 
 class Stepper:
-    """FP64 stepper for one solve.
+    """Stepper for one solve, in the plain FP64 form (bit-faithful to the
+    reference up to FFT rounding; advances ``X`` in place) or the
+    FP32-compensated form (``precision="fp32c"``: X - X0 as an FP32 hi/lo
+    pair, FP32 stencils/table/FFT, FP64 closure/sums/dt; read the field with
+    ``field()``).
 
     Parameters mirror the reference driver's state: dense table ``grid``
     (n,n,n,n,9) with its ``resolution`` and per-axis ``node_coord``; initial
@@ -29,7 +33,8 @@ class Stepper:
 
     def __init__(self, *, grid, resolution, node_coord, X, X0, kappa, dx, lvec, bk, ctld, t_cfl,
                  dt, adaptive=True, lower_limit=1e-5, upper_limit=1e-3, max_change_factor=2.0,
-                 oob_interval=100, max_nn_dist=None, stream=None, autotune=True):
+                 oob_interval=100, max_nn_dist=None, stream=None, autotune=True,
+                 precision="fp64"):
         import torch
         self._torch = torch
         self.L = _lib.load()
@@ -39,6 +44,9 @@ class Stepper:
         self.dim = len(self.shape)
         if self.dim not in (1, 2, 3):
             raise ValueError(f"Unsupported system_dim={self.dim}. Choose 1, 2, or 3.")
+        if precision not in ("fp64", "fp32c"):
+            raise ValueError(f"precision must be 'fp64' or 'fp32c' (got {precision!r})")
+        self.precision = precision
         self.grid = device_table(grid, torch)
         self.node_coord = torch.from_numpy(np.ascontiguousarray(node_coord,
                                                                 dtype=np.float64)).cuda()
@@ -78,6 +86,14 @@ class Stepper:
         d.adaptive = 1 if adaptive else 0
         d.dt0 = float(dt)
         d.oob_interval = int(oob_interval)
+        d.precision = _lib.PRECISION_FP64 if precision == "fp64" else _lib.PRECISION_FP32C
+        if precision == "fp32c":
+            mu0 = reference_mu(grid, resolution, X0)
+            self.grid32 = device_table32(grid, mu0, torch)
+            d.grid32 = self.grid32.data_ptr()
+            d.node_stride32 = NODE_STRIDE32
+            for i in range(4):
+                d.mu0[i] = float(mu0[i])
         self.desc = d
         h = ctypes.c_void_p()
         _lib.check(self.L.pf5d_stepper_create(ctypes.byref(d), _lib.ptr(self.X), self._s(),
@@ -137,6 +153,19 @@ class Stepper:
     def set_variant(self, variant):
         _lib.check(self.L.pf5d_stepper_set_variant(self.h, int(variant)), "set_variant")
 
+    def field(self):
+        """Current field X as a (*shape, 4) float64 CUDA tensor (a copy)."""
+        out = self._torch.empty((*self.shape, 4), dtype=self._torch.float64, device="cuda")
+        _lib.check(self.L.pf5d_stepper_field(self.h, _lib.ptr(out), self._s()), "field")
+        return out
+
+    def mass(self):
+        """FP64 mean composition per component (the quantity the flux form
+        conserves; its change over a run is the mass drift)."""
+        ptr, keep = _lib.f64_array([0.0] * 4)
+        _lib.check(self.L.pf5d_stepper_mass(self.h, ptr, self._s()), "mass")
+        return np.array(list(keep))
+
     def launch_stage(self, stage):
         """Diagnostics: enqueue one stage of a step (``_lib.STAGE_*``) alone."""
         _lib.check(self.L.pf5d_stepper_launch_stage(self.h, int(stage), self._s()), "stage")
@@ -158,6 +187,26 @@ class Stepper:
 
 
 NODE_STRIDE = 10
+NODE_STRIDE32 = 12
+
+
+def reference_mu(grid, resolution, X0):
+    """mu(X0) from the FP64 table (quadrilinear, host): the shift the FP32
+    table subtracts so it stores small deviations."""
+    from .solver.table import host_table_eval
+    g = grid.cpu().numpy() if hasattr(grid, "cpu") else np.asarray(grid)
+    return host_table_eval(np.asarray(X0, dtype=np.float64)[None, :], g[..., :9], resolution)[0, :4]
+
+
+def device_table32(grid, mu0, torch):
+    """FP32 table, 12 floats per node (48-byte nodes, three float4 loads):
+    mu - mu0 (4), M (5), pad.  Absent nodes stay NaN."""
+    g = grid.cpu().numpy() if hasattr(grid, "cpu") else np.asarray(grid)
+    g = g[..., :9].astype(np.float64)
+    out = np.zeros((*g.shape[:-1], NODE_STRIDE32), dtype=np.float32)
+    out[..., :4] = (g[..., :4] - np.asarray(mu0, dtype=np.float64)).astype(np.float32)
+    out[..., 4:9] = g[..., 4:9].astype(np.float32)
+    return torch.from_numpy(out).cuda()
 
 
 def device_table(grid, torch):

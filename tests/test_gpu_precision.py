@@ -1,0 +1,102 @@
+"""FP32-compensated form against the plain FP64 form on the GPU.
+
+Tolerance (stated by the precision target): max |X_fp32c - X_fp64| <=
+1e-6 * max |X_fp64| after N steps; the mass drift of the compensated form
+stays at FP64-accumulation level (<= 1e-12 in the mean composition).
+"""
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+FIELD_RTOL_FP32C = 1e-6
+MASS_DRIFT_TOL = 1e-12
+
+
+@pytest.fixture(scope="module")
+def torch_cuda():
+    import torch
+    if not torch.cuda.is_available():
+        pytest.skip("no CUDA device")
+    return torch
+
+
+def _check(rep):
+    assert not rep["halted"], rep
+    assert rep["max_rel_err_X"] <= FIELD_RTOL_FP32C, rep
+    assert max(abs(v) for v in rep["mass_drift_fp32c"]) <= MASS_DRIFT_TOL, rep
+
+
+def test_fp32c_2d_512_vs_fp64(torch_cuda):
+    from phasefield5d_b200 import workload as W
+    from phasefield5d_b200.precision import compare_forms
+    rep = compare_forms(W.build_problem(W.config_2d_adaptive()), 2000)
+    _check(rep)
+
+
+def test_fp32c_1d_1280_fixed_dt_vs_fp64(torch_cuda):
+    from phasefield5d_b200 import workload as W
+    from phasefield5d_b200.precision import compare_forms
+    rep = compare_forms(W.build_problem(W.config_1d_fixed()), 10_000)
+    _check(rep)
+    assert rep["time_fp32c"] == rep["time_fp64"]      # fixed dt: identical clocks
+
+
+def test_fp32c_3d_64_vs_fp64(torch_cuda):
+    from phasefield5d_b200 import workload as W
+    from phasefield5d_b200.precision import compare_forms
+    cfg = W.config_3d_precision()
+    cfg.shape = (64, 64, 64)
+    rep = compare_forms(W.build_problem(cfg), 500)
+    _check(rep)
+
+
+def test_fp32c_variants_bitwise_identical(torch_cuda):
+    from phasefield5d_b200 import workload as W
+    from phasefield5d_b200.stepper import Stepper
+    for dim, shape in [(2, (40, 70)), (3, (12, 20, 36))]:
+        cfg = W.SolveConfig(system_dim=dim, initial_composition=(0.1, 0.2, 0.2, 0.25),
+                            resolution=0.05, kappa_value=5e-16, mw=4, ppw=16, shape=shape,
+                            adaptive=True, n_k=2000, fluctuation=2e-2)
+        prob = W.build_problem(cfg)
+        ref = None
+        for v in range(6):
+            st = Stepper.from_problem(prob, autotune=False, precision="fp32c")
+            st.set_variant(v)
+            st.run(7)
+            X = st.field().cpu().numpy()
+            st.close()
+            if ref is None:
+                ref = X
+            assert np.array_equal(X, ref), (dim, v)
+
+
+def test_fp32c_out_of_bounds_halts(torch_cuda):
+    from phasefield5d_b200 import workload as W
+    from phasefield5d_b200.stepper import Stepper
+    cfg = W.SolveConfig(system_dim=1, initial_composition=(0.1, 0.2, 0.2, 0.25), resolution=0.05,
+                        kappa_value=5e-16, mw=4, ppw=16, shape=(64,), adaptive=True, n_k=2000)
+    prob = W.build_problem(cfg)
+    X = prob.X_init.copy()
+    X[9, 1] = -0.01
+    prob.X_init = X
+    st = Stepper.from_problem(prob, precision="fp32c")
+    state = st.run(50)
+    assert state["halted"] and state["step"] == 0
+    st.close()
+
+
+def test_fp32c_nearest_row_fallback(torch_cuda):
+    """Points beyond the linear-region threshold take the FP32 table's
+    nearest row; the run still tracks FP64 within the tolerance."""
+    from phasefield5d_b200 import workload as W
+    from phasefield5d_b200.precision import compare_forms
+    cfg = W.SolveConfig(system_dim=2, initial_composition=(0.1, 0.2, 0.2, 0.25), resolution=0.05,
+                        kappa_value=5e-16, mw=4, ppw=16, shape=(24, 20), adaptive=True, n_k=2000)
+    prob = W.build_problem(cfg)
+    rng = np.random.default_rng(11)
+    X = prob.X_init.copy()
+    X[..., 3] += rng.uniform(0.0, 0.1, size=X.shape[:-1])
+    prob.X_init = X
+    rep = compare_forms(prob, 30)
+    assert rep["max_rel_err_X"] <= FIELD_RTOL_FP32C, rep
