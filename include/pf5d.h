@@ -234,6 +234,46 @@ pf5d_status pf5d_stepper_set_variant(pf5d_stepper *h, int32_t variant);
 pf5d_status pf5d_stepper_reset(pf5d_stepper *h, double dt, double time, void *stream);
 pf5d_status pf5d_stepper_destroy(pf5d_stepper *h);
 
+/* ------------------------------------------------------- batched form -----
+ * Many independent FP32-compensated 1D/2D solves advanced together: one
+ * persistent rate launch over the tiles of all solves, one compensated-update
+ * launch, cuFFT plans batched per 2D shape; each solve keeps its own
+ * adaptive dt.  This replaces the reference's one-process-per-solve sweeps
+ * (run/launch.py:119-150) with one device-resident batch. */
+typedef struct {
+  int32_t dim;                 /* 1 or 2                                      */
+  int64_t shape[2];
+  double dx;
+  double kappa[4];
+  double x0[4];
+  int32_t elastic;
+  double lvec[4];
+  const double *bk;            /* host B(k) on the rfft half-grid            */
+  int32_t table;               /* index into the batch's FP32 tables         */
+  double max_nn_dist;
+  double ctld, t_cfl, lower_limit, upper_limit, max_change_factor;
+  int32_t adaptive;
+  double dt0;
+  int32_t oob_interval;
+  const double *X;             /* device (*shape, 4) float64 initial field   */
+} pf5d_batch_solve;
+
+typedef struct pf5d_batch pf5d_batch;
+
+/* tables32: device FP32 tables (12 floats per node: mu - mu_ref (4), M (5),
+ * pad), all with table_n nodes per axis and the given resolution. */
+pf5d_status pf5d_batch_create(const pf5d_batch_solve *solves, int32_t nsolves,
+                              const float *const *tables32, int32_t ntables, int32_t table_n,
+                              double resolution, const double *node_coord, void *stream,
+                              pf5d_batch **out);
+pf5d_status pf5d_batch_advance(pf5d_batch *h, int64_t nsteps, void *stream);
+/* out: nsolves entries; synchronises `stream`. */
+pf5d_status pf5d_batch_states(pf5d_batch *h, pf5d_step_state *out, void *stream);
+pf5d_status pf5d_batch_field(pf5d_batch *h, int32_t i, double *X_out, void *stream);
+pf5d_status pf5d_batch_autotune(pf5d_batch *h, int32_t *variant, float *best_ms, void *stream);
+pf5d_status pf5d_batch_set_variant(pf5d_batch *h, int32_t variant);
+pf5d_status pf5d_batch_destroy(pf5d_batch *h);
+
 #if defined(__GNUC__)
 #pragma GCC visibility pop
 #endif

@@ -55,6 +55,17 @@ class StepperDesc(ctypes.Structure):
     ]
 
 
+class BatchSolve(ctypes.Structure):
+    """pf5d_batch_solve (include/pf5d.h)."""
+    _fields_ = [
+        ("dim", _i32), ("shape", _i64 * 2), ("dx", _f64), ("kappa", _f64 * 4), ("x0", _f64 * 4),
+        ("elastic", _i32), ("lvec", _f64 * 4), ("bk", _f64p), ("table", _i32),
+        ("max_nn_dist", _f64), ("ctld", _f64), ("t_cfl", _f64), ("lower_limit", _f64),
+        ("upper_limit", _f64), ("max_change_factor", _f64), ("adaptive", _i32), ("dt0", _f64),
+        ("oob_interval", _i32), ("X", _vp),
+    ]
+
+
 class StepState(ctypes.Structure):
     """pf5d_step_state (include/pf5d.h)."""
     _fields_ = [("dt", _f64), ("time", _f64), ("xdotmax", _f64), ("step", _i64),
@@ -93,6 +104,15 @@ _SIGS = {
     "pf5d_stepper_set_variant": (_i32, [_vp, _i32]),
     "pf5d_stepper_reset": (_i32, [_vp, _f64, _f64, _vp]),
     "pf5d_stepper_destroy": (_i32, [_vp]),
+    "pf5d_batch_create": (_i32, [ctypes.POINTER(BatchSolve), _i32, ctypes.POINTER(_vp), _i32,
+                                 _i32, _f64, _vp, _vp, ctypes.POINTER(_vp)]),
+    "pf5d_batch_advance": (_i32, [_vp, _i64, _vp]),
+    "pf5d_batch_states": (_i32, [_vp, ctypes.POINTER(StepState), _vp]),
+    "pf5d_batch_field": (_i32, [_vp, _i32, _vp, _vp]),
+    "pf5d_batch_autotune": (_i32, [_vp, ctypes.POINTER(_i32), ctypes.POINTER(ctypes.c_float),
+                                   _vp]),
+    "pf5d_batch_set_variant": (_i32, [_vp, _i32]),
+    "pf5d_batch_destroy": (_i32, [_vp]),
 }
 
 _lib = None

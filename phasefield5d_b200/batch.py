@@ -1,0 +1,137 @@
+"""Batched form: many independent FP32-compensated 1D/2D solves advanced
+together by the batched CUDA stepper (``pf5d_batch_*``).
+
+This is the in-process replacement for the reference's one-process-per-solve
+parameter sweeps (run/launch.py:119-150): every solve of the batch shares
+each launch of a step, keeps its own adaptive dt, and reads one of a few
+temperature tables resident in HBM.
+"""
+from __future__ import annotations
+
+import ctypes
+
+import numpy as np
+
+from . import _lib
+from .solver.table import host_table_eval
+from .stepper import NODE_STRIDE32
+
+
+def _table32(grid, mu_ref, torch):
+    g = np.asarray(grid)[..., :9].astype(np.float64)
+    out = np.zeros((*g.shape[:-1], NODE_STRIDE32), dtype=np.float32)
+    out[..., :4] = (g[..., :4] - np.asarray(mu_ref)).astype(np.float32)
+    out[..., 4:9] = g[..., 4:9].astype(np.float32)
+    return torch.from_numpy(out).cuda()
+
+
+class BatchStepper:
+    """Advance a list of ``workload.Problem`` (1D/2D, same table resolution)
+    together.  Problems with the same temperature share one device table;
+    the FP32 table stores mu minus the mean mu(X0) of its solves."""
+
+    def __init__(self, problems, stream=None, autotune=True, oob_interval=100):
+        import torch
+        self._torch = torch
+        self.L = _lib.load()
+        self.stream = stream
+        self.problems = list(problems)
+        res = {p.cfg.resolution for p in self.problems}
+        if len(res) != 1:
+            raise ValueError("all solves of a batch must use one table resolution")
+        self.resolution = res.pop()
+        keys = []
+        for p in self.problems:
+            k = (p.cfg.temperature, p.table.seed)
+            if k not in keys:
+                keys.append(k)
+        self.table_keys = keys
+        self.tables = []
+        for k in keys:
+            members = [p for p in self.problems if (p.cfg.temperature, p.table.seed) == k]
+            grid = members[0].grid
+            mus = [host_table_eval(np.asarray(p.X0)[None, :], grid, self.resolution)[0, :4]
+                   for p in members]
+            self.tables.append(_table32(grid, np.mean(mus, axis=0), torch))
+        self.node_coord = torch.from_numpy(np.ascontiguousarray(self.problems[0].node_coord)).cuda()
+        self.X_init = [torch.from_numpy(np.ascontiguousarray(p.X_init)).cuda() for p in self.problems]
+        self._bk = []
+        arr = (_lib.BatchSolve * len(self.problems))()
+        for i, p in enumerate(self.problems):
+            q = arr[i]
+            q.dim = p.dim
+            for d in range(2):
+                q.shape[d] = p.shape[d] if d < p.dim else 1
+            q.dx = p.dx
+            kap = np.asarray(p.kappa, dtype=np.float64).reshape(-1)
+            elastic = p.lvec is not None and p.bk is not None
+            for c in range(4):
+                q.kappa[c] = float(kap[c])
+                q.x0[c] = float(p.X0[c])
+                q.lvec[c] = float(p.lvec[c]) if elastic else 0.0
+            q.elastic = 1 if elastic else 0
+            if elastic:
+                bk = np.ascontiguousarray(p.bk, dtype=np.float64)
+                self._bk.append(bk)
+                q.bk = bk.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
+            q.table = keys.index((p.cfg.temperature, p.table.seed))
+            q.max_nn_dist = -1.0
+            q.ctld, q.t_cfl = p.ctld, p.t_cfl
+            q.lower_limit, q.upper_limit = p.cfg.lower_limit, p.cfg.upper_limit
+            q.max_change_factor = 2.0
+            q.adaptive = 1 if p.cfg.adaptive else 0
+            q.dt0 = p.dt0
+            q.oob_interval = int(oob_interval)
+            q.X = self.X_init[i].data_ptr()
+        tabs = (ctypes.c_void_p * len(self.tables))(*[t.data_ptr() for t in self.tables])
+        h = ctypes.c_void_p()
+        _lib.check(self.L.pf5d_batch_create(arr, len(self.problems), tabs, len(self.tables),
+                                            int(self.problems[0].grid.shape[0]), self.resolution,
+                                            _lib.ptr(self.node_coord), self._s(), ctypes.byref(h)),
+                   "BatchStepper")
+        self.h = h
+        self._arr = arr
+        self.variant, self.tuned_ms = (self.autotune() if autotune else (0, None))
+
+    def _s(self):
+        return _lib.stream_handle(self.stream)
+
+    @property
+    def n_points(self):
+        return int(sum(p.n_points for p in self.problems))
+
+    def advance(self, n_steps):
+        _lib.check(self.L.pf5d_batch_advance(self.h, int(n_steps), self._s()), "advance")
+
+    def states(self):
+        out = (_lib.StepState * len(self.problems))()
+        _lib.check(self.L.pf5d_batch_states(self.h, out, self._s()), "states")
+        return [dict(dt=s.dt, time=s.time, xdotmax=s.xdotmax, step=int(s.step),
+                     flags=int(s.flags), halted=bool(s.halted)) for s in out]
+
+    def field(self, i):
+        p = self.problems[i]
+        out = self._torch.empty((*p.shape, 4), dtype=self._torch.float64, device="cuda")
+        _lib.check(self.L.pf5d_batch_field(self.h, int(i), _lib.ptr(out), self._s()), "field")
+        return out
+
+    def autotune(self):
+        v = ctypes.c_int32()
+        ms = ctypes.c_float()
+        _lib.check(self.L.pf5d_batch_autotune(self.h, ctypes.byref(v), ctypes.byref(ms), self._s()),
+                   "autotune")
+        return int(v.value), float(ms.value)
+
+    def set_variant(self, v):
+        _lib.check(self.L.pf5d_batch_set_variant(self.h, int(v)), "set_variant")
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.L.pf5d_batch_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

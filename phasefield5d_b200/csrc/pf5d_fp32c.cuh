@@ -1,0 +1,451 @@
+// pf5d_fp32c.cuh -- device numerics of the FP32-compensated form, shared by
+// the single-solve stepper (precision.cu) and the batched stepper
+// (batch.cu): step state, FP32 table view and per-solve parameters, cell /
+// interpolation / face-flux routines, the per-plane mu evaluation with the
+// shared table window, and the compensated-update helpers.
+#pragma once
+
+#include <climits>
+
+#include <cufft.h>
+
+#include "pf5d_device.cuh"
+#include "pf5d_tiles.cuh"
+#include "pf5d_window.cuh"
+
+namespace pf5d {
+
+struct StepState32 {
+  double dt;
+  double time;
+  double xdotmax;
+  double xacc;
+  unsigned blocks_done;
+  unsigned flags;
+  unsigned halt;
+  unsigned pad;
+  long long step;
+};
+
+constexpr int kStride32 = 12;   // floats per FP32 table node (9 props + 3 pad = 48 bytes)
+
+struct Table32 {
+  const float *grid;
+  const double *coord;
+  int n;
+  int stride;
+  double inv_step, threshold, exact_d2, max_nn_dist;
+  float inv_step_f;
+  int ib[S];          // floor(X0_d / res)
+  float fb[S];        // X0_d / res - floor(X0_d / res)
+  double x0[S];
+  double sum_x0;
+};
+
+struct Rate32 {
+  int nz, ny, nx;
+  const float4 *D;     // hi part of X - X0
+  const float *sp;     // s' scaled by 1/N, or nullptr
+  float4 *dX;
+  Table32 T;
+  float kappa[S], lvec[S], x0f[S];
+  double c_fe;         // 1 - sum X0
+  float inv_dx, inv_dx2;
+  double ctld, t_cfl, lower, upper, factor;
+  int adaptive;
+  StepState32 *st;
+};
+
+// ------------------------------------------------------------------------
+// Device numerics
+// ------------------------------------------------------------------------
+
+// Table cell and fractional coordinates of X = X0 + d (interpolation.py:103-121
+// clamping).  Returns false when the point is outside the linear region
+// (sum X > 1 - 4 res - 1e-9, tested in FP64) and takes the nearest-row path.
+__device__ __forceinline__ bool cell32(const Table32 &T, const float d[S], int ii[S], float tt[S]) {
+  const double sd = (((double)d[0] + (double)d[1]) + (double)d[2]) + (double)d[3];
+  if (!(T.sum_x0 + sd <= T.threshold)) return false;
+#pragma unroll
+  for (int a = 0; a < S; ++a) {
+    const float v = fmaf(d[a], T.inv_step_f, T.fb[a]);
+    const float k = floorf(v);
+    int i = T.ib[a] + (int)k;
+    float t = v - k;
+    if (i < 0) {
+      i = 0;
+      t = 0.f;
+    } else if (i > T.n - 2) {
+      i = T.n - 2;
+      t = 1.f;
+    }
+    ii[a] = i;
+    tt[a] = t;
+  }
+  return true;
+}
+
+// Quadrilinear interpolation of the 9 props from 16 corner nodes laid out
+// with node strides (s0, s1, s2, s3) in float4 units from `base` (global
+// table or shared window; 3 float4 per node).
+__device__ __forceinline__ void interp_nodes32(const float4 *base, int s0, int s1, int s2, int s3,
+                                               const float tt[S], float out[NP]) {
+  const float q0 = 1.f - tt[0], q1 = 1.f - tt[1], q2 = 1.f - tt[2], q3 = 1.f - tt[3];
+#pragma unroll
+  for (int c = 0; c < 16; ++c) {
+    const int b0 = (c >> 3) & 1, b1 = (c >> 2) & 1, b2 = (c >> 1) & 1, b3 = c & 1;
+    const float w = (b0 ? tt[0] : q0) * (b1 ? tt[1] : q1) * (b2 ? tt[2] : q2) * (b3 ? tt[3] : q3);
+    const float4 *node = base + b0 * s0 + b1 * s1 + b2 * s2 + b3 * s3;
+    const float4 a = node[0], b = node[1], e = node[2];
+    const float v[NP] = {a.x, a.y, a.z, a.w, b.x, b.y, b.z, b.w, e.x};
+#pragma unroll
+    for (int p = 0; p < NP; ++p) out[p] = (c == 0) ? w * v[p] : fmaf(w, v[p], out[p]);
+  }
+}
+
+constexpr int kWin32 = 4;                       // window nodes per axis (3 cells)
+constexpr int kWinNodes32 = kWin32 * kWin32 * kWin32 * kWin32;
+
+// Table value at X0 + d: from the shared window `win` when the point's cell
+// fits in it (win_lo = box origin), else from the global table; nearest row
+// outside the linear region.
+__device__ __forceinline__ void interp32(const Rate32 &P, const float d[S], const float4 *win,
+                                         const int *win_lo, float out[NP], unsigned *flags) {
+  const Table32 &T = P.T;
+  int ii[S];
+  float tt[S];
+  if (cell32(T, d, ii, tt)) {
+    const int off = win ? window_cell<kWin32>(ii, win_lo) : -1;
+    if (off >= 0) {
+      constexpr int w3 = 3, w2 = kWin32 * w3, w1 = kWin32 * w2, w0 = kWin32 * w1;
+      interp_nodes32(win + off * 3, w0, w1, w2, w3, tt, out);
+    } else {
+      const int s3 = 3, s2 = T.n * s3, s1 = T.n * s2;
+      const int64_t s0 = (int64_t)T.n * s1;
+      const float4 *g = reinterpret_cast<const float4 *>(T.grid);
+      interp_nodes32(g + ii[0] * s0 + (int64_t)ii[1] * s1 + (int64_t)ii[2] * s2 + ii[3] * s3,
+                     (int)s0, s1, s2, s3, tt, out);
+    }
+    return;
+  }
+  const NearestNode r = nearest_node_g<float>(T.grid, T.stride, T.coord, T.n, T.inv_step,
+                                              T.exact_d2, T.max_nn_dist, T.x0[0] + (double)d[0],
+                                              T.x0[1] + (double)d[1], T.x0[2] + (double)d[2],
+                                              T.x0[3] + (double)d[3]);
+  *flags |= r.flags;
+  const float *row = T.grid + (r.node < 0 ? 0 : r.node) * T.stride;
+#pragma unroll
+  for (int p = 0; p < NP; ++p) out[p] = r.node < 0 ? __int_as_float(0x7fc00000) : __ldg(row + p);
+}
+
+// mu (relative to mu(X0)) and M at one point.
+__device__ __forceinline__ void chem32(const Rate32 &P, const float d[S], const float lap[S],
+                                       float spv, const float4 *win, const int *win_lo,
+                                       float mu[S], float M[NM], unsigned *flags) {
+  float v[NP];
+  interp32(P, d, win, win_lo, v, flags);
+#pragma unroll
+  for (int c = 0; c < S; ++c) {
+    float m = fmaf(-lap[c], P.kappa[c], v[c]);
+    if (P.sp) m = fmaf(spv, P.lvec[c], m);
+    mu[c] = m;
+  }
+#pragma unroll
+  for (int c = 0; c < NM; ++c) M[c] = v[S + c];
+}
+
+// Face flux (phasefield5d/solver/fluxes.py:128-160) in FP32 with the FP64
+// closure X_Fe = (1 - sum X0) - sum Dmid.
+__device__ __forceinline__ void face_flux32(const Rate32 &P, const float Dc[S], const float Mc[NM],
+                                            const float Dn[S], const float Mn[NM],
+                                            const float g[S], float J[S]) {
+  float dm[S], xm[S], mm[NM], dk[S];
+#pragma unroll
+  for (int a = 0; a < S; ++a) {
+    dm[a] = 0.5f * (Dc[a] + Dn[a]);
+    xm[a] = P.x0f[a] + dm[a];
+  }
+#pragma unroll
+  for (int a = 0; a < NM; ++a) mm[a] = 0.5f * (Mc[a] + Mn[a]);
+  const double x_fe = P.c_fe - (((double)dm[0] + (double)dm[1]) + (double)dm[2] + (double)dm[3]);
+  const float w_fe = (float)x_fe * mm[0];
+  float dot = 0.f;
+#pragma unroll
+  for (int b = 0; b < S; ++b) dot = fmaf(xm[b], g[b], dot);
+#pragma unroll
+  for (int k = 0; k < S; ++k) dk[k] = g[k] - dot;
+  float swk = 0.f;
+#pragma unroll
+  for (int k = 0; k < S; ++k) swk = fmaf(xm[k] * mm[1 + k], dk[k], swk);
+#pragma unroll
+  for (int a = 0; a < S; ++a) J[a] = w_fe * xm[a] * dot + xm[a] * mm[1 + a] * dk[a] - xm[a] * swk;
+}
+
+// Fold this thread's max |dX/dt| into the block and the solve's device
+// accumulator; the block completing the solve's `total` tiles runs the FP64
+// dt controller and advances dt / time / step.
+__device__ __forceinline__ void finish_tiles32(const Rate32 &P, float m32, double *red,
+                                               unsigned total) {
+  double m = (double)m32;
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
+  const int tid = threadIdx.y * blockDim.x + threadIdx.x;
+  const int nw = (blockDim.x * blockDim.y + 31) >> 5;
+  __syncthreads();
+  if ((tid & 31) == 0) red[tid >> 5] = m;
+  __syncthreads();
+  if (tid == 0) {
+    for (int w = 1; w < nw; ++w) m = fmax(m, red[w]);
+    StepState32 *st = P.st;
+    atomic_max_nonneg(&st->xacc, m);
+    __threadfence();
+    if (atomicAdd(&st->blocks_done, 1u) == total - 1) {
+      __threadfence();
+      const double xmax = __longlong_as_double(
+          (long long)atomicAdd(reinterpret_cast<unsigned long long *>(&st->xacc), 0ULL));
+      double dt = st->dt;
+      if (P.adaptive) dt = adaptive_dt(dt, xmax, P.ctld, P.t_cfl, P.lower, P.upper, P.factor);
+      st->dt = dt;
+      st->time = st->time + dt;
+      st->xdotmax = xmax;
+      st->step = st->step + 1;
+      st->xacc = 0.0;
+      st->blocks_done = 0;
+    }
+  }
+}
+
+__device__ __forceinline__ void finish_rate32(const Rate32 &P, float m32, double *red) {
+  finish_tiles32(P, m32, red, gridDim.x * gridDim.y * gridDim.z);
+}
+
+template <int PX, int PM>
+__device__ __forceinline__ void face32_between(const Rate32 &P, const float *XL, const float *ML,
+                                               int pl, int ql, const float *XH, const float *MH,
+                                               int ph, int qh, float J[S]) {
+  float Dc[S], Dn[S], Mc[NM], Mn[NM], g[S];
+#pragma unroll
+  for (int c = 0; c < S; ++c) {
+    Dc[c] = XL[c * PX + pl];
+    Dn[c] = XH[c * PX + ph];
+    g[c] = (MH[c * PM + qh] - ML[c * PM + ql]) * P.inv_dx;
+  }
+#pragma unroll
+  for (int c = 0; c < NM; ++c) {
+    Mc[c] = ML[(S + c) * PM + ql];
+    Mn[c] = MH[(S + c) * PM + qh];
+  }
+  face_flux32(P, Dc, Mc, Dn, Mn, g, J);
+}
+
+template <int TX, int TY>
+__device__ __forceinline__ void plane_faces32(const Rate32 &P, const float *Xp, const float *Mp,
+                                              float *Fx, float *Fy, int tid) {
+  using G = PlaneGeom<TX, TY>;
+  for (int f = tid; f < G::NFX + G::NFY; f += G::NT) {
+    float J[S];
+    if (f < G::NFX) {
+      const int fy = f / (TX + 1), fx = f - fy * (TX + 1);
+      const int pl = (fy + 2) * G::HX + (fx + 1), ql = (fy + 1) * G::MX + fx;
+      face32_between<G::PX, G::PM>(P, Xp, Mp, pl, ql, Xp, Mp, pl + 1, ql + 1, J);
+#pragma unroll
+      for (int c = 0; c < S; ++c) Fx[c * G::NFX + f] = J[c];
+    } else {
+      const int f2 = f - G::NFX;
+      const int fy = f2 / TX, fx = f2 - fy * TX;
+      const int pl = (fy + 1) * G::HX + (fx + 2), ql = fy * G::MX + (fx + 1);
+      face32_between<G::PX, G::PM>(P, Xp, Mp, pl, ql, Xp, Mp, pl + G::HX, ql + G::MX, J);
+#pragma unroll
+      for (int c = 0; c < S; ++c) Fy[c * G::NFY + f2] = J[c];
+    }
+  }
+}
+
+template <int TX, int TY>
+__device__ __forceinline__ void load_plane32(const float4 *__restrict__ D, int64_t plane_off,
+                                             const int *wx, const int *wy, int nx, float *dst,
+                                             int tid) {
+  using G = PlaneGeom<TX, TY>;
+  for (int pos = tid; pos < G::PX; pos += G::NT) {
+    const int hy = pos / G::HX, hx = pos - hy * G::HX;
+    const float4 v = __ldg(D + plane_off + (int64_t)wy[hy] * nx + wx[hx]);
+    dst[0 * G::PX + pos] = v.x;
+    dst[1 * G::PX + pos] = v.y;
+    dst[2 * G::PX + pos] = v.z;
+    dst[3 * G::PX + pos] = v.w;
+  }
+}
+
+__device__ __forceinline__ void store_rate(float4 *dX, int64_t g, const float out[S], float &vmax) {
+#pragma unroll
+  for (int c = 0; c < S; ++c) vmax = fmaxf(vmax, fabsf(out[c]));
+  dX[g] = make_float4(out[0], out[1], out[2], out[3]);
+}
+
+
+// Skip test for mu/M positions: corners of the halo ring are never used;
+// interior_only keeps the tile positions only.
+template <int MX, int MY>
+__device__ __forceinline__ bool skip_pos(int mx, int my, bool interior_only) {
+  const bool ex = (mx == 0 || mx == MX - 1), ey = (my == 0 || my == MY - 1);
+  return interior_only ? (ex || ey) : (ex && ey);
+}
+
+// mu/M of one plane (tile + 1-cell halo, or the tile only) into dst.  Xm/Xp
+// are the neighbouring planes along axis 0 in 3D (nullptr in 2D, where the
+// y-neighbours sit in the same plane).  Stages the table window first.
+template <int TX, int TY, int DIM, bool WIN>
+__device__ __forceinline__ void mu_plane32(const Rate32 &P, const float *Xm, const float *Xc,
+                                           const float *Xp, float *dst, int64_t zoff,
+                                           const int *wx, const int *wy, bool interior_only,
+                                           float4 *win, int *red, int *win_lo, unsigned *flags,
+                                           int tid) {
+  using G = PlaneGeom<TX, TY>;
+  // 1. table window around the tile centre's cell (reloaded if it moved).
+  int rep[S];
+  float tr[S];
+  float dc[S];
+  const int cp = (TY / 2 + 2) * G::HX + (TX / 2 + 2);
+#pragma unroll
+  for (int c = 0; c < S; ++c) dc[c] = Xc[c * G::PX + cp];
+  const bool use_win = WIN && cell32(P.T, dc, rep, tr);
+  int o[S] = {0, 0, 0, 0};
+  if (use_win) {
+    window_origin<kWin32>(rep, tr, o);
+    ensure_window<kWin32, 3, float4, G::NT>(reinterpret_cast<const float4 *>(P.T.grid), P.T.n, o,
+                                            win, win_lo, tid);
+  }
+  // 2. interpolation + Laplacian + mu assembly.
+  for (int pos = tid; pos < G::PM; pos += G::NT) {
+    const int my = pos / G::MX, mx = pos - my * G::MX;
+    if (skip_pos<G::MX, G::MY>(mx, my, interior_only)) continue;
+    const int px = (my + 1) * G::HX + (mx + 1);
+    float d[S], lap[S];
+#pragma unroll
+    for (int c = 0; c < S; ++c) {
+      const float *q = Xc + c * G::PX;
+      d[c] = q[px];
+      if (DIM == 3)
+        lap[c] = (Xp[c * G::PX + px] + Xm[c * G::PX + px] + q[px + G::HX] + q[px - G::HX] +
+                  q[px + 1] + q[px - 1] - 6.f * d[c]) * P.inv_dx2;
+      else
+        lap[c] = (q[px + G::HX] + q[px - G::HX] + q[px + 1] + q[px - 1] - 4.f * d[c]) * P.inv_dx2;
+    }
+    const float spv = P.sp ? __ldg(P.sp + zoff + (int64_t)wy[my + 1] * P.nx + wx[mx + 1]) : 0.f;
+    float mu[S], M[NM];
+    chem32(P, d, lap, spv, use_win ? win : nullptr, o, mu, M, flags);
+#pragma unroll
+    for (int c = 0; c < S; ++c) dst[c * G::PM + pos] = mu[c];
+#pragma unroll
+    for (int c = 0; c < NM; ++c) dst[(S + c) * G::PM + pos] = M[c];
+  }
+}
+
+// Shared memory common to the plane kernels, after the kernel-specific
+// arrays: block-max scratch (double), the table window (float4), window
+// reduction scratch and origin (int), halo index tables (int).
+template <int TX, int TY>
+struct Smem32Tail {
+  using G = PlaneGeom<TX, TY>;
+  static constexpr size_t bytes = (G::NT / 32) * sizeof(double) + kWinNodes32 * 3 * sizeof(float4) +
+                                  (S * (G::NT / 32) + S + 1) * sizeof(int) +
+                                  (G::HX + G::HY) * sizeof(int);
+};
+
+
+// (h, l) += inc with TwoSum and renormalisation; explicit _rn intrinsics keep
+// every operation separately rounded.
+__device__ __forceinline__ void comp_add(float &h, float &l, float inc) {
+  const float s = __fadd_rn(h, inc);
+  const float bb = __fsub_rn(s, h);
+  const float err = __fadd_rn(__fsub_rn(h, __fsub_rn(s, bb)), __fsub_rn(inc, bb));
+  const float lo = __fadd_rn(l, err);
+  const float hn = __fadd_rn(s, lo);
+  l = __fsub_rn(lo, __fsub_rn(hn, s));
+  h = hn;
+}
+
+__device__ __forceinline__ unsigned oob_flags_x(const double x[S]) {
+  unsigned f = 0;
+  double sum = 0.0;
+#pragma unroll
+  for (int c = 0; c < S; ++c) {
+    if (!isfinite(x[c])) f |= PF5D_FLAG_NONFINITE;
+    sum = sum + x[c];
+    if (x[c] < 0.0 - 1e-3 || x[c] > 1.0 + 1e-3) f |= PF5D_FLAG_OOB_HARD;
+    if (x[c] < 0.0 - 1e-5 || x[c] > 1.0 + 1e-5) f |= PF5D_FLAG_OOB_SOFT;
+  }
+  if (sum > 1.0 + 1e-3 || sum < 0.0 - 1e-3) f |= PF5D_FLAG_OOB_HARD;
+  if (sum > 1.0 + 1e-5 || sum < 0.0 - 1e-5) f |= PF5D_FLAG_OOB_SOFT;
+  return f;
+}
+
+__device__ __forceinline__ void raise32(StepState32 *st, unsigned f) {
+  if (!f) return;
+  atomicOr(&st->flags, f);
+  if (f & (PF5D_FLAG_NONFINITE | PF5D_FLAG_OOB_HARD)) atomicExch(&st->halt, 1u);
+}
+
+
+// ------------------------------------------------------------------------
+// One 2D plane tile of a solve (shared by the single-solve and batched
+// kernels).  Shared-memory layout, in order: table window, block-max
+// scratch, X (tile + 2 halo), mu/M (tile + 1 halo), x- and y-face fluxes,
+// window scratch/origin, halo index tables.
+// ------------------------------------------------------------------------
+template <int TX, int TY>
+struct Tile2dSmem32 {
+  using G = PlaneGeom<TX, TY>;
+  static constexpr size_t bytes = Smem32Tail<TX, TY>::bytes +
+      (S * G::PX + NP * G::PM + S * G::NFX + S * G::NFY) * sizeof(float);
+  static __device__ __forceinline__ double *red(float4 *sm4) {
+    return reinterpret_cast<double *>(sm4 + kWinNodes32 * 3);
+  }
+};
+
+// Evaluates tile (bx, by) of solve P and writes its dX/dt; returns this
+// thread's max |dX/dt|.  Ends with all threads past a barrier.
+template <int TX, int TY, bool WIN>
+__device__ __forceinline__ float tile2d32_body(const Rate32 &P, int bx, int by, float4 *sm4,
+                                               unsigned *flags, int tid) {
+  using G = PlaneGeom<TX, TY>;
+  float4 *win = sm4;
+  double *red = Tile2dSmem32<TX, TY>::red(sm4);
+  float *Xs = reinterpret_cast<float *>(red + G::NT / 32);
+  float *Ms = Xs + S * G::PX;
+  float *Fx = Ms + NP * G::PM;
+  float *Fy = Fx + S * G::NFX;
+  int *wred = reinterpret_cast<int *>(Fy + S * G::NFY);
+  int *win_lo = wred + S * (G::NT / 32);
+  int *wx = win_lo + S + 1;
+  int *wy = wx + G::HX;
+  const int tx = tid % TX, ty = tid / TX;
+  const int x0 = bx * TX, y0 = by * TY;
+  if (tid == 0) win_lo[S] = 0;
+  for (int i = tid; i < G::HX + G::HY; i += G::NT) {
+    if (i < G::HX) wx[i] = wrap_any(x0 + i - 2, P.nx);
+    else wy[i - G::HX] = wrap_any(y0 + (i - G::HX) - 2, P.ny);
+  }
+  __syncthreads();
+  load_plane32<TX, TY>(P.D, 0, wx, wy, P.nx, Xs, tid);
+  __syncthreads();
+  mu_plane32<TX, TY, 2, WIN>(P, nullptr, Xs, nullptr, Ms, 0, wx, wy, false, win, wred, win_lo,
+                             flags, tid);
+  __syncthreads();
+  plane_faces32<TX, TY>(P, Xs, Ms, Fx, Fy, tid);
+  __syncthreads();
+  float vmax = 0.f;
+  if (x0 + tx < P.nx && y0 + ty < P.ny) {
+    float out[S];
+#pragma unroll
+    for (int c = 0; c < S; ++c) {
+      const float a = (Fy[c * G::NFY + (ty + 1) * TX + tx] - Fy[c * G::NFY + ty * TX + tx]) +
+                      (Fx[c * G::NFX + ty * (TX + 1) + tx + 1] - Fx[c * G::NFX + ty * (TX + 1) + tx]);
+      out[c] = a * P.inv_dx;
+    }
+    store_rate(P.dX, (int64_t)(y0 + ty) * P.nx + (x0 + tx), out, vmax);
+  }
+  return vmax;
+}
+
+}  // namespace pf5d

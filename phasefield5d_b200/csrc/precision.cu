@@ -28,323 +28,47 @@
 
 #include "pf5d_device.cuh"
 #include "pf5d_fp32c.h"
+#include "pf5d_fp32c.cuh"
 #include "pf5d_host.h"
 #include "pf5d_tiles.cuh"
+#include "pf5d_window.cuh"
 
 namespace pf5d {
-
-struct StepState32 {
-  double dt;
-  double time;
-  double xdotmax;
-  double xacc;
-  unsigned blocks_done;
-  unsigned flags;
-  unsigned halt;
-  unsigned pad;
-  long long step;
-};
-
-constexpr int kStride32 = 12;   // floats per FP32 table node (9 props + 3 pad = 48 bytes)
-
-struct Table32 {
-  const float *grid;
-  const double *coord;
-  int n;
-  int stride;
-  double inv_step, threshold, exact_d2, max_nn_dist;
-  float inv_step_f;
-  int ib[S];          // floor(X0_d / res)
-  float fb[S];        // X0_d / res - floor(X0_d / res)
-  double x0[S];
-  double sum_x0;
-};
-
-struct Rate32 {
-  int nz, ny, nx;
-  const float4 *D;     // hi part of X - X0
-  const float *sp;     // s' scaled by 1/N, or nullptr
-  float4 *dX;
-  Table32 T;
-  float kappa[S], lvec[S], x0f[S];
-  double c_fe;         // 1 - sum X0
-  float inv_dx, inv_dx2;
-  double ctld, t_cfl, lower, upper, factor;
-  int adaptive;
-  StepState32 *st;
-};
-
-// ------------------------------------------------------------------------
-// Device numerics
-// ------------------------------------------------------------------------
-
-__device__ __forceinline__ void interp32(const Rate32 &P, const float d[S], float out[NP],
-                                         unsigned *flags) {
-  const Table32 &T = P.T;
-  const double sd = (((double)d[0] + (double)d[1]) + (double)d[2]) + (double)d[3];
-  if (T.sum_x0 + sd <= T.threshold) {
-    int ii[S];
-    float tt[S];
-#pragma unroll
-    for (int a = 0; a < S; ++a) {
-      const float v = fmaf(d[a], T.inv_step_f, T.fb[a]);
-      const float k = floorf(v);
-      int i = T.ib[a] + (int)k;
-      float t = v - k;
-      if (i < 0) {
-        i = 0;
-        t = 0.f;
-      } else if (i > T.n - 2) {
-        i = T.n - 2;
-        t = 1.f;
-      }
-      ii[a] = i;
-      tt[a] = t;
-    }
-    const float q0 = 1.f - tt[0], q1 = 1.f - tt[1], q2 = 1.f - tt[2], q3 = 1.f - tt[3];
-    const int64_t s3 = T.stride, s2 = (int64_t)T.n * s3, s1 = (int64_t)T.n * s2,
-                  s0 = (int64_t)T.n * s1;
-    const float *base = T.grid + ii[0] * s0 + ii[1] * s1 + ii[2] * s2 + ii[3] * s3;
-#pragma unroll
-    for (int c = 0; c < 16; ++c) {
-      const int b0 = (c >> 3) & 1, b1 = (c >> 2) & 1, b2 = (c >> 1) & 1, b3 = c & 1;
-      const float w = (b0 ? tt[0] : q0) * (b1 ? tt[1] : q1) * (b2 ? tt[2] : q2) * (b3 ? tt[3] : q3);
-      const float4 *node = reinterpret_cast<const float4 *>(base + b0 * s0 + b1 * s1 + b2 * s2 +
-                                                             b3 * s3);
-      const float4 a = __ldg(node), b = __ldg(node + 1), e = __ldg(node + 2);
-      const float v[NP] = {a.x, a.y, a.z, a.w, b.x, b.y, b.z, b.w, e.x};
-#pragma unroll
-      for (int p = 0; p < NP; ++p) out[p] = (c == 0) ? w * v[p] : fmaf(w, v[p], out[p]);
-    }
-    return;
-  }
-  const NearestNode r = nearest_node_g<float>(T.grid, T.stride, T.coord, T.n, T.inv_step,
-                                              T.exact_d2, T.max_nn_dist, T.x0[0] + (double)d[0],
-                                              T.x0[1] + (double)d[1], T.x0[2] + (double)d[2],
-                                              T.x0[3] + (double)d[3]);
-  *flags |= r.flags;
-  const float *row = T.grid + (r.node < 0 ? 0 : r.node) * T.stride;
-#pragma unroll
-  for (int p = 0; p < NP; ++p) out[p] = r.node < 0 ? __int_as_float(0x7fc00000) : __ldg(row + p);
-}
-
-// mu (relative to mu(X0)) and M at one point.
-__device__ __forceinline__ void chem32(const Rate32 &P, const float d[S], const float lap[S],
-                                       float spv, float mu[S], float M[NM], unsigned *flags) {
-  float v[NP];
-  interp32(P, d, v, flags);
-#pragma unroll
-  for (int c = 0; c < S; ++c) {
-    float m = fmaf(-lap[c], P.kappa[c], v[c]);
-    if (P.sp) m = fmaf(spv, P.lvec[c], m);
-    mu[c] = m;
-  }
-#pragma unroll
-  for (int c = 0; c < NM; ++c) M[c] = v[S + c];
-}
-
-// Face flux (phasefield5d/solver/fluxes.py:128-160) in FP32 with the FP64
-// closure X_Fe = (1 - sum X0) - sum Dmid.
-__device__ __forceinline__ void face_flux32(const Rate32 &P, const float Dc[S], const float Mc[NM],
-                                            const float Dn[S], const float Mn[NM],
-                                            const float g[S], float J[S]) {
-  float dm[S], xm[S], mm[NM], dk[S];
-#pragma unroll
-  for (int a = 0; a < S; ++a) {
-    dm[a] = 0.5f * (Dc[a] + Dn[a]);
-    xm[a] = P.x0f[a] + dm[a];
-  }
-#pragma unroll
-  for (int a = 0; a < NM; ++a) mm[a] = 0.5f * (Mc[a] + Mn[a]);
-  const double x_fe = P.c_fe - (((double)dm[0] + (double)dm[1]) + (double)dm[2] + (double)dm[3]);
-  const float w_fe = (float)x_fe * mm[0];
-  float dot = 0.f;
-#pragma unroll
-  for (int b = 0; b < S; ++b) dot = fmaf(xm[b], g[b], dot);
-#pragma unroll
-  for (int k = 0; k < S; ++k) dk[k] = g[k] - dot;
-  float swk = 0.f;
-#pragma unroll
-  for (int k = 0; k < S; ++k) swk = fmaf(xm[k] * mm[1 + k], dk[k], swk);
-#pragma unroll
-  for (int a = 0; a < S; ++a) J[a] = w_fe * xm[a] * dot + xm[a] * mm[1 + a] * dk[a] - xm[a] * swk;
-}
-
-__device__ __forceinline__ void finish_rate32(const Rate32 &P, float m32, double *red) {
-  double m = (double)m32;
-#pragma unroll
-  for (int o = 16; o > 0; o >>= 1) m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
-  const int tid = threadIdx.y * blockDim.x + threadIdx.x;
-  const int nw = (blockDim.x * blockDim.y + 31) >> 5;
-  __syncthreads();
-  if ((tid & 31) == 0) red[tid >> 5] = m;
-  __syncthreads();
-  if (tid == 0) {
-    for (int w = 1; w < nw; ++w) m = fmax(m, red[w]);
-    StepState32 *st = P.st;
-    atomic_max_nonneg(&st->xacc, m);
-    __threadfence();
-    const unsigned total = gridDim.x * gridDim.y * gridDim.z;
-    if (atomicAdd(&st->blocks_done, 1u) == total - 1) {
-      __threadfence();
-      const double xmax = __longlong_as_double(
-          (long long)atomicAdd(reinterpret_cast<unsigned long long *>(&st->xacc), 0ULL));
-      double dt = st->dt;
-      if (P.adaptive) dt = adaptive_dt(dt, xmax, P.ctld, P.t_cfl, P.lower, P.upper, P.factor);
-      st->dt = dt;
-      st->time = st->time + dt;
-      st->xdotmax = xmax;
-      st->step = st->step + 1;
-      st->xacc = 0.0;
-      st->blocks_done = 0;
-    }
-  }
-}
-
-template <int PX, int PM>
-__device__ __forceinline__ void face32_between(const Rate32 &P, const float *XL, const float *ML,
-                                               int pl, int ql, const float *XH, const float *MH,
-                                               int ph, int qh, float J[S]) {
-  float Dc[S], Dn[S], Mc[NM], Mn[NM], g[S];
-#pragma unroll
-  for (int c = 0; c < S; ++c) {
-    Dc[c] = XL[c * PX + pl];
-    Dn[c] = XH[c * PX + ph];
-    g[c] = (MH[c * PM + qh] - ML[c * PM + ql]) * P.inv_dx;
-  }
-#pragma unroll
-  for (int c = 0; c < NM; ++c) {
-    Mc[c] = ML[(S + c) * PM + ql];
-    Mn[c] = MH[(S + c) * PM + qh];
-  }
-  face_flux32(P, Dc, Mc, Dn, Mn, g, J);
-}
-
-template <int TX, int TY>
-__device__ __forceinline__ void plane_faces32(const Rate32 &P, const float *Xp, const float *Mp,
-                                              float *Fx, float *Fy, int tid) {
-  using G = PlaneGeom<TX, TY>;
-  for (int f = tid; f < G::NFX + G::NFY; f += G::NT) {
-    float J[S];
-    if (f < G::NFX) {
-      const int fy = f / (TX + 1), fx = f - fy * (TX + 1);
-      const int pl = (fy + 2) * G::HX + (fx + 1), ql = (fy + 1) * G::MX + fx;
-      face32_between<G::PX, G::PM>(P, Xp, Mp, pl, ql, Xp, Mp, pl + 1, ql + 1, J);
-#pragma unroll
-      for (int c = 0; c < S; ++c) Fx[c * G::NFX + f] = J[c];
-    } else {
-      const int f2 = f - G::NFX;
-      const int fy = f2 / TX, fx = f2 - fy * TX;
-      const int pl = (fy + 1) * G::HX + (fx + 2), ql = fy * G::MX + (fx + 1);
-      face32_between<G::PX, G::PM>(P, Xp, Mp, pl, ql, Xp, Mp, pl + G::HX, ql + G::MX, J);
-#pragma unroll
-      for (int c = 0; c < S; ++c) Fy[c * G::NFY + f2] = J[c];
-    }
-  }
-}
-
-template <int TX, int TY>
-__device__ __forceinline__ void load_plane32(const float4 *__restrict__ D, int64_t plane_off,
-                                             const int *wx, const int *wy, int nx, float *dst,
-                                             int tid) {
-  using G = PlaneGeom<TX, TY>;
-  for (int pos = tid; pos < G::PX; pos += G::NT) {
-    const int hy = pos / G::HX, hx = pos - hy * G::HX;
-    const float4 v = __ldg(D + plane_off + (int64_t)wy[hy] * nx + wx[hx]);
-    dst[0 * G::PX + pos] = v.x;
-    dst[1 * G::PX + pos] = v.y;
-    dst[2 * G::PX + pos] = v.z;
-    dst[3 * G::PX + pos] = v.w;
-  }
-}
-
-__device__ __forceinline__ void store_rate(float4 *dX, int64_t g, const float out[S], float &vmax) {
-#pragma unroll
-  for (int c = 0; c < S; ++c) vmax = fmaxf(vmax, fabsf(out[c]));
-  dX[g] = make_float4(out[0], out[1], out[2], out[3]);
-}
 
 // ------------------------------------------------------------------------
 // Rate kernels (same tiling as the FP64 kernels)
 // ------------------------------------------------------------------------
-template <int TX, int TY, int MINB>
+
+template <int TX, int TY, int MINB, bool WIN>
 __global__ void __launch_bounds__(TX * TY, MINB) k32_rate_tile2d(Rate32 P) {
-  using G = PlaneGeom<TX, TY>;
   if (P.st->halt) return;
-  extern __shared__ double sm64[];
-  double *red = sm64;                                    // [NT/32]
-  float *Xs = reinterpret_cast<float *>(red + G::NT / 32);   // [S][PX]
-  float *Ms = Xs + S * G::PX;                            // [NP][PM]
-  float *Fx = Ms + NP * G::PM;                           // [S][NFX]
-  float *Fy = Fx + S * G::NFX;                           // [S][NFY]
-  int *wx = reinterpret_cast<int *>(Fy + S * G::NFY);
-  int *wy = wx + G::HX;
-  const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * TX + tx;
-  const int x0 = blockIdx.x * TX, y0 = blockIdx.y * TY;
+  extern __shared__ float4 sm4[];
+  const int tid = threadIdx.y * TX + threadIdx.x;
   unsigned flags = 0;
-  for (int i = tid; i < G::HX + G::HY; i += G::NT) {
-    if (i < G::HX) wx[i] = wrap_any(x0 + i - 2, P.nx);
-    else wy[i - G::HX] = wrap_any(y0 + (i - G::HX) - 2, P.ny);
-  }
-  __syncthreads();
-  load_plane32<TX, TY>(P.D, 0, wx, wy, P.nx, Xs, tid);
-  __syncthreads();
-  for (int pos = tid; pos < G::PM; pos += G::NT) {
-    const int my = pos / G::MX, mx = pos - my * G::MX;
-    if ((mx == 0 || mx == G::MX - 1) && (my == 0 || my == G::MY - 1)) continue;
-    const int px = (my + 1) * G::HX + (mx + 1);
-    float d[S], lap[S];
-#pragma unroll
-    for (int c = 0; c < S; ++c) {
-      const float *q = Xs + c * G::PX;
-      d[c] = q[px];
-      lap[c] = (q[px + G::HX] + q[px - G::HX] + q[px + 1] + q[px - 1] - 4.f * d[c]) * P.inv_dx2;
-    }
-    const float spv = P.sp ? __ldg(P.sp + (int64_t)wy[my + 1] * P.nx + wx[mx + 1]) : 0.f;
-    float mu[S], M[NM];
-    chem32(P, d, lap, spv, mu, M, &flags);
-#pragma unroll
-    for (int c = 0; c < S; ++c) Ms[c * G::PM + pos] = mu[c];
-#pragma unroll
-    for (int c = 0; c < NM; ++c) Ms[(S + c) * G::PM + pos] = M[c];
-  }
-  __syncthreads();
-  plane_faces32<TX, TY>(P, Xs, Ms, Fx, Fy, tid);
-  __syncthreads();
-  float vmax = 0.f;
-  if (x0 + tx < P.nx && y0 + ty < P.ny) {
-    float out[S];
-#pragma unroll
-    for (int c = 0; c < S; ++c) {
-      const float a = (Fy[c * G::NFY + (ty + 1) * TX + tx] - Fy[c * G::NFY + ty * TX + tx]) +
-                      (Fx[c * G::NFX + ty * (TX + 1) + tx + 1] - Fx[c * G::NFX + ty * (TX + 1) + tx]);
-      out[c] = a * P.inv_dx;
-    }
-    store_rate(P.dX, (int64_t)(y0 + ty) * P.nx + (x0 + tx), out, vmax);
-  }
+  const float vmax = tile2d32_body<TX, TY, WIN>(P, blockIdx.x, blockIdx.y, sm4, &flags, tid);
   if (flags) atomicOr(&P.st->flags, flags);
-  finish_rate32(P, vmax, red);
+  finish_rate32(P, vmax, Tile2dSmem32<TX, TY>::red(sm4));
 }
 
 template <int TX, int TY>
 constexpr size_t tile2d32_smem() {
-  using G = PlaneGeom<TX, TY>;
-  return (G::NT / 32) * sizeof(double) +
-         (S * G::PX + NP * G::PM + S * G::NFX + S * G::NFY) * sizeof(float) +
-         (G::HX + G::HY) * sizeof(int);
+  return Tile2dSmem32<TX, TY>::bytes;
 }
 
-template <int TX, int TY, int MINB>
+template <int TX, int TY, int MINB, bool WIN>
 __global__ void __launch_bounds__(TX * TY, MINB) k32_rate_march3d(Rate32 P, int zc) {
   using G = PlaneGeom<TX, TY>;
   if (P.st->halt) return;
-  extern __shared__ double sm64[];
-  double *red = sm64;
-  float *Xs = reinterpret_cast<float *>(red + G::NT / 32);   // [3][S][PX]
-  float *Ms = Xs + 3 * S * G::PX;                        // [2][NP][PM]
+  extern __shared__ float4 sm4[];
+  float4 *win = sm4;
+  double *red = reinterpret_cast<double *>(win + kWinNodes32 * 3);
+  float *Xs = reinterpret_cast<float *>(red + G::NT / 32);      // [3][S][PX]
+  float *Ms = Xs + 3 * S * G::PX;                                // [2][NP][PM]
   float *Fx = Ms + 2 * NP * G::PM;
   float *Fy = Fx + S * G::NFX;
-  int *wx = reinterpret_cast<int *>(Fy + S * G::NFY);
+  int *wred = reinterpret_cast<int *>(Fy + S * G::NFY);
+  int *win_lo = wred + S * (G::NT / 32);
+  int *wx = win_lo + S + 1;
   int *wy = wx + G::HX;
   const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * TX + tx;
   const int x0 = blockIdx.x * TX, y0 = blockIdx.y * TY;
@@ -352,6 +76,7 @@ __global__ void __launch_bounds__(TX * TY, MINB) k32_rate_march3d(Rate32 P, int 
   const int ze = min(zb + zc, P.nz);
   const int64_t plane = (int64_t)P.ny * P.nx;
   unsigned flags = 0;
+  if (tid == 0) win_lo[S] = 0;
   for (int i = tid; i < G::HX + G::HY; i += G::NT) {
     if (i < G::HX) wx[i] = wrap_any(x0 + i - 2, P.nx);
     else wy[i - G::HX] = wrap_any(y0 + (i - G::HX) - 2, P.ny);
@@ -362,31 +87,9 @@ __global__ void __launch_bounds__(TX * TY, MINB) k32_rate_march3d(Rate32 P, int 
     load_plane32<TX, TY>(P.D, (int64_t)wrap_any(z, P.nz) * plane, wx, wy, P.nx, xplane(z), tid);
   };
   auto compute_mu = [&](int z, bool interior_only) {
-    const float *Xm = xplane(z - 1), *Xc = xplane(z), *Xp = xplane(z + 1);
-    float *dst = mplane(z);
-    const int64_t zoff = (int64_t)wrap_any(z, P.nz) * plane;
-    for (int pos = tid; pos < G::PM; pos += G::NT) {
-      const int my = pos / G::MX, mx = pos - my * G::MX;
-      const bool ex = (mx == 0 || mx == G::MX - 1), ey = (my == 0 || my == G::MY - 1);
-      if (interior_only ? (ex || ey) : (ex && ey)) continue;
-      const int px = (my + 1) * G::HX + (mx + 1);
-      float d[S], lap[S];
-#pragma unroll
-      for (int c = 0; c < S; ++c) {
-        const float *q = Xc + c * G::PX;
-        d[c] = q[px];
-        lap[c] = (Xp[c * G::PX + px] + Xm[c * G::PX + px] + q[px + G::HX] + q[px - G::HX] +
-                  q[px + 1] + q[px - 1] - 6.f * d[c]) * P.inv_dx2;
-      }
-      const float spv =
-          P.sp ? __ldg(P.sp + zoff + (int64_t)wy[my + 1] * P.nx + wx[mx + 1]) : 0.f;
-      float mu[S], M[NM];
-      chem32(P, d, lap, spv, mu, M, &flags);
-#pragma unroll
-      for (int c = 0; c < S; ++c) dst[c * G::PM + pos] = mu[c];
-#pragma unroll
-      for (int c = 0; c < NM; ++c) dst[(S + c) * G::PM + pos] = M[c];
-    }
+    mu_plane32<TX, TY, 3, WIN>(P, xplane(z - 1), xplane(z), xplane(z + 1), mplane(z),
+                          (int64_t)wrap_any(z, P.nz) * plane, wx, wy, interior_only, win, wred,
+                          win_lo, &flags, tid);
   };
   const int pX = (ty + 2) * G::HX + (tx + 2);
   const int pM = (ty + 1) * G::MX + (tx + 1);
@@ -438,9 +141,8 @@ __global__ void __launch_bounds__(TX * TY, MINB) k32_rate_march3d(Rate32 P, int 
 template <int TX, int TY>
 constexpr size_t march3d32_smem() {
   using G = PlaneGeom<TX, TY>;
-  return (G::NT / 32) * sizeof(double) +
-         (3 * S * G::PX + 2 * NP * G::PM + S * G::NFX + S * G::NFY) * sizeof(float) +
-         (G::HX + G::HY) * sizeof(int);
+  return Smem32Tail<TX, TY>::bytes +
+         (3 * S * G::PX + 2 * NP * G::PM + S * G::NFX + S * G::NFY) * sizeof(float);
 }
 
 template <int TX>
@@ -473,7 +175,7 @@ __global__ void __launch_bounds__(TX) k32_rate_1d(Rate32 P) {
     }
     const float spv = P.sp ? __ldg(P.sp + wrap_any(x0 + pos - 1, n)) : 0.f;
     float mu[S], M[NM];
-    chem32(P, d, lap, spv, mu, M, &flags);
+    chem32(P, d, lap, spv, nullptr, nullptr, mu, M, &flags);
 #pragma unroll
     for (int c = 0; c < S; ++c) Ms[c][pos] = mu[c];
 #pragma unroll
@@ -523,39 +225,6 @@ struct Update32 {
   float *s;          // next misfit or nullptr
   int oob_interval;
 };
-
-// (h, l) += inc with TwoSum and renormalisation; explicit _rn intrinsics keep
-// every operation separately rounded.
-__device__ __forceinline__ void comp_add(float &h, float &l, float inc) {
-  const float s = __fadd_rn(h, inc);
-  const float bb = __fsub_rn(s, h);
-  const float err = __fadd_rn(__fsub_rn(h, __fsub_rn(s, bb)), __fsub_rn(inc, bb));
-  const float lo = __fadd_rn(l, err);
-  const float hn = __fadd_rn(s, lo);
-  l = __fsub_rn(lo, __fsub_rn(hn, s));
-  h = hn;
-}
-
-__device__ __forceinline__ unsigned oob_flags_x(const double x[S]) {
-  unsigned f = 0;
-  double sum = 0.0;
-#pragma unroll
-  for (int c = 0; c < S; ++c) {
-    if (!isfinite(x[c])) f |= PF5D_FLAG_NONFINITE;
-    sum = sum + x[c];
-    if (x[c] < 0.0 - 1e-3 || x[c] > 1.0 + 1e-3) f |= PF5D_FLAG_OOB_HARD;
-    if (x[c] < 0.0 - 1e-5 || x[c] > 1.0 + 1e-5) f |= PF5D_FLAG_OOB_SOFT;
-  }
-  if (sum > 1.0 + 1e-3 || sum < 0.0 - 1e-3) f |= PF5D_FLAG_OOB_HARD;
-  if (sum > 1.0 + 1e-5 || sum < 0.0 - 1e-5) f |= PF5D_FLAG_OOB_SOFT;
-  return f;
-}
-
-__device__ __forceinline__ void raise32(StepState32 *st, unsigned f) {
-  if (!f) return;
-  atomicOr(&st->flags, f);
-  if (f & (PF5D_FLAG_NONFINITE | PF5D_FLAG_OOB_HARD)) atomicExch(&st->halt, 1u);
-}
 
 __global__ void k32_update(Update32 U) {
   StepState32 *st = U.st;
@@ -706,7 +375,7 @@ struct Variant32 {
   void (*launch3d)(dim3, dim3, size_t, cudaStream_t, const Rate32 &, int);
 };
 
-template <int TX, int TY, int MINB>
+template <int TX, int TY, int MINB, bool WIN = true>
 Variant32 make_variant32() {
   Variant32 v;
   v.tx = TX;
@@ -716,14 +385,14 @@ Variant32 make_variant32() {
   v.smem3d = march3d32_smem<TX, TY>();
   v.set_attrs = []() {
     const auto a = cudaFuncAttributeMaxDynamicSharedMemorySize;
-    cudaFuncSetAttribute(k32_rate_tile2d<TX, TY, MINB>, a, (int)tile2d32_smem<TX, TY>());
-    cudaFuncSetAttribute(k32_rate_march3d<TX, TY, MINB>, a, (int)march3d32_smem<TX, TY>());
+    cudaFuncSetAttribute(k32_rate_tile2d<TX, TY, MINB, WIN>, a, (int)tile2d32_smem<TX, TY>());
+    cudaFuncSetAttribute(k32_rate_march3d<TX, TY, MINB, WIN>, a, (int)march3d32_smem<TX, TY>());
   };
   v.launch2d = [](dim3 g, dim3 b, size_t sm, cudaStream_t s, const Rate32 &P) {
-    k32_rate_tile2d<TX, TY, MINB><<<g, b, sm, s>>>(P);
+    k32_rate_tile2d<TX, TY, MINB, WIN><<<g, b, sm, s>>>(P);
   };
   v.launch3d = [](dim3 g, dim3 b, size_t sm, cudaStream_t s, const Rate32 &P, int zc) {
-    k32_rate_march3d<TX, TY, MINB><<<g, b, sm, s>>>(P, zc);
+    k32_rate_march3d<TX, TY, MINB, WIN><<<g, b, sm, s>>>(P, zc);
   };
   return v;
 }
@@ -731,7 +400,8 @@ Variant32 make_variant32() {
 const std::vector<Variant32> &variants32() {
   static const std::vector<Variant32> v = {
       make_variant32<32, 8, 2>(), make_variant32<32, 8, 3>(), make_variant32<32, 8, 4>(),
-      make_variant32<32, 4, 6>(), make_variant32<64, 4, 3>(), make_variant32<32, 16, 2>()};
+      make_variant32<32, 4, 6>(), make_variant32<64, 4, 3>(), make_variant32<32, 16, 2>(),
+      make_variant32<32, 8, 2, false>(), make_variant32<32, 16, 2, false>()};
   return v;
 }
 

@@ -32,6 +32,7 @@
 #include "pf5d_fft.h"
 #include "pf5d_fp32c.h"
 #include "pf5d_tiles.cuh"
+#include "pf5d_window.cuh"
 
 namespace pf5d {
 
@@ -80,6 +81,136 @@ __device__ __forceinline__ void chem_point(const RateParams &P, const double x[S
   }
 #pragma unroll
   for (int c = 0; c < NM; ++c) M[c] = v[S + c];
+}
+
+constexpr int kWin64 = 3;                       // window nodes per axis (2 cells)
+constexpr int kWinNodes64 = kWin64 * kWin64 * kWin64 * kWin64;
+constexpr int kNodeV64 = 5;                     // double2 per 10-double table node
+
+// Table cell of x exactly as the reference computes it (interpolation.py:103-121).
+__device__ __forceinline__ bool cell64(const Table &T, const double x[S], int ii[S], double tt[S]) {
+  if (!linear_region(T, x)) return false;
+#pragma unroll
+  for (int a = 0; a < S; ++a) axis_coord(x[a] * T.inv_step, T.n, ii[a], tt[a]);
+  return true;
+}
+
+// The 16-corner sum of interp_linear<true> from node-strided double2 data
+// (global table or shared window); identical arithmetic and order.
+__device__ __forceinline__ void interp_nodes64(const double2 *base, int64_t s0, int64_t s1,
+                                               int64_t s2, int64_t s3, const double tt[S],
+                                               double out[NP]) {
+  const double q0 = 1.0 - tt[0], q1 = 1.0 - tt[1], q2 = 1.0 - tt[2], q3 = 1.0 - tt[3];
+#pragma unroll
+  for (int c = 0; c < 16; ++c) {
+    const int b0 = (c >> 3) & 1, b1 = (c >> 2) & 1, b2 = (c >> 1) & 1, b3 = c & 1;
+    const double w = (b0 ? tt[0] : q0) * (b1 ? tt[1] : q1) * (b2 ? tt[2] : q2) * (b3 ? tt[3] : q3);
+    const double2 *node = base + b0 * s0 + b1 * s1 + b2 * s2 + b3 * s3;
+    double v[NP + 1];
+#pragma unroll
+    for (int k = 0; k < kNodeV64; ++k) {
+      const double2 a = node[k];
+      v[2 * k] = a.x;
+      v[2 * k + 1] = a.y;
+    }
+#pragma unroll
+    for (int p = 0; p < NP; ++p) {
+      const double term = w * v[p];
+      out[p] = (c == 0) ? term : out[p] + term;
+    }
+  }
+}
+
+// Table value at x with the shared window (VEC tables only): window when the
+// cell fits, global table otherwise, nearest row outside the linear region.
+template <bool VEC>
+__device__ __forceinline__ void interp_win64(const Table &T, const double x[S], const double2 *win,
+                                             const int *win_lo, double out[NP], unsigned *flags) {
+  if (!VEC) {
+    interp_point<false>(T, x, out, flags);
+    return;
+  }
+  int ii[S];
+  double tt[S];
+  if (cell64(T, x, ii, tt)) {
+    const int off = win ? window_cell<kWin64>(ii, win_lo) : -1;
+    if (off >= 0) {
+      constexpr int w3 = kNodeV64, w2 = kWin64 * w3, w1 = kWin64 * w2, w0 = kWin64 * w1;
+      interp_nodes64(win + off * kNodeV64, w0, w1, w2, w3, tt, out);
+    } else {
+      const int64_t s3 = kNodeV64, s2 = (int64_t)T.n * s3, s1 = (int64_t)T.n * s2,
+                    s0 = (int64_t)T.n * s1;
+      const double2 *g = reinterpret_cast<const double2 *>(T.grid);
+      interp_nodes64(g + ii[0] * s0 + ii[1] * s1 + ii[2] * s2 + ii[3] * s3, s0, s1, s2, s3, tt,
+                     out);
+    }
+    return;
+  }
+  const NearestNode r = nearest_node(T, x[0], x[1], x[2], x[3]);
+  *flags |= r.flags;
+  const double *row = T.grid + (r.node < 0 ? 0 : r.node) * T.stride;
+#pragma unroll
+  for (int p = 0; p < NP; ++p)
+    out[p] = r.node < 0 ? __longlong_as_double(0x7ff8000000000000LL) : __ldg(row + p);
+}
+
+// mu/M of one plane (tile + 1-cell halo, or tile only) into dst, making the
+// table window in `win` current first (win_lo: origin + valid flag).  Xm/Xp: axis-0 neighbour planes (3D) or
+// nullptr (2D).  Laplacian neighbour order as operators.py:49-76.
+template <int TX, int TY, int DIM, bool VEC, bool WIN>
+__device__ __forceinline__ void mu_plane64(const RateParams &P, const double *Xm, const double *Xc,
+                                           const double *Xp, double *dst, int64_t zoff,
+                                           const int *wx, const int *wy, bool interior_only,
+                                           double2 *win, int *win_lo, unsigned *flags, int tid) {
+  using G = PlaneGeom<TX, TY>;
+  auto skip = [&](int mx, int my) {
+    const bool ex = (mx == 0 || mx == G::MX - 1), ey = (my == 0 || my == G::MY - 1);
+    return interior_only ? (ex || ey) : (ex && ey);
+  };
+  // Table window around the tile centre's cell (reloaded if it moved).
+  bool use_win = false;
+  int o[S] = {0, 0, 0, 0};
+  if (VEC && WIN) {
+    int rep[S];
+    double tr[S], xc[S];
+    const int cp = (TY / 2 + 2) * G::HX + (TX / 2 + 2);
+#pragma unroll
+    for (int c = 0; c < S; ++c) xc[c] = Xc[c * G::PX + cp];
+    use_win = cell64(P.T, xc, rep, tr);
+    if (use_win) {
+      window_origin<kWin64>(rep, tr, o);
+      ensure_window<kWin64, kNodeV64, double2, G::NT>(reinterpret_cast<const double2 *>(P.T.grid),
+                                                       P.T.n, o, win, win_lo, tid);
+    }
+  }
+  for (int pos = tid; pos < G::PM; pos += G::NT) {
+    const int my = pos / G::MX, mx = pos - my * G::MX;
+    if (skip(mx, my)) continue;
+    const int px = (my + 1) * G::HX + (mx + 1);
+    double x[S], lap[S];
+#pragma unroll
+    for (int c = 0; c < S; ++c) {
+      const double *q = Xc + c * G::PX;
+      x[c] = q[px];
+      if (DIM == 3)
+        lap[c] = (Xp[c * G::PX + px] + Xm[c * G::PX + px] + q[px + G::HX] + q[px - G::HX] +
+                  q[px + 1] + q[px - 1] - 6.0 * x[c]) * P.inv_dx2;
+      else
+        lap[c] = (q[px + G::HX] + q[px - G::HX] + q[px + 1] + q[px - 1] - 4.0 * x[c]) * P.inv_dx2;
+    }
+    const double spv = P.sp ? __ldg(P.sp + zoff + (int64_t)wy[my + 1] * P.nx + wx[mx + 1]) : 0.0;
+    double v[NP];
+    interp_win64<VEC>(P.T, x, use_win ? win : nullptr, o, v, flags);
+#pragma unroll
+    for (int c = 0; c < S; ++c) {
+      const double lk = lap[c] * P.kappa.v[c];
+      double m = v[c] - lk;
+      if (P.sp) m = m + spv * P.lvec.v[c];
+      dst[c * G::PM + pos] = m;
+    }
+#pragma unroll
+    for (int c = 0; c < NM; ++c) dst[(S + c) * G::PM + pos] = v[S + c];
+  }
 }
 
 // Fold this thread's max |dX/dt| into the block, then into the device
@@ -185,7 +316,7 @@ __device__ __forceinline__ void load_plane(const double *__restrict__ X, int64_t
 // Axis 0 of the (n0, n1) field is the tile's y, axis 1 its x.  Laplacian
 // (operators.py:49-60) and divergence (fluxes.py:349) keep the reference's
 // axis order: axis-0 terms first.
-template <int TX, int TY, int MINB, bool VEC>
+template <int TX, int TY, int MINB, bool VEC, bool WIN>
 __global__ void __launch_bounds__(TX * TY, MINB) k_rate_tile2d(RateParams P) {
   using G = PlaneGeom<TX, TY>;
   if (P.st->halt) return;
@@ -193,13 +324,15 @@ __global__ void __launch_bounds__(TX * TY, MINB) k_rate_tile2d(RateParams P) {
   double *Xs = sm;                       // [S][PX]
   double *Ms = Xs + S * G::PX;           // [NP][PM]
   double *Fx = Ms + NP * G::PM;          // [S][NFX]
-  double *Fy = Fx + S * G::NFX;          // [S][NFY]
+  double *Fy = Fx + S * G::NFX;          // [S][NFY]   (Fx/Fy also hold the table window)
   double *red = Fy + S * G::NFY;         // [NT/32]
   int *wx = reinterpret_cast<int *>(red + G::NT / 32);   // [HX]
   int *wy = wx + G::HX;                                  // [HY]
+  int *win_lo = wy + G::HY;                              // [S+1] window origin, valid
   const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * TX + tx;
   const int x0 = blockIdx.x * TX, y0 = blockIdx.y * TY;
   unsigned flags = 0;
+  if (tid == 0) win_lo[S] = 0;
 
   for (int i = tid; i < G::HX + G::HY; i += G::NT) {
     if (i < G::HX) wx[i] = wrap_any(x0 + i - 2, P.nx);
@@ -208,25 +341,8 @@ __global__ void __launch_bounds__(TX * TY, MINB) k_rate_tile2d(RateParams P) {
   __syncthreads();
   load_plane<TX, TY>(P.X, 0, wx, wy, P.nx, Xs, tid);
   __syncthreads();
-  for (int pos = tid; pos < G::PM; pos += G::NT) {
-    const int my = pos / G::MX, mx = pos - my * G::MX;
-    if ((mx == 0 || mx == G::MX - 1) && (my == 0 || my == G::MY - 1)) continue;
-    const int px = (my + 1) * G::HX + (mx + 1);
-    double x[S], lap[S];
-#pragma unroll
-    for (int c = 0; c < S; ++c) {
-      const double *q = Xs + c * G::PX;
-      x[c] = q[px];
-      lap[c] = (q[px + G::HX] + q[px - G::HX] + q[px + 1] + q[px - 1] - 4.0 * x[c]) * P.inv_dx2;
-    }
-    const double spv = P.sp ? __ldg(P.sp + (int64_t)wy[my + 1] * P.nx + wx[mx + 1]) : 0.0;
-    double mu[S], M[NM];
-    chem_point<VEC>(P, x, lap, spv, mu, M, &flags);
-#pragma unroll
-    for (int c = 0; c < S; ++c) Ms[c * G::PM + pos] = mu[c];
-#pragma unroll
-    for (int c = 0; c < NM; ++c) Ms[(S + c) * G::PM + pos] = M[c];
-  }
+  mu_plane64<TX, TY, 2, VEC, WIN>(P, nullptr, Xs, nullptr, Ms, 0, wx, wy, false,
+                             reinterpret_cast<double2 *>(Fx), win_lo, &flags, tid);
   __syncthreads();
   plane_faces<TX, TY>(Xs, Ms, Fx, Fy, P.inv_dx, tid);
   __syncthreads();
@@ -254,8 +370,10 @@ __global__ void __launch_bounds__(TX * TY, MINB) k_rate_tile2d(RateParams P) {
 template <int TX, int TY>
 constexpr size_t tile2d_smem() {
   using G = PlaneGeom<TX, TY>;
+  static_assert(S * (G::NFX + G::NFY) * sizeof(double) >= kWinNodes64 * kNodeV64 * sizeof(double2),
+                "face buffers must hold the table window");
   return (S * G::PX + NP * G::PM + S * G::NFX + S * G::NFY + G::NT / 32) * sizeof(double) +
-         (G::HX + G::HY) * sizeof(int);
+         (G::HX + G::HY + S + 1) * sizeof(int);
 }
 
 // ------------------------------------------------------------------------
@@ -263,22 +381,55 @@ constexpr size_t tile2d_smem() {
 // ------------------------------------------------------------------------
 // Each block owns a TY x TX tile of (axis 1, axis 2) and a chunk of axis-0
 // planes.  Rings in shared memory: 3 X planes (2-cell halo), 2 mu/M planes
-// (1-cell halo).  Per output plane z: stage X(z+2), evaluate mu/M(z+1),
-// compute the plane's x/y faces (flat loop) and each point's +z face, and
-// form the divergence with the -z face kept in registers from plane z-1.
-// Laplacian order (operators.py:68-76): +z, -z, +y, -y, +x, -x.
-template <int TX, int TY, int MINB, bool VEC>
+// (1-cell halo); a persistent table window.  Per output plane z: stage
+// X(z+2), evaluate mu/M(z+1), each point's +z face, then the y-faces and
+// the x-faces through one face buffer, forming the divergence in the
+// reference's axis order: (+z - -z) + (+y - -y) + (+x - -x), with the -z
+// face kept in registers from plane z-1.  Laplacian order
+// (operators.py:68-76): +z, -z, +y, -y, +x, -x.
+
+// One family of faces of a plane tile into F: AXIS 0 = x-faces (TY x (TX+1)),
+// AXIS 1 = y-faces ((TY+1) x TX).
+template <int TX, int TY, int AXIS>
+__device__ __forceinline__ void plane_faces_axis(const double *Xp, const double *Mp, double *F,
+                                                 double inv_dx, int tid) {
+  using G = PlaneGeom<TX, TY>;
+  constexpr int NF = AXIS == 0 ? G::NFX : G::NFY;
+  for (int f = tid; f < NF; f += G::NT) {
+    double J[S];
+    if (AXIS == 0) {
+      const int fy = f / (TX + 1), fx = f - fy * (TX + 1);
+      const int pl = (fy + 2) * G::HX + (fx + 1), ql = (fy + 1) * G::MX + fx;
+      face_between<G::PX, G::PM>(Xp, Mp, pl, ql, Xp, Mp, pl + 1, ql + 1, inv_dx, J);
+    } else {
+      const int fy = f / TX, fx = f - fy * TX;
+      const int pl = (fy + 1) * G::HX + (fx + 2), ql = fy * G::MX + (fx + 1);
+      face_between<G::PX, G::PM>(Xp, Mp, pl, ql, Xp, Mp, pl + G::HX, ql + G::MX, inv_dx, J);
+    }
+#pragma unroll
+    for (int c = 0; c < S; ++c) F[c * NF + f] = J[c];
+  }
+}
+
+template <int TX, int TY>
+struct March64Geom {
+  using G = PlaneGeom<TX, TY>;
+  static constexpr int NFMAX = G::NFX > G::NFY ? G::NFX : G::NFY;
+};
+
+template <int TX, int TY, int MINB, bool VEC, bool WIN>
 __global__ void __launch_bounds__(TX * TY, MINB) k_rate_march3d(RateParams P, int zc) {
   using G = PlaneGeom<TX, TY>;
   if (P.st->halt) return;
   extern __shared__ double sm[];
-  double *Xs = sm;                       // [3][S][PX]
-  double *Ms = Xs + 3 * S * G::PX;       // [2][NP][PM]
-  double *Fx = Ms + 2 * NP * G::PM;      // [S][NFX]
-  double *Fy = Fx + S * G::NFX;          // [S][NFY]
-  double *red = Fy + S * G::NFY;         // [NT/32]
+  double *Xs = sm;                                           // [3][S][PX]
+  double *Ms = Xs + 3 * S * G::PX;                           // [2][NP][PM]
+  double *F = Ms + 2 * NP * G::PM;                           // [S][NFMAX]
+  double2 *win = reinterpret_cast<double2 *>(F + S * March64Geom<TX, TY>::NFMAX);
+  double *red = reinterpret_cast<double *>(win + kWinNodes64 * kNodeV64);   // [NT/32]
   int *wx = reinterpret_cast<int *>(red + G::NT / 32);
   int *wy = wx + G::HX;
+  int *win_lo = wy + G::HY;                                  // [S+1]
   const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * TX + tx;
   const int x0 = blockIdx.x * TX, y0 = blockIdx.y * TY;
   const int zb = blockIdx.z * zc;
@@ -290,37 +441,16 @@ __global__ void __launch_bounds__(TX * TY, MINB) k_rate_march3d(RateParams P, in
     if (i < G::HX) wx[i] = wrap_any(x0 + i - 2, P.nx);
     else wy[i - G::HX] = wrap_any(y0 + (i - G::HX) - 2, P.ny);
   }
+  if (tid == 0) win_lo[S] = 0;
   auto xplane = [&](int z) { return Xs + ((z - zb + 3) % 3) * S * G::PX; };
   auto mplane = [&](int z) { return Ms + ((z - zb + 2) & 1) * NP * G::PM; };
   auto load_x = [&](int z) {
     load_plane<TX, TY>(P.X, (int64_t)wrap_any(z, P.nz) * plane, wx, wy, P.nx, xplane(z), tid);
   };
   auto compute_mu = [&](int z, bool interior_only) {
-    const double *Xm = xplane(z - 1), *Xc = xplane(z), *Xp = xplane(z + 1);
-    double *dst = mplane(z);
-    const int64_t zoff = (int64_t)wrap_any(z, P.nz) * plane;
-    for (int pos = tid; pos < G::PM; pos += G::NT) {
-      const int my = pos / G::MX, mx = pos - my * G::MX;
-      const bool ex = (mx == 0 || mx == G::MX - 1), ey = (my == 0 || my == G::MY - 1);
-      if (interior_only ? (ex || ey) : (ex && ey)) continue;
-      const int px = (my + 1) * G::HX + (mx + 1);
-      double x[S], lap[S];
-#pragma unroll
-      for (int c = 0; c < S; ++c) {
-        const double *q = Xc + c * G::PX;
-        x[c] = q[px];
-        lap[c] = (Xp[c * G::PX + px] + Xm[c * G::PX + px] + q[px + G::HX] + q[px - G::HX] +
-                  q[px + 1] + q[px - 1] - 6.0 * x[c]) * P.inv_dx2;
-      }
-      const double spv =
-          P.sp ? __ldg(P.sp + zoff + (int64_t)wy[my + 1] * P.nx + wx[mx + 1]) : 0.0;
-      double mu[S], M[NM];
-      chem_point<VEC>(P, x, lap, spv, mu, M, &flags);
-#pragma unroll
-      for (int c = 0; c < S; ++c) dst[c * G::PM + pos] = mu[c];
-#pragma unroll
-      for (int c = 0; c < NM; ++c) dst[(S + c) * G::PM + pos] = M[c];
-    }
+    mu_plane64<TX, TY, 3, VEC, WIN>(P, xplane(z - 1), xplane(z), xplane(z + 1), mplane(z),
+                               (int64_t)wrap_any(z, P.nz) * plane, wx, wy, interior_only, win,
+                               win_lo, &flags, tid);
   };
   const int pX = (ty + 2) * G::HX + (tx + 2);
   const int pM = (ty + 1) * G::MX + (tx + 1);
@@ -347,31 +477,40 @@ __global__ void __launch_bounds__(TX * TY, MINB) k_rate_march3d(RateParams P, in
     __syncthreads();
     compute_mu(z + 1, false);
     __syncthreads();
-    double Jz[S];
+    double a[S];
     face_between<G::PX, G::PM>(xplane(z), mplane(z), pX, pM, xplane(z + 1), mplane(z + 1), pX,
-                               pM, P.inv_dx, Jz);
-    plane_faces<TX, TY>(xplane(z), mplane(z), Fx, Fy, P.inv_dx, tid);
+                               pM, P.inv_dx, a);
+#pragma unroll
+    for (int c = 0; c < S; ++c) {
+      const double jz = a[c];
+      a[c] = jz - Jm[c];
+      Jm[c] = jz;
+    }
+    plane_faces_axis<TX, TY, 1>(xplane(z), mplane(z), F, P.inv_dx, tid);
+    __syncthreads();
+#pragma unroll
+    for (int c = 0; c < S; ++c) {
+      a[c] = a[c] + F[c * G::NFY + (ty + 1) * TX + tx];
+      a[c] = a[c] - F[c * G::NFY + ty * TX + tx];
+    }
+    __syncthreads();
+    plane_faces_axis<TX, TY, 0>(xplane(z), mplane(z), F, P.inv_dx, tid);
     __syncthreads();
     if (in_tile) {
       double out[S];
 #pragma unroll
       for (int c = 0; c < S; ++c) {
-        double a = Jz[c] - Jm[c];
-        a = a + Fy[c * G::NFY + (ty + 1) * TX + tx];
-        a = a - Fy[c * G::NFY + ty * TX + tx];
-        a = a + Fx[c * G::NFX + ty * (TX + 1) + tx + 1];
-        a = a - Fx[c * G::NFX + ty * (TX + 1) + tx];
-        out[c] = a * P.inv_dx;
-        const double v = fabs(out[c]);
-        if (v > vmax) vmax = v;
+        double v = a[c] + F[c * G::NFX + ty * (TX + 1) + tx + 1];
+        v = v - F[c * G::NFX + ty * (TX + 1) + tx];
+        out[c] = v * P.inv_dx;
+        const double m = fabs(out[c]);
+        if (m > vmax) vmax = m;
       }
       const int64_t g = (int64_t)z * plane + (int64_t)(y0 + ty) * P.nx + (x0 + tx);
       double2 *o = reinterpret_cast<double2 *>(P.dX + 4 * g);
       o[0] = make_double2(out[0], out[1]);
       o[1] = make_double2(out[2], out[3]);
     }
-#pragma unroll
-    for (int c = 0; c < S; ++c) Jm[c] = Jz[c];
   }
   if (flags) atomicOr(&P.st->flags, flags);
   finish_rate(P, vmax, red);
@@ -380,9 +519,9 @@ __global__ void __launch_bounds__(TX * TY, MINB) k_rate_march3d(RateParams P, in
 template <int TX, int TY>
 constexpr size_t march3d_smem() {
   using G = PlaneGeom<TX, TY>;
-  return (3 * S * G::PX + 2 * NP * G::PM + S * G::NFX + S * G::NFY + G::NT / 32) *
+  return (3 * S * G::PX + 2 * NP * G::PM + S * March64Geom<TX, TY>::NFMAX + G::NT / 32) *
              sizeof(double) +
-         (G::HX + G::HY) * sizeof(int);
+         kWinNodes64 * kNodeV64 * sizeof(double2) + (G::HX + G::HY + S + 1) * sizeof(int);
 }
 
 // ------------------------------------------------------------------------
@@ -616,6 +755,7 @@ constexpr int kGraphSteps = 50;      // steps per captured graph
 // threads) and the minimum resident blocks per SM (which caps registers).
 struct RateVariant {
   int tx, ty, minb;
+  bool win;
   size_t smem2d, smem3d;
   void (*set_attrs)(bool vec);
   void (*launch2d)(bool vec, dim3 g, dim3 b, size_t sm, cudaStream_t s, const RateParams &P);
@@ -623,33 +763,34 @@ struct RateVariant {
                    int zc);
 };
 
-template <int TX, int TY, int MINB>
+template <int TX, int TY, int MINB, bool WIN = true>
 RateVariant make_variant() {
   RateVariant v;
   v.tx = TX;
   v.ty = TY;
   v.minb = MINB;
+  v.win = WIN;
   v.smem2d = tile2d_smem<TX, TY>();
   v.smem3d = march3d_smem<TX, TY>();
   v.set_attrs = [](bool vec) {
     const int s2 = (int)tile2d_smem<TX, TY>(), s3 = (int)march3d_smem<TX, TY>();
     const auto a = cudaFuncAttributeMaxDynamicSharedMemorySize;
     if (vec) {
-      cudaFuncSetAttribute(k_rate_tile2d<TX, TY, MINB, true>, a, s2);
-      cudaFuncSetAttribute(k_rate_march3d<TX, TY, MINB, true>, a, s3);
+      cudaFuncSetAttribute(k_rate_tile2d<TX, TY, MINB, true, WIN>, a, s2);
+      cudaFuncSetAttribute(k_rate_march3d<TX, TY, MINB, true, WIN>, a, s3);
     } else {
-      cudaFuncSetAttribute(k_rate_tile2d<TX, TY, MINB, false>, a, s2);
-      cudaFuncSetAttribute(k_rate_march3d<TX, TY, MINB, false>, a, s3);
+      cudaFuncSetAttribute(k_rate_tile2d<TX, TY, MINB, false, WIN>, a, s2);
+      cudaFuncSetAttribute(k_rate_march3d<TX, TY, MINB, false, WIN>, a, s3);
     }
   };
   v.launch2d = [](bool vec, dim3 g, dim3 b, size_t sm, cudaStream_t s, const RateParams &P) {
-    if (vec) k_rate_tile2d<TX, TY, MINB, true><<<g, b, sm, s>>>(P);
-    else k_rate_tile2d<TX, TY, MINB, false><<<g, b, sm, s>>>(P);
+    if (vec) k_rate_tile2d<TX, TY, MINB, true, WIN><<<g, b, sm, s>>>(P);
+    else k_rate_tile2d<TX, TY, MINB, false, WIN><<<g, b, sm, s>>>(P);
   };
   v.launch3d = [](bool vec, dim3 g, dim3 b, size_t sm, cudaStream_t s, const RateParams &P,
                   int zc) {
-    if (vec) k_rate_march3d<TX, TY, MINB, true><<<g, b, sm, s>>>(P, zc);
-    else k_rate_march3d<TX, TY, MINB, false><<<g, b, sm, s>>>(P, zc);
+    if (vec) k_rate_march3d<TX, TY, MINB, true, WIN><<<g, b, sm, s>>>(P, zc);
+    else k_rate_march3d<TX, TY, MINB, false, WIN><<<g, b, sm, s>>>(P, zc);
   };
   return v;
 }
@@ -657,7 +798,8 @@ RateVariant make_variant() {
 const std::vector<RateVariant> &rate_variants() {
   static const std::vector<RateVariant> v = {
       make_variant<32, 8, 2>(), make_variant<32, 8, 3>(), make_variant<32, 4, 4>(),
-      make_variant<16, 8, 4>(), make_variant<64, 4, 2>(), make_variant<32, 4, 6>()};
+      make_variant<16, 8, 4>(), make_variant<64, 4, 2>(), make_variant<32, 4, 6>(),
+      make_variant<32, 8, 2, false>(), make_variant<32, 8, 3, false>()};
   return v;
 }
 

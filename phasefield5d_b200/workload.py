@@ -308,3 +308,119 @@ def config_3d_precision():
     return SolveConfig(system_dim=3, initial_composition=(0.1, 0.2, 0.3, 0.2), mw=16, ppw=16,
                        kappa_value=7.6e-15, resolution=0.02, adaptive=True,
                        total_timesteps=5_000, steps_per_ctld=1000)
+
+
+# ---------------------------------------------------------------------------
+# Batched workload: many uneven solves
+# ---------------------------------------------------------------------------
+
+BATCH_TEMPERATURES = (773.0, 873.0, 973.0, 1073.0)
+
+
+def random_composition(rng, lo=0.05, hi=0.4, max_sum=0.88):
+    """X_i ~ U[lo, hi] (a uniform point of that box of the simplex),
+    rejection-sampled to sum(X) <= max_sum so every point starts in the
+    table's linear region."""
+    while True:
+        x = rng.uniform(lo, hi, size=4)
+        if x.sum() <= max_sum:
+            return tuple(float(v) for v in x)
+
+
+def batched_configs(n_solves=64, seed=2026, resolution=0.025, steps=10_000, n_k=2000):
+    """The batched workload: n_solves solves alternating 1D (N in 2048..8192,
+    step 16) and 2D (N x N, N in 128..384, step 16); compositions uniform in
+    [0.05, 0.4] per component; kappa log-uniform in [1e-16, 1e-14]; one of
+    four temperature tables (773/873/973/1073 K) round-robin."""
+    rng = np.random.default_rng(seed)
+    cfgs = []
+    for i in range(n_solves):
+        dim = 1 if i % 2 == 0 else 2
+        if dim == 1:
+            shape = (int(rng.choice(np.arange(2048, 8192 + 1, 16))),)
+        else:
+            n = int(rng.choice(np.arange(128, 384 + 1, 16)))
+            shape = (n, n)
+        cfgs.append(SolveConfig(
+            system_dim=dim, initial_composition=random_composition(rng),
+            kappa_value=float(10 ** rng.uniform(-16, -14)), resolution=resolution,
+            temperature=BATCH_TEMPERATURES[i % len(BATCH_TEMPERATURES)], shape=shape,
+            adaptive=True, total_timesteps=steps, misfit_seed=1, ic_seed=100 + i,
+            omega_seed=0, n_k=n_k))
+    return cfgs
+
+
+def analytic_hessian(omega, temperature, X):
+    """d mu_i / d x_j of the regular-solution G (module docstring) at X:
+    RT (delta_ij / x_i + 1 / x_0) + Omega_ij - Omega_i0 - Omega_0j."""
+    X = np.asarray(X, dtype=float)
+    x0 = 1.0 - X.sum()
+    RT = R_GAS * float(temperature)
+    H = RT * (np.diag(1.0 / X) + 1.0 / x0)
+    H = H + omega[1:, 1:] - omega[1:, 0][:, None] - omega[0, 1:][None, :]
+    return H
+
+
+def analytically_unstable(omega, temperature, X, elastic_matrix=None):
+    """True when the chemical (+ elastic) Hessian at X has a negative
+    eigenvalue, i.e. X lies inside the spinodal of the regular solution."""
+    H = analytic_hessian(omega, temperature, X)
+    if elastic_matrix is not None:
+        H = H + elastic_matrix
+    return float(np.linalg.eigvalsh(0.5 * (H + H.T))[0]) < 0.0
+
+
+def _elastic_matrix_for(cfg, X0):
+    if not cfg.include_cubic_anisotropy:
+        return None
+    vm = float(els.calculate_molar_volume(X0, MOLAR_VOLUMES_FEMNNICOCU))
+    return els.get_elastic_matrix(_misfit(cfg.misfit_seed), vm, cfg.c11, cfg.c12, cfg.c44,
+                                  cfg.direction)
+
+
+def pick_omega_seed(cfg, rng, samples=200, min_fraction=0.2, max_seeds=400):
+    """First Omega seed >= cfg.omega_seed under which at least `min_fraction`
+    of compositions drawn like the batched workload's are spinodal (at high
+    temperature, where no seed reaches that, the seed with the largest
+    spinodal share)."""
+    xs = [random_composition(rng) for _ in range(samples)]
+    els_m = [_elastic_matrix_for(cfg, np.array(x)) for x in xs]
+    best, best_hits = None, 0
+    for seed in range(cfg.omega_seed, cfg.omega_seed + max_seeds):
+        om, _ = draw_omega(seed)
+        hits = sum(analytically_unstable(om, cfg.temperature, x, e) for x, e in zip(xs, els_m))
+        if hits >= min_fraction * samples:
+            return seed
+        if hits > best_hits:
+            best, best_hits = seed, hits
+    if best is None:
+        raise RuntimeError(f"no Omega seed with a spinodal region at {cfg.temperature} K")
+    return best
+
+
+def build_batched_problems(cfgs, max_tries=400, seed=77):
+    """Host setup of every solve.  Each temperature gets one table whose
+    Omega seed leaves a good share of the composition box spinodal; each
+    solve redraws its composition until it is spinodal for its table
+    (analytic Hessian test, confirmed by the CTLD setup).  Returns
+    (problems, {temperature: table})."""
+    rng = np.random.default_rng(seed)
+    tables = {}
+    probs = []
+    for cfg in cfgs:
+        T = cfg.temperature
+        if T not in tables:
+            tables[T] = make_table(cfg.resolution, T, pick_omega_seed(cfg, rng))
+        table = tables[T]
+        for _ in range(max_tries):
+            x = np.array(cfg.initial_composition)
+            if analytically_unstable(table.omega, T, x, _elastic_matrix_for(cfg, x)):
+                try:
+                    probs.append(build_problem(cfg, table=table))
+                    break
+                except ValueError:
+                    pass
+            cfg.initial_composition = random_composition(rng)
+        else:
+            raise RuntimeError(f"no unstable composition found at {T} K")
+    return probs, tables

@@ -223,7 +223,7 @@ def test_rate_variants_bitwise_identical(torch_cuda):
                             adaptive=True, n_k=2000, fluctuation=2e-2)
         prob = W.build_problem(cfg)
         ref = None
-        for v in range(6):
+        for v in range(8):
             st = Stepper.from_problem(prob, autotune=False)
             st.set_variant(v)
             st.run(7)
