@@ -25,10 +25,16 @@ def _table32(grid, mu_ref, torch):
     return torch.from_numpy(out).cuda()
 
 
+# Reference composition whose mu each FP32 table subtracts: the equiatomic
+# point of the five species.  It is fixed per table, so a solve's table (and
+# its trajectory) does not depend on which other solves share the batch.
+TABLE_REFERENCE_X = (0.2, 0.2, 0.2, 0.2)
+
+
 class BatchStepper:
     """Advance a list of ``workload.Problem`` (1D/2D, same table resolution)
-    together.  Problems with the same temperature share one device table;
-    the FP32 table stores mu minus the mean mu(X0) of its solves."""
+    together.  Problems with the same temperature share one device table,
+    which stores mu - mu(TABLE_REFERENCE_X) and M in FP32."""
 
     def __init__(self, problems, stream=None, autotune=True, oob_interval=100):
         import torch
@@ -48,11 +54,10 @@ class BatchStepper:
         self.table_keys = keys
         self.tables = []
         for k in keys:
-            members = [p for p in self.problems if (p.cfg.temperature, p.table.seed) == k]
-            grid = members[0].grid
-            mus = [host_table_eval(np.asarray(p.X0)[None, :], grid, self.resolution)[0, :4]
-                   for p in members]
-            self.tables.append(_table32(grid, np.mean(mus, axis=0), torch))
+            grid = next(p for p in self.problems if (p.cfg.temperature, p.table.seed) == k).grid
+            mu_ref = host_table_eval(np.asarray(TABLE_REFERENCE_X)[None, :], grid,
+                                     self.resolution)[0, :4]
+            self.tables.append(_table32(grid, mu_ref, torch))
         self.node_coord = torch.from_numpy(np.ascontiguousarray(self.problems[0].node_coord)).cuda()
         self.X_init = [torch.from_numpy(np.ascontiguousarray(p.X_init)).cuda() for p in self.problems]
         self._bk = []
