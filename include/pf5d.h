@@ -256,6 +256,12 @@ typedef struct {
   double dt0;
   int32_t oob_interval;
   const double *X;             /* device (*shape, 4) float64 initial field   */
+  /* Optional exact resume (continuous batching): when hi / lo are not NULL
+   * they seed X - X0 as the FP32 pair (device, 4 floats per point each)
+   * instead of X, and time0 / step0 seed the step state (dt from dt0). */
+  const float *hi, *lo;
+  double time0;
+  int64_t step0;
 } pf5d_batch_solve;
 
 typedef struct pf5d_batch pf5d_batch;
@@ -270,6 +276,9 @@ pf5d_status pf5d_batch_advance(pf5d_batch *h, int64_t nsteps, void *stream);
 /* out: nsolves entries; synchronises `stream`. */
 pf5d_status pf5d_batch_states(pf5d_batch *h, pf5d_step_state *out, void *stream);
 pf5d_status pf5d_batch_field(pf5d_batch *h, int32_t i, double *X_out, void *stream);
+/* Copy solve i's FP32 pair (X - X0 = hi + lo; device, 4 floats per point
+ * each) for an exact resume in another batch. */
+pf5d_status pf5d_batch_export(pf5d_batch *h, int32_t i, float *hi_out, float *lo_out, void *stream);
 pf5d_status pf5d_batch_autotune(pf5d_batch *h, int32_t *variant, float *best_ms, void *stream);
 pf5d_status pf5d_batch_set_variant(pf5d_batch *h, int32_t variant);
 pf5d_status pf5d_batch_destroy(pf5d_batch *h);

@@ -62,7 +62,8 @@ class BatchSolve(ctypes.Structure):
         ("elastic", _i32), ("lvec", _f64 * 4), ("bk", _f64p), ("table", _i32),
         ("max_nn_dist", _f64), ("ctld", _f64), ("t_cfl", _f64), ("lower_limit", _f64),
         ("upper_limit", _f64), ("max_change_factor", _f64), ("adaptive", _i32), ("dt0", _f64),
-        ("oob_interval", _i32), ("X", _vp),
+        ("oob_interval", _i32), ("X", _vp), ("hi", _vp), ("lo", _vp), ("time0", _f64),
+        ("step0", _i64),
     ]
 
 
@@ -109,6 +110,7 @@ _SIGS = {
     "pf5d_batch_advance": (_i32, [_vp, _i64, _vp]),
     "pf5d_batch_states": (_i32, [_vp, ctypes.POINTER(StepState), _vp]),
     "pf5d_batch_field": (_i32, [_vp, _i32, _vp, _vp]),
+    "pf5d_batch_export": (_i32, [_vp, _i32, _vp, _vp, _vp]),
     "pf5d_batch_autotune": (_i32, [_vp, ctypes.POINTER(_i32), ctypes.POINTER(ctypes.c_float),
                                    _vp]),
     "pf5d_batch_set_variant": (_i32, [_vp, _i32]),

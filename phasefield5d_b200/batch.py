@@ -36,7 +36,10 @@ class BatchStepper:
     together.  Problems with the same temperature share one device table,
     which stores mu - mu(TABLE_REFERENCE_X) and M in FP32."""
 
-    def __init__(self, problems, stream=None, autotune=True, oob_interval=100):
+    def __init__(self, problems, stream=None, autotune=True, oob_interval=100, resume=None):
+        """``resume[i]`` (optional): ``(hi, lo, dt, time, step)`` from
+        ``export(j)`` of another batch -- solve i then continues that state
+        exactly instead of starting from ``problems[i].X_init``."""
         import torch
         self._torch = torch
         self.L = _lib.load()
@@ -59,7 +62,11 @@ class BatchStepper:
                                      self.resolution)[0, :4]
             self.tables.append(_table32(grid, mu_ref, torch))
         self.node_coord = torch.from_numpy(np.ascontiguousarray(self.problems[0].node_coord)).cuda()
-        self.X_init = [torch.from_numpy(np.ascontiguousarray(p.X_init)).cuda() for p in self.problems]
+        resume = list(resume) if resume is not None else [None] * len(self.problems)
+        self._resume = resume
+        self.X_init = [None if r is not None else
+                       torch.from_numpy(np.ascontiguousarray(p.X_init)).cuda()
+                       for p, r in zip(self.problems, resume)]
         self._bk = []
         arr = (_lib.BatchSolve * len(self.problems))()
         for i, p in enumerate(self.problems):
@@ -87,7 +94,13 @@ class BatchStepper:
             q.adaptive = 1 if p.cfg.adaptive else 0
             q.dt0 = p.dt0
             q.oob_interval = int(oob_interval)
-            q.X = self.X_init[i].data_ptr()
+            r = resume[i]
+            if r is None:
+                q.X = self.X_init[i].data_ptr()
+            else:
+                hi, lo, dt, time, step = r
+                q.hi, q.lo = hi.data_ptr(), lo.data_ptr()
+                q.dt0, q.time0, q.step0 = float(dt), float(time), int(step)
         tabs = (ctypes.c_void_p * len(self.tables))(*[t.data_ptr() for t in self.tables])
         h = ctypes.c_void_p()
         _lib.check(self.L.pf5d_batch_create(arr, len(self.problems), tabs, len(self.tables),
@@ -119,6 +132,16 @@ class BatchStepper:
         out = self._torch.empty((*p.shape, 4), dtype=self._torch.float64, device="cuda")
         _lib.check(self.L.pf5d_batch_field(self.h, int(i), _lib.ptr(out), self._s()), "field")
         return out
+
+    def export(self, i):
+        """(hi, lo, dt, time, step) of solve i for an exact resume elsewhere."""
+        p = self.problems[i]
+        hi = self._torch.empty((p.n_points, 4), dtype=self._torch.float32, device="cuda")
+        lo = self._torch.empty_like(hi)
+        _lib.check(self.L.pf5d_batch_export(self.h, int(i), _lib.ptr(hi), _lib.ptr(lo), self._s()),
+                   "export")
+        st = self.states()[i]
+        return hi, lo, st["dt"], st["time"], st["step"]
 
     def autotune(self):
         v = ctypes.c_int32()

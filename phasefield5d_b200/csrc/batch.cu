@@ -299,6 +299,45 @@ __global__ void kb_split(const double *__restrict__ X, const BSolve *__restrict_
   }
 }
 
+// Exact resume of one solve from its FP32 pair: copy hi/lo, recompute the
+// misfit and the 1D partial sums exactly as the update kernel forms them.
+__global__ void kb_resume(const float4 *__restrict__ hi_in, const float4 *__restrict__ lo_in,
+                          const BSolve *__restrict__ solves, int si) {
+  __shared__ double red[kUpdThreads / 32];
+  const BSolve &B = solves[si];
+  const int tid = threadIdx.x;
+  for (int chunk = blockIdx.x; chunk < B.nchunks; chunk += gridDim.x) {
+    double ssum = 0.0;
+    for (int k = 0; k < kChunk / kUpdThreads; ++k) {
+      const int64_t p = (int64_t)chunk * kChunk + k * kUpdThreads + tid;
+      if (p >= B.npts) break;
+      const float4 H = hi_in[p], L = lo_in[p];
+      B.hi[p] = H;
+      B.lo[p] = L;
+      if (B.emode) {
+        const float h[S] = {H.x, H.y, H.z, H.w}, l[S] = {L.x, L.y, L.z, L.w};
+        float acc = 0.f;
+#pragma unroll
+        for (int c = 0; c < S; ++c) acc = fmaf(h[c] + l[c], B.lvec[c], acc);
+        B.s[p] = acc;
+        ssum += (double)acc;
+      }
+    }
+    if (B.emode == 1) {
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) ssum += __shfl_xor_sync(0xffffffffu, ssum, o);
+      __syncthreads();
+      if ((tid & 31) == 0) red[tid >> 5] = ssum;
+      __syncthreads();
+      if (tid == 0) {
+        double v = 0.0;
+        for (int w = 0; w < kUpdThreads / 32; ++w) v += red[w];
+        B.spart[chunk] = v;
+      }
+    }
+  }
+}
+
 __global__ void kb_join(const BSolve *__restrict__ solves, int si, double *__restrict__ X) {
   const BSolve &B = solves[si];
   for (int64_t p = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; p < B.npts;
@@ -504,7 +543,7 @@ pf5d_status pf5d_batch_create(const pf5d_batch_solve *solves, int32_t nsolves,
   std::map<std::pair<int, int>, std::vector<int>> by_shape;
   for (int i = 0; i < nsolves; ++i) {
     const pf5d_batch_solve &q = solves[i];
-    if (q.dim < 1 || q.dim > 2 || q.table < 0 || q.table >= ntables || !q.X) {
+    if (q.dim < 1 || q.dim > 2 || q.table < 0 || q.table >= ntables || !(q.X || (q.hi && q.lo))) {
       set_error("solve %d: batched solves must be 1D or 2D with a valid table and field", i);
       return fail(PF5D_ERR_ARG);
     }
@@ -652,6 +691,10 @@ pf5d_status pf5d_batch_create(const pf5d_batch_solve *solves, int32_t nsolves,
     P.st = h->st + i;
     init[i] = StepState32{};
     init[i].dt = q.dt0;
+    if (q.hi && q.lo) {
+      init[i].time = q.time0;
+      init[i].step = q.step0;
+    }
     h->solves.push_back(b);
   }
   h->total_chunks = (int)chunk;
@@ -665,8 +708,13 @@ pf5d_status pf5d_batch_create(const pf5d_batch_solve *solves, int32_t nsolves,
   pf5d_status st = configure_batch(h, 0);
   if (st != PF5D_OK) return fail(st);
   for (int i = 0; i < nsolves; ++i) {
-    kb_split<<<std::max(1, std::min(h->solves[i].nchunks, 1024)), kUpdThreads, 0, s>>>(
-        solves[i].X, h->d_solves, i);
+    const unsigned g = std::max(1, std::min(h->solves[i].nchunks, 1024));
+    if (solves[i].hi && solves[i].lo)
+      kb_resume<<<g, kUpdThreads, 0, s>>>(reinterpret_cast<const float4 *>(solves[i].hi),
+                                          reinterpret_cast<const float4 *>(solves[i].lo),
+                                          h->d_solves, i);
+    else
+      kb_split<<<g, kUpdThreads, 0, s>>>(solves[i].X, h->d_solves, i);
     if (cudaGetLastError() != cudaSuccess) {
       set_error("split launch failed");
       return fail(PF5D_ERR_CUDA);
@@ -717,6 +765,17 @@ pf5d_status pf5d_batch_field(pf5d_batch *h, int32_t i, double *X_out, void *stre
   kb_join<<<grid_for(h->solves[i].npts, 256, 2), 256, 0, as_stream(stream)>>>(h->d_solves, i,
                                                                               X_out);
   PF5D_LAUNCHED();
+  return PF5D_OK;
+}
+
+pf5d_status pf5d_batch_export(pf5d_batch *h, int32_t i, float *hi_out, float *lo_out,
+                              void *stream) {
+  PF5D_REQUIRE(h && hi_out && lo_out && i >= 0 && i < (int)h->solves.size(), PF5D_ERR_ARG,
+               "bad arguments");
+  const BSolve &b = h->solves[i];
+  cudaStream_t s = as_stream(stream);
+  PF5D_CUDA(cudaMemcpyAsync(hi_out, b.hi, b.npts * sizeof(float4), cudaMemcpyDeviceToDevice, s));
+  PF5D_CUDA(cudaMemcpyAsync(lo_out, b.lo, b.npts * sizeof(float4), cudaMemcpyDeviceToDevice, s));
   return PF5D_OK;
 }
 

@@ -1,0 +1,318 @@
+"""Serving form: a continuous-batching solve server on one GPU.
+
+Requests (a ``workload.Problem`` plus a step count) arrive over time.  The
+server admits them while batch slots and free HBM allow, keeps their fields
+and the temperature tables resident on the device, and advances all admitted
+solves together in step blocks:
+
+* 1D and 2D solves share one batched stepper (``batch.BatchStepper``);
+  whenever membership changes (a request admitted, finished, halted or
+  cancelled) the batch is rebuilt and every continuing solve resumes its
+  exact FP32 state (hi/lo pair, dt, time, step), so a request's trajectory
+  does not depend on when others come and go;
+* 3D solves each get their own FP32-compensated ``Stepper`` on their own
+  stream, so their work overlaps the batch on the device.
+
+A step block never takes a solve past its requested step count.  Each
+finished request records its time to solution (arrival to result on the
+host); ``stats()`` gives p50/p99 and the aggregate grid-point steps/s.
+
+Scheduling (``Scheduler``) is separate from the device work (``GpuBackend``)
+so the admission and block logic can be exercised with a fake backend.
+"""
+from __future__ import annotations
+
+import time
+from dataclasses import dataclass, field
+
+import numpy as np
+
+# Device bytes per grid point of an admitted FP32-compensated solve: hi, lo
+# and dX/dt (3 x 16), the misfit scalar and its half spectrum (~4 + 8), and
+# working room for cuFFT (16).
+BYTES_PER_POINT = 96
+FIXED_BYTES_PER_SOLVE = 4 << 20
+
+
+@dataclass
+class Request:
+    rid: int
+    problem: object
+    n_steps: int
+    arrival: float = 0.0
+    status: str = "queued"          # queued, active, done, halted, cancelled
+    admitted: float | None = None
+    done: float | None = None
+    steps_done: int = 0
+    result: np.ndarray | None = None
+    final_state: dict | None = None
+
+    @property
+    def dim(self):
+        return self.problem.dim
+
+    @property
+    def n_points(self):
+        return int(self.problem.n_points)
+
+    @property
+    def remaining(self):
+        return self.n_steps - self.steps_done
+
+    def device_bytes(self):
+        return BYTES_PER_POINT * self.n_points + FIXED_BYTES_PER_SOLVE
+
+
+class Scheduler:
+    """Admission, step blocks and retirement, independent of the device.
+
+    ``backend`` provides: ``sync(active)`` (make the device set match the
+    active requests), ``advance(blocks)`` (steps per request id),
+    ``states()`` (request id -> state dict), ``collect(req)`` (host field),
+    ``free_bytes()``.
+    """
+
+    def __init__(self, backend, max_slots=64, step_block=50, reserve_bytes=1 << 30,
+                 clock=time.perf_counter):
+        self.backend = backend
+        self.max_slots = int(max_slots)
+        self.step_block = int(step_block)
+        self.reserve = int(reserve_bytes)
+        self.clock = clock
+        self.t0 = None
+        self.queue: list[Request] = []
+        self.active: list[Request] = []
+        self.finished: list[Request] = []
+        self.points_steps = 0
+
+    def now(self):
+        if self.t0 is None:
+            self.t0 = self.clock()
+        return self.clock() - self.t0
+
+    def submit(self, req: Request):
+        self.queue.append(req)
+        self.queue.sort(key=lambda r: r.arrival)
+
+    def cancel(self, rid):
+        for r in list(self.queue):
+            if r.rid == rid:
+                self.queue.remove(r)
+                r.status = "cancelled"
+                self.finished.append(r)
+                return True
+        for r in list(self.active):
+            if r.rid == rid:
+                self.active.remove(r)
+                r.status = "cancelled"
+                r.done = self.now()
+                self.finished.append(r)
+                self.backend.sync(self.active)
+                return True
+        return False
+
+    def admit(self):
+        """Admit arrived requests in arrival order while slots and HBM allow."""
+        now = self.now()
+        admitted = []
+        free = self.backend.free_bytes()
+        for r in list(self.queue):
+            if r.arrival > now or len(self.active) >= self.max_slots:
+                break
+            need = r.device_bytes()
+            if free - need < self.reserve:
+                break                       # head-of-line: keep arrival order
+            self.queue.remove(r)
+            r.status, r.admitted = "active", now
+            self.active.append(r)
+            admitted.append(r)
+            free -= need
+        return admitted
+
+    def block_sizes(self):
+        """Steps each active request advances this block: the step block, cut
+        so no 1D/2D request (they move in lockstep) passes its count."""
+        shared = [r for r in self.active if r.dim < 3]
+        n_shared = min([self.step_block] + [r.remaining for r in shared]) if shared else 0
+        return {r.rid: (n_shared if r.dim < 3 else min(self.step_block, r.remaining))
+                for r in self.active}
+
+    def tick(self):
+        """One scheduling iteration; returns False when nothing is left."""
+        changed = bool(self.admit())
+        if changed:
+            self.backend.sync(self.active)
+        if not self.active:
+            if not self.queue:
+                return False
+            wait = self.queue[0].arrival - self.now()
+            if wait > 0:
+                time.sleep(min(wait, 0.01))
+            return True
+        blocks = self.block_sizes()
+        self.backend.advance(blocks)
+        states = self.backend.states()
+        retired = False
+        for r in list(self.active):
+            st = states[r.rid]
+            self.points_steps += r.n_points * (st["step"] - r.steps_done)
+            r.steps_done = st["step"]
+            if st["halted"] or r.steps_done >= r.n_steps:
+                r.status = "halted" if st["halted"] else "done"
+                r.final_state = st
+                r.result = self.backend.collect(r)
+                r.done = self.now()
+                self.active.remove(r)
+                self.finished.append(r)
+                retired = True
+        if retired:
+            self.backend.sync(self.active)
+        return True
+
+    def run(self, timeout=None):
+        start = self.now()
+        while self.tick():
+            if timeout is not None and self.now() - start > timeout:
+                break
+        return self.stats()
+
+    def stats(self):
+        done = [r for r in self.finished if r.status == "done"]
+        tts = np.array([r.done - r.arrival for r in done]) if done else np.array([np.nan])
+        span = (max(r.done for r in done) - min(r.arrival for r in done)) if done else np.nan
+        return {
+            "requests_done": len(done),
+            "requests_halted": sum(r.status == "halted" for r in self.finished),
+            "requests_cancelled": sum(r.status == "cancelled" for r in self.finished),
+            "p50_time_to_solution_s": float(np.percentile(tts, 50)),
+            "p99_time_to_solution_s": float(np.percentile(tts, 99)),
+            "grid_point_steps_per_s": float(self.points_steps / span) if done else float("nan"),
+            "wall_s": float(span),
+        }
+
+
+class GpuBackend:
+    """Device side of the server: one batch for 1D/2D, one stepper per 3D."""
+
+    def __init__(self, device=0):
+        import torch
+        from .batch import BatchStepper
+        from .stepper import Stepper
+        self.torch = torch
+        self.BatchStepper = BatchStepper
+        self.Stepper = Stepper
+        torch.cuda.set_device(device)
+        self.batch = None
+        self.batch_ids: list[int] = []
+        self.steppers: dict[int, object] = {}
+        self.streams: dict[int, object] = {}
+        self.reqs: dict[int, Request] = {}
+        self.batch_stream = torch.cuda.Stream()
+        self.variants: dict[tuple, int] = {}      # 3D shape -> autotuned kernel variant
+
+    def free_bytes(self):
+        free, _total = self.torch.cuda.mem_get_info()
+        return int(free)
+
+    def sync(self, active):
+        torch = self.torch
+        ids = [r.rid for r in active]
+        self.reqs = {r.rid: r for r in active}
+        for rid in list(self.steppers):
+            if rid not in ids:
+                self.steppers.pop(rid).close()
+                self.streams.pop(rid)
+        for r in active:
+            if r.dim == 3 and r.rid not in self.steppers:
+                s = torch.cuda.Stream()
+                key = tuple(r.problem.shape)
+                with torch.cuda.stream(s):
+                    st = self.Stepper.from_problem(r.problem, precision="fp32c", stream=s,
+                                                   autotune=key not in self.variants)
+                    if key in self.variants:
+                        st.set_variant(self.variants[key])
+                    else:
+                        self.variants[key] = st.variant
+                self.steppers[r.rid] = st
+                self.streams[r.rid] = s
+        want = [r.rid for r in active if r.dim < 3]
+        if want == self.batch_ids:
+            return
+        resume = {}
+        if self.batch is not None:
+            with torch.cuda.stream(self.batch_stream):
+                for k, rid in enumerate(self.batch_ids):
+                    if rid in want:
+                        resume[rid] = self.batch.export(k)
+            self.batch_stream.synchronize()
+            self.batch.close()
+            self.batch = None
+        self.batch_ids = want
+        if want:
+            with torch.cuda.stream(self.batch_stream):
+                self.batch = self.BatchStepper([self.reqs[i].problem for i in want],
+                                               stream=self.batch_stream, autotune=False,
+                                               resume=[resume.get(i) for i in want])
+
+    def advance(self, blocks):
+        if self.batch is not None and self.batch_ids:
+            n = blocks[self.batch_ids[0]]
+            if n > 0:
+                self.batch.advance(n)
+        for rid, st in self.steppers.items():
+            if blocks.get(rid, 0) > 0:
+                st.advance(blocks[rid])
+        self.torch.cuda.synchronize()
+
+    def states(self):
+        out = {}
+        if self.batch is not None:
+            for rid, st in zip(self.batch_ids, self.batch.states()):
+                out[rid] = st
+        for rid, st in self.steppers.items():
+            out[rid] = st.state()
+        return out
+
+    def collect(self, req):
+        if req.rid in self.steppers:
+            return self.steppers[req.rid].field().cpu().numpy()
+        k = self.batch_ids.index(req.rid)
+        return self.batch.field(k).cpu().numpy()
+
+
+class Server(Scheduler):
+    """Scheduler + GPU backend."""
+
+    def __init__(self, device=0, **kw):
+        super().__init__(GpuBackend(device), **kw)
+
+
+# ---------------------------------------------------------------------------
+# Request streams
+# ---------------------------------------------------------------------------
+
+def poisson_arrivals(rate, n, seed=0):
+    """Arrival times (s) of n requests of a Poisson process of `rate` req/s."""
+    rng = np.random.default_rng(seed)
+    return np.cumsum(rng.exponential(1.0 / rate, size=n))
+
+
+def serving_configs(n, seed=0, steps=2000, sizes_3d=(64, 96, 128, 160, 192)):
+    """The serving mix: 1D 4096, 2D 256^2 and 3D 64^3-192^3 requests (equal
+    shares), random compositions, kappa log-uniform in [1e-16, 1e-14], one
+    of the four temperature tables, `steps` adaptive steps each."""
+    from .workload import BATCH_TEMPERATURES, SolveConfig, random_composition
+    rng = np.random.default_rng(seed)
+    cfgs = []
+    for i in range(n):
+        kind = i % 3
+        shape = [(4096,), (256, 256), None][kind]
+        if shape is None:
+            m = int(rng.choice(sizes_3d))
+            shape = (m, m, m)
+        cfgs.append(SolveConfig(
+            system_dim=len(shape), initial_composition=random_composition(rng),
+            kappa_value=float(10 ** rng.uniform(-16, -14)), resolution=0.025,
+            temperature=BATCH_TEMPERATURES[int(rng.integers(0, 4))], shape=shape, adaptive=True,
+            total_timesteps=steps, ic_seed=1000 + i, n_k=2000))
+    return cfgs
