@@ -67,6 +67,13 @@ def parse():
                     help="steps of the FP32c-vs-FP64 accuracy report")
     ap.add_argument("--cpu-steps", type=int, default=3, help="steps in the CPU-baseline sample")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--forms", default="fp32c,batch,serve",
+                    help="extra measurements at N=1 (comma list of fp32c, batch, serve; 'none')")
+    ap.add_argument("--batch-steps", type=int, default=1000,
+                    help="timed steps of the 64-solve batched form (and its FP64 comparison)")
+    ap.add_argument("--serve-requests", type=int, default=12)
+    ap.add_argument("--serve-rates", default="1,10,50", help="Poisson arrival rates, req/s")
+    ap.add_argument("--serve-steps", type=int, default=2000)
     return ap.parse_args()
 
 
@@ -199,6 +206,194 @@ def run_reference(args, rank):
                 "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
+
+
+def _events(torch):
+    return torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+
+
+def _stepper_timing(prob, precision, args, flush, torch):
+    """Device-resident one-step timing with L2 flushed between steps, and the
+    fused rate kernel launched alone: (ms per step, rate ms, variant)."""
+    from phasefield5d_b200 import _lib
+    from phasefield5d_b200.stepper import Stepper
+    stream = torch.cuda.current_stream()
+    st = Stepper.from_problem(prob, precision=precision)
+    st.advance(1)
+    for _ in range(args.warmup):
+        flush.zero_()
+        st.advance(1)
+    ev = []
+    for _ in range(args.steps):
+        flush.zero_()
+        a, b = _events(torch)
+        a.record(stream)
+        st.advance(1)
+        b.record(stream)
+        ev.append((a, b))
+    torch.cuda.synchronize()
+    step_ms = sum(a.elapsed_time(b) for a, b in ev) / len(ev)
+    rate = []
+    for _ in range(3):
+        st.launch_stage(_lib.STAGE_RATE)
+    for _ in range(max(args.steps, 10)):
+        flush.zero_()
+        a, b = _events(torch)
+        a.record(stream)
+        st.launch_stage(_lib.STAGE_RATE)
+        b.record(stream)
+        rate.append((a, b))
+    torch.cuda.synchronize()
+    rate_ms = sum(a.elapsed_time(b) for a, b in rate) / len(rate)
+    variant = st.variant
+    st.close()
+    return step_ms, rate_ms, variant
+
+
+def form_fp32c(prob, args, flush, torch):
+    """FP32-compensated form on the headline workload, with its accuracy
+    report against the plain FP64 form (max/RMS error, mass drift)."""
+    from phasefield5d_b200.precision import compare_forms
+    peak, peak_kind = measured_peak()
+    P = prob.n_points
+    step_ms, rate_ms, variant = _stepper_timing(prob, "fp32c", args, flush, torch)
+    rate_bytes = RATE_BYTES_FP32C * P
+    value = P / (step_ms * 1e-3)
+    out = {"value": value, "unit": "grid-point steps/s", "ms_per_step": step_ms,
+           "l2": "flushed (256 MiB write) between timed steps", "rate_variant": variant,
+           "rate_kernel": {"ms_per_launch": rate_ms,
+                           "achieved_gbs": rate_bytes / (rate_ms * 1e-3) / 1e9,
+                           "algorithmic_bytes_per_launch": rate_bytes,
+                           "frac": rate_bytes / (rate_ms * 1e-3) / 1e9 / peak,
+                           "peak_kind": peak_kind},
+           "step_roofline": {"bytes_per_grid_point_step": STEP_BYTES_FP32C,
+                             "achieved_gbs": STEP_BYTES_FP32C * value / 1e9,
+                             "frac": STEP_BYTES_FP32C * value / 1e9 / peak}}
+    if args.accuracy_steps > 0:
+        out["accuracy_vs_fp64"] = compare_forms(prob, args.accuracy_steps)
+    return out
+
+
+def form_batch(args, flush, torch):
+    """The 64-solve batched FP32-compensated form (uneven 1D 2048-8192 and
+    2D 128^2-384^2 grids, four temperature tables) against the plain FP64
+    form on the same 64 solves, each on its own stream.  Both run the same
+    steps; the accuracy report compares every solve's field afterwards."""
+    from phasefield5d_b200 import workload as W
+    from phasefield5d_b200.batch import BatchStepper
+    from phasefield5d_b200.stepper import Stepper
+    probs, _ = W.build_batched_problems(W.batched_configs(64))
+    P = sum(p.n_points for p in probs)
+    block = 50
+    n_blocks = max(args.batch_steps // block, 1)
+    n_warm = 3
+    stream = torch.cuda.current_stream()
+
+    b = BatchStepper(probs, stream=stream)
+    for _ in range(n_warm):
+        b.advance(block)
+    ev = []
+    for _ in range(n_blocks):
+        flush.zero_()
+        e0, e1 = _events(torch)
+        e0.record(stream)
+        b.advance(block)
+        e1.record(stream)
+        ev.append((e0, e1))
+    torch.cuda.synchronize()
+    batch_ms = sum(x.elapsed_time(y) for x, y in ev) / (n_blocks * block)
+
+    streams = [torch.cuda.Stream() for _ in probs]
+    singles = []
+    for p, s in zip(probs, streams):
+        with torch.cuda.stream(s):
+            singles.append(Stepper.from_problem(p, precision="fp64", stream=s))
+    torch.cuda.synchronize()
+
+    def fp64_block():
+        e0, e1 = _events(torch)
+        e0.record(stream)
+        for st, s in zip(singles, streams):
+            s.wait_event(e0)
+            st.advance(block)
+            stream.wait_stream(s)
+        e1.record(stream)
+        return e0, e1
+
+    for _ in range(n_warm):
+        fp64_block()
+    ev = []
+    for _ in range(n_blocks):
+        flush.zero_()
+        ev.append(fp64_block())
+    torch.cuda.synchronize()
+    fp64_ms = sum(x.elapsed_time(y) for x, y in ev) / (n_blocks * block)
+
+    errs, rms, drift = [], [], []
+    states = b.states()
+    for i, (p, st) in enumerate(zip(probs, singles)):
+        if states[i]["halted"] or st.state()["halted"]:
+            raise RuntimeError(f"batched solve {i} halted during the benchmark")
+        xb = b.field(i).cpu().numpy().reshape(-1, 4)
+        x64 = st.field().cpu().numpy().reshape(-1, 4)
+        scale = np.max(np.abs(x64))
+        errs.append(float(np.max(np.abs(xb - x64)) / scale))
+        rms.append(float(np.sqrt(np.mean((xb - x64) ** 2)) / scale))
+        drift.append(float(np.max(np.abs(xb.mean(axis=0) - p.X_init.reshape(-1, 4).mean(axis=0)))))
+        st.close()
+    variant, tuned = b.variant, b.tuned_ms
+    b.close()
+    v_b = P / (batch_ms * 1e-3)
+    v_64 = P / (fp64_ms * 1e-3)
+    return {"solves": len(probs), "grid_points": P, "steps": (n_warm + n_blocks) * block,
+            "timed_steps": n_blocks * block,
+            "fp32c_batched": {"value": v_b, "unit": "grid-point steps/s", "ms_per_step": batch_ms,
+                              "variant": variant, "tuned_rate_ms": tuned,
+                              "bytes_per_grid_point_step": STEP_BYTES_FP32C,
+                              "step_roofline_frac": STEP_BYTES_FP32C * v_b / 1e9 / measured_peak()[0]},
+            "fp64_streams": {"value": v_64, "unit": "grid-point steps/s", "ms_per_step": fp64_ms,
+                             "note": "64 plain FP64 steppers, one stream each, 50-step graphs"},
+            "speedup_fp32c_batched_vs_fp64": v_b / v_64,
+            "max_rel_err_vs_fp64": max(errs), "rms_rel_err_vs_fp64_max": max(rms),
+            "mass_drift_max_fp32c": max(drift),
+            "timing": "CUDA events around each 50-step graph launch, L2 flushed between blocks",
+            "note": "the workload runs 10,000 steps per solve; a fixed number of steps is "
+                    "timed (per-step cost does not depend on the step index)"}
+
+
+def form_serve(args):
+    """The serving form: Poisson streams of mixed 1D 4096 / 2D 256^2 / 3D
+    64^3-192^3 requests at each rate, FP32-compensated continuous batching
+    against one plain FP64 stepper per request."""
+    import copy
+    from phasefield5d_b200 import workload as W
+    from phasefield5d_b200.serving import Request, Server, poisson_arrivals, serving_configs
+    cfgs = serving_configs(args.serve_requests, seed=0, steps=args.serve_steps)
+    probs, _ = W.build_batched_problems(cfgs)
+    rates = [float(r) for r in args.serve_rates.split(",") if r]
+    out = {"requests": len(probs), "steps_per_request": args.serve_steps,
+           "mix": [list(p.shape) for p in probs], "rates": {}}
+    variants = {}
+    for prec in ("fp32c", "fp64"):           # untimed pass: autotune each shape once
+        warm = Server(precision=prec, reserve_bytes=1 << 30)
+        for i, p in enumerate(probs):
+            warm.submit(Request(rid=i, problem=p, n_steps=50, arrival=0.0))
+        warm.run(timeout=600)
+        variants[prec] = dict(warm.backend.variants)
+    for rate in rates:
+        arr = poisson_arrivals(rate, len(probs), seed=int(rate * 1000))
+        row = {}
+        for prec in ("fp32c", "fp64"):
+            srv = Server(precision=prec, reserve_bytes=1 << 30)
+            srv.backend.variants = dict(variants[prec])
+            for i, (p, a) in enumerate(zip(probs, arr)):
+                srv.submit(Request(rid=i, problem=copy.copy(p), n_steps=args.serve_steps,
+                                   arrival=float(a)))
+            row[prec] = srv.run(timeout=900)
+        out["rates"][f"{rate:g}"] = row
+    out["timing"] = ("host clock: arrival to result on the host per request; "
+                     "throughput = grid-point steps / (last result - first arrival)")
+    return out
 
 
 def run_ours(args, rank, world, local_rank):
@@ -364,8 +559,18 @@ def run_ours(args, rank, world, local_rank):
     if fp32c and args.accuracy_steps > 0:
         from phasefield5d_b200.precision import compare_forms
         line["accuracy_vs_fp64"] = compare_forms(prob, args.accuracy_steps)
-    print(json.dumps(line), flush=True)
     st.close()
+    forms = [f for f in args.forms.split(",") if f and f != "none"]
+    if world == 1 and forms:
+        extra = {}
+        if "fp32c" in forms and not fp32c:
+            extra["fp32c_same_workload"] = form_fp32c(prob, args, flush, torch)
+        if "batch" in forms:
+            extra["batch64"] = form_batch(args, flush, torch)
+        if "serve" in forms:
+            extra["serving"] = form_serve(args)
+        line["forms"] = extra
+    print(json.dumps(line), flush=True)
 
 
 def main():

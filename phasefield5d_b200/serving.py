@@ -13,6 +13,10 @@ solves together in step blocks:
 * 3D solves each get their own FP32-compensated ``Stepper`` on their own
   stream, so their work overlaps the batch on the device.
 
+``GpuBackend(precision="fp64")`` is the plain-FP64 comparison: every request
+gets its own bit-faithful FP64 ``Stepper`` on its own stream (the FP64 form
+has no batched kernel), with the same admission and step blocks.
+
 A step block never takes a solve past its requested step count.  Each
 finished request records its time to solution (arrival to result on the
 host); ``stats()`` gives p50/p99 and the aggregate grid-point steps/s.
@@ -31,6 +35,9 @@ import numpy as np
 # and dX/dt (3 x 16), the misfit scalar and its half spectrum (~4 + 8), and
 # working room for cuFFT (16).
 BYTES_PER_POINT = 96
+# The plain FP64 form: X and dX/dt (2 x 32), the FP64 misfit scalar and its
+# half spectrum (8 + 16), cuFFT working room (32).
+BYTES_PER_POINT_FP64 = 120
 FIXED_BYTES_PER_SOLVE = 4 << 20
 
 
@@ -59,8 +66,8 @@ class Request:
     def remaining(self):
         return self.n_steps - self.steps_done
 
-    def device_bytes(self):
-        return BYTES_PER_POINT * self.n_points + FIXED_BYTES_PER_SOLVE
+    def device_bytes(self, bytes_per_point=BYTES_PER_POINT):
+        return bytes_per_point * self.n_points + FIXED_BYTES_PER_SOLVE
 
 
 class Scheduler:
@@ -119,7 +126,7 @@ class Scheduler:
         for r in list(self.queue):
             if r.arrival > now or len(self.active) >= self.max_slots:
                 break
-            need = r.device_bytes()
+            need = r.device_bytes(getattr(self.backend, "bytes_per_point", BYTES_PER_POINT))
             if free - need < self.reserve:
                 break                       # head-of-line: keep arrival order
             self.queue.remove(r)
@@ -131,10 +138,12 @@ class Scheduler:
 
     def block_sizes(self):
         """Steps each active request advances this block: the step block, cut
-        so no 1D/2D request (they move in lockstep) passes its count."""
-        shared = [r for r in self.active if r.dim < 3]
+        so no request of the shared batch (they move in lockstep) passes its
+        count."""
+        in_batch = getattr(self.backend, "shares_batch", lambda r: r.dim < 3)
+        shared = [r for r in self.active if in_batch(r)]
         n_shared = min([self.step_block] + [r.remaining for r in shared]) if shared else 0
-        return {r.rid: (n_shared if r.dim < 3 else min(self.step_block, r.remaining))
+        return {r.rid: (n_shared if in_batch(r) else min(self.step_block, r.remaining))
                 for r in self.active}
 
     def tick(self):
@@ -192,10 +201,16 @@ class Scheduler:
 
 
 class GpuBackend:
-    """Device side of the server: one batch for 1D/2D, one stepper per 3D."""
+    """Device side of the server.  ``precision="fp32c"``: one batch for the
+    1D/2D requests, one FP32-compensated stepper per 3D request.
+    ``precision="fp64"``: one plain FP64 stepper per request."""
 
-    def __init__(self, device=0):
+    def __init__(self, device=0, precision="fp32c"):
         import torch
+        if precision not in ("fp32c", "fp64"):
+            raise ValueError(f"unknown precision {precision!r}")
+        self.precision = precision
+        self.bytes_per_point = BYTES_PER_POINT if precision == "fp32c" else BYTES_PER_POINT_FP64
         from .batch import BatchStepper
         from .stepper import Stepper
         self.torch = torch
@@ -208,7 +223,11 @@ class GpuBackend:
         self.streams: dict[int, object] = {}
         self.reqs: dict[int, Request] = {}
         self.batch_stream = torch.cuda.Stream()
-        self.variants: dict[tuple, int] = {}      # 3D shape -> autotuned kernel variant
+        self.variants: dict[tuple, int] = {}      # shape -> autotuned kernel variant
+
+    def shares_batch(self, req):
+        """True when the request advances in the shared 1D/2D batch."""
+        return self.precision == "fp32c" and req.dim < 3
 
     def free_bytes(self):
         free, _total = self.torch.cuda.mem_get_info()
@@ -223,11 +242,11 @@ class GpuBackend:
                 self.steppers.pop(rid).close()
                 self.streams.pop(rid)
         for r in active:
-            if r.dim == 3 and r.rid not in self.steppers:
+            if not self.shares_batch(r) and r.rid not in self.steppers:
                 s = torch.cuda.Stream()
                 key = tuple(r.problem.shape)
                 with torch.cuda.stream(s):
-                    st = self.Stepper.from_problem(r.problem, precision="fp32c", stream=s,
+                    st = self.Stepper.from_problem(r.problem, precision=self.precision, stream=s,
                                                    autotune=key not in self.variants)
                     if key in self.variants:
                         st.set_variant(self.variants[key])
@@ -235,7 +254,7 @@ class GpuBackend:
                         self.variants[key] = st.variant
                 self.steppers[r.rid] = st
                 self.streams[r.rid] = s
-        want = [r.rid for r in active if r.dim < 3]
+        want = [r.rid for r in active if self.shares_batch(r)]
         if want == self.batch_ids:
             return
         resume = {}
@@ -283,8 +302,8 @@ class GpuBackend:
 class Server(Scheduler):
     """Scheduler + GPU backend."""
 
-    def __init__(self, device=0, **kw):
-        super().__init__(GpuBackend(device), **kw)
+    def __init__(self, device=0, precision="fp32c", **kw):
+        super().__init__(GpuBackend(device, precision), **kw)
 
 
 # ---------------------------------------------------------------------------

@@ -68,3 +68,18 @@ def test_poisson_stream_completes(torch_cuda):
     assert st["requests_done"] == len(reqs)
     assert 0 < st["p50_time_to_solution_s"] <= st["p99_time_to_solution_s"]
     assert st["grid_point_steps_per_s"] > 0
+
+
+def test_fp64_backend_alone_equals_mix(torch_cuda):
+    """The plain-FP64 comparison backend (one FP64 stepper per request):
+    every request's result is bit-identical alone and in the mix."""
+    import copy
+    reqs = _requests(steps=60)[:4]
+    srv, st = _serve([copy.copy(r) for r in reqs], [0.0, 0.01, 0.02, 0.03], precision="fp64")
+    assert st["requests_done"] == len(reqs)
+    mixed = {r.rid: r for r in srv.finished}
+    for r in reqs:
+        alone_srv, _st = _serve([copy.copy(r)], [0.0], precision="fp64")
+        alone = alone_srv.finished[0]
+        assert alone.final_state["step"] == mixed[r.rid].final_state["step"] == r.n_steps
+        assert np.array_equal(alone.result, mixed[r.rid].result), r.rid
