@@ -36,10 +36,14 @@ class BatchStepper:
     together.  Problems with the same temperature share one device table,
     which stores mu - mu(TABLE_REFERENCE_X) and M in FP32."""
 
-    def __init__(self, problems, stream=None, autotune=True, oob_interval=100, resume=None):
+    def __init__(self, problems, stream=None, autotune=True, oob_interval=100, resume=None,
+                 table_cache=None):
         """``resume[i]`` (optional): ``(hi, lo, dt, time, step)`` from
         ``export(j)`` of another batch -- solve i then continues that state
-        exactly instead of starting from ``problems[i].X_init``."""
+        exactly instead of starting from ``problems[i].X_init``.
+        ``table_cache`` (optional dict): device tables kept across batches,
+        keyed by (temperature, table seed, resolution); a batch rebuilt for
+        new membership then reuses the resident tables."""
         import torch
         self._torch = torch
         self.L = _lib.load()
@@ -56,11 +60,16 @@ class BatchStepper:
                 keys.append(k)
         self.table_keys = keys
         self.tables = []
+        cache = table_cache if table_cache is not None else {}
         for k in keys:
-            grid = next(p for p in self.problems if (p.cfg.temperature, p.table.seed) == k).grid
-            mu_ref = host_table_eval(np.asarray(TABLE_REFERENCE_X)[None, :], grid,
-                                     self.resolution)[0, :4]
-            self.tables.append(_table32(grid, mu_ref, torch))
+            ck = (*k, self.resolution)
+            if ck not in cache:
+                grid = next(p for p in self.problems
+                            if (p.cfg.temperature, p.table.seed) == k).grid
+                mu_ref = host_table_eval(np.asarray(TABLE_REFERENCE_X)[None, :], grid,
+                                         self.resolution)[0, :4]
+                cache[ck] = _table32(grid, mu_ref, torch)
+            self.tables.append(cache[ck])
         self.node_coord = torch.from_numpy(np.ascontiguousarray(self.problems[0].node_coord)).cuda()
         resume = list(resume) if resume is not None else [None] * len(self.problems)
         self._resume = resume

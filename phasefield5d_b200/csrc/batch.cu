@@ -406,6 +406,9 @@ const std::vector<BatchVariant> &batch_variants() {
   return v;
 }
 
+// Parallel FFT branches of a batch step graph (one stream per branch).
+constexpr int kFftBranches = 8;
+
 struct ShapeGroup {
   int ny, nx, count;
   int64_t s_off, k_off, nk;
@@ -430,6 +433,13 @@ struct pf5d_batch {
   int total_tiles = 0, total_chunks = 0;
   int variant = 0, rate_grid = 1, upd_grid = 1;
   cudaStream_t cap = nullptr;
+  // Shape groups' FFT chains run as parallel branches of the step graph:
+  // forked from the capture stream onto `aux`, joined back before the rate
+  // kernel.  `order` lists the groups largest first, dealt round-robin.
+  std::vector<cudaStream_t> aux;
+  std::vector<cudaEvent_t> join;
+  cudaEvent_t fork = nullptr;
+  std::vector<int> order;
   std::map<int64_t, cudaGraphExec_t> graphs;
   int64_t total_points = 0;
 };
@@ -467,20 +477,31 @@ pf5d_status configure_batch(pf5d_batch *h, int variant) {
 }
 
 pf5d_status enqueue_batch_step(pf5d_batch *h, cudaStream_t s) {
-  for (auto &g : h->groups) {
-    if (cufftSetStream(g.fwd, s) != CUFFT_SUCCESS ||
+  const int na = std::min<int>((int)h->groups.size(), (int)h->aux.size());
+  if (na > 0) {
+    PF5D_CUDA(cudaEventRecord(h->fork, s));
+    for (int a = 0; a < na; ++a) PF5D_CUDA(cudaStreamWaitEvent(h->aux[a], h->fork, 0));
+  }
+  for (int j = 0; j < (int)h->order.size(); ++j) {
+    ShapeGroup &g = h->groups[h->order[j]];
+    cudaStream_t gs = h->aux[j % na];
+    if (cufftSetStream(g.fwd, gs) != CUFFT_SUCCESS ||
         cufftExecR2C(g.fwd, h->s + g.s_off, h->k + g.k_off) != CUFFT_SUCCESS) {
       set_error("batch cuFFT R2C failed");
       return PF5D_ERR_CUFFT;
     }
     const int64_t total = g.nk * g.count;
-    kb_bmul<<<grid_for(total, 256), 256, 0, s>>>(h->k + g.k_off, g.bk, g.nk, total);
+    kb_bmul<<<grid_for(total, 256), 256, 0, gs>>>(h->k + g.k_off, g.bk, g.nk, total);
     PF5D_LAUNCHED();
-    if (cufftSetStream(g.inv, s) != CUFFT_SUCCESS ||
+    if (cufftSetStream(g.inv, gs) != CUFFT_SUCCESS ||
         cufftExecC2R(g.inv, h->k + g.k_off, h->s + g.s_off) != CUFFT_SUCCESS) {
       set_error("batch cuFFT C2R failed");
       return PF5D_ERR_CUFFT;
     }
+  }
+  for (int a = 0; a < na; ++a) {
+    PF5D_CUDA(cudaEventRecord(h->join[a], h->aux[a]));
+    PF5D_CUDA(cudaStreamWaitEvent(s, h->join[a], 0));
   }
   batch_variants()[h->variant].launch(h->rate_grid, s, h->d_solves, (int)h->solves.size(),
                                       h->total_tiles);
@@ -625,6 +646,32 @@ pf5d_status pf5d_batch_create(const pf5d_batch_solve *solves, int32_t nsolves,
       set_error("device allocation failed");
       return fail(PF5D_ERR_CUDA);
     }
+  }
+  // --- FFT branches: groups largest first over up to kFftBranches streams ----
+  for (int j = 0; j < (int)h->groups.size(); ++j) h->order.push_back(j);
+  std::stable_sort(h->order.begin(), h->order.end(), [&](int a, int b) {
+    const auto &ga = h->groups[a], &gb = h->groups[b];
+    return (int64_t)ga.ny * ga.nx * ga.count > (int64_t)gb.ny * gb.nx * gb.count;
+  });
+  const int nbranch = std::min<int>((int)h->groups.size(), kFftBranches);
+  if (nbranch > 0 &&
+      cudaEventCreateWithFlags(&h->fork, cudaEventDisableTiming) != cudaSuccess) {
+    set_error("event creation failed");
+    return fail(PF5D_ERR_CUDA);
+  }
+  for (int a = 0; a < nbranch; ++a) {
+    cudaStream_t as = nullptr;
+    cudaEvent_t ev = nullptr;
+    if (cudaStreamCreateWithFlags(&as, cudaStreamNonBlocking) != cudaSuccess) {
+      set_error("stream creation failed");
+      return fail(PF5D_ERR_CUDA);
+    }
+    h->aux.push_back(as);
+    if (cudaEventCreateWithFlags(&ev, cudaEventDisableTiming) != cudaSuccess) {
+      set_error("event creation failed");
+      return fail(PF5D_ERR_CUDA);
+    }
+    h->join.push_back(ev);
   }
   // --- per-solve descriptors -------------------------------------------------
   int64_t chunk = 0;
@@ -843,6 +890,9 @@ pf5d_status pf5d_batch_destroy(pf5d_batch *h) {
   cudaFree(h->st);
   cudaFree(h->d_solves);
   if (h->cap) cudaStreamDestroy(h->cap);
+  for (auto as : h->aux) cudaStreamDestroy(as);
+  for (auto ev : h->join) cudaEventDestroy(ev);
+  if (h->fork) cudaEventDestroy(h->fork);
   delete h;
   return PF5D_OK;
 }

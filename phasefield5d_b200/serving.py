@@ -74,9 +74,12 @@ class Scheduler:
     """Admission, step blocks and retirement, independent of the device.
 
     ``backend`` provides: ``sync(active)`` (make the device set match the
-    active requests), ``advance(blocks)`` (steps per request id),
-    ``states()`` (request id -> state dict), ``collect(req)`` (host field),
-    ``free_bytes()``.
+    active requests), ``collect(req)`` (host field), ``free_bytes()``, and
+    either the asynchronous pair ``launch(blocks)`` / ``poll(timeout)`` with
+    ``busy()`` -- each device unit (the shared batch, each own stepper)
+    takes its next block as soon as its last one is done, and ``poll``
+    returns the states of the units that finished -- or the synchronous pair
+    ``advance(blocks)`` / ``states()``, where every block waits for all.
     """
 
     def __init__(self, backend, max_slots=64, step_block=50, reserve_bytes=1 << 30,
@@ -158,11 +161,22 @@ class Scheduler:
             if wait > 0:
                 time.sleep(min(wait, 0.01))
             return True
-        blocks = self.block_sizes()
-        self.backend.advance(blocks)
-        states = self.backend.states()
+        if hasattr(self.backend, "launch"):
+            busy = self.backend.busy()
+            blocks = {rid: n for rid, n in self.block_sizes().items()
+                      if n > 0 and rid not in busy}
+            self.backend.launch(blocks)
+            wait = 0.005
+            if self.queue:
+                wait = min(wait, max(self.queue[0].arrival - self.now(), 0.0))
+            states = self.backend.poll(wait)
+        else:
+            self.backend.advance(self.block_sizes())
+            states = self.backend.states()
         retired = False
         for r in list(self.active):
+            if r.rid not in states:
+                continue
             st = states[r.rid]
             self.points_steps += r.n_points * (st["step"] - r.steps_done)
             r.steps_done = st["step"]
@@ -224,6 +238,9 @@ class GpuBackend:
         self.reqs: dict[int, Request] = {}
         self.batch_stream = torch.cuda.Stream()
         self.variants: dict[tuple, int] = {}      # shape -> autotuned kernel variant
+        self.tables: dict[tuple, object] = {}     # resident FP32 tables of the batch
+        self.pending: dict[object, object] = {}   # unit ("batch" or rid) -> event of its block
+        self.fresh = False                        # batch rebuilt: report its states
 
     def shares_batch(self, req):
         """True when the request advances in the shared 1D/2D batch."""
@@ -239,8 +256,10 @@ class GpuBackend:
         self.reqs = {r.rid: r for r in active}
         for rid in list(self.steppers):
             if rid not in ids:
+                self.streams[rid].synchronize()
                 self.steppers.pop(rid).close()
                 self.streams.pop(rid)
+                self.pending.pop(rid, None)
         for r in active:
             if not self.shares_batch(r) and r.rid not in self.steppers:
                 s = torch.cuda.Stream()
@@ -266,12 +285,15 @@ class GpuBackend:
             self.batch_stream.synchronize()
             self.batch.close()
             self.batch = None
+            self.pending.pop("batch", None)
         self.batch_ids = want
         if want:
             with torch.cuda.stream(self.batch_stream):
                 self.batch = self.BatchStepper([self.reqs[i].problem for i in want],
                                                stream=self.batch_stream, autotune=False,
-                                               resume=[resume.get(i) for i in want])
+                                               resume=[resume.get(i) for i in want],
+                                               table_cache=self.tables)
+            self.fresh = True
 
     def advance(self, blocks):
         if self.batch is not None and self.batch_ids:
@@ -283,6 +305,56 @@ class GpuBackend:
                 st.advance(blocks[rid])
         self.torch.cuda.synchronize()
 
+    # -- asynchronous protocol: every unit runs its own blocks -------------
+    def busy(self):
+        """Request ids whose unit has a block not yet reported by poll."""
+        out = set()
+        for unit in self.pending:
+            if unit == "batch":
+                out.update(self.batch_ids)
+            else:
+                out.add(unit)
+        return out
+
+    def launch(self, blocks):
+        torch = self.torch
+        if self.batch is not None and self.batch_ids and "batch" not in self.pending:
+            n = blocks.get(self.batch_ids[0], 0)
+            if n > 0:
+                self.batch.advance(n)
+                ev = torch.cuda.Event()
+                ev.record(self.batch_stream)
+                self.pending["batch"] = ev
+        for rid, st in self.steppers.items():
+            n = blocks.get(rid, 0)
+            if n > 0 and rid not in self.pending:
+                st.advance(n)
+                ev = torch.cuda.Event()
+                ev.record(self.streams[rid])
+                self.pending[rid] = ev
+
+    def poll(self, timeout):
+        """States of the units whose block finished (waits up to `timeout`
+        seconds for the first one)."""
+        deadline = time.perf_counter() + timeout
+        while True:
+            out = {}
+            if self.fresh and self.batch is not None and "batch" not in self.pending:
+                out.update(zip(self.batch_ids, self.batch.states()))
+            self.fresh = False
+            for unit, ev in list(self.pending.items()):
+                if not ev.query():
+                    continue
+                del self.pending[unit]
+                if unit == "batch":
+                    out.update(zip(self.batch_ids, self.batch.states()))
+                else:
+                    out[unit] = self.steppers[unit].state()
+            if out or time.perf_counter() >= deadline:
+                return out
+            time.sleep(0.0002)
+
+    # -- synchronous protocol ----------------------------------------------
     def states(self):
         out = {}
         if self.batch is not None:

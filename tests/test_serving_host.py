@@ -135,3 +135,69 @@ def test_poisson_arrivals_rate():
     t = poisson_arrivals(20.0, 4000, seed=1)
     assert np.all(np.diff(t) > 0)
     assert t[-1] / 4000 == pytest.approx(1 / 20.0, rel=0.1)
+
+
+class AsyncFakeBackend(FakeBackend):
+    """Asynchronous protocol: the shared batch (dim < 3) and each 3D request
+    are units; a unit's block takes `cost` polls per grid point-step."""
+
+    def __init__(self, free, cost=1e-4):
+        super().__init__(free)
+        self.cost = cost
+        self.inflight = {}      # unit -> [polls left, {rid: steps}]
+
+    def shares_batch(self, r):
+        return r.dim < 3
+
+    def _unit(self, rid):
+        r = next(r for r in self.active if r.rid == rid)
+        return "batch" if r.dim < 3 else rid
+
+    def busy(self):
+        out = set()
+        for unit in self.inflight:
+            out.update(r.rid for r in self.active if self._unit(r.rid) == unit)
+        return out
+
+    def launch(self, blocks):
+        self.blocks.append(dict(blocks))
+        for rid, n in blocks.items():
+            unit = self._unit(rid)
+            work = self.inflight.setdefault(unit, [0, {}])
+            r = next(r for r in self.active if r.rid == rid)
+            work[0] += max(1, int(self.cost * n * r.n_points))
+            work[1][rid] = n
+
+    def poll(self, timeout):
+        out = {}
+        for unit in list(self.inflight):
+            work = self.inflight[unit]
+            work[0] -= 1
+            if work[0] <= 0:
+                del self.inflight[unit]
+                for rid, n in work[1].items():
+                    self.steps[rid] += n
+                states = self.states()
+                out.update({rid: states[rid] for rid in work[1] if rid in states})
+        return out
+
+
+def test_async_units_progress_independently():
+    """A small request admitted after a large 3D one finishes first: units
+    take their next block as soon as their own last block is done."""
+    be = AsyncFakeBackend(free=1 << 40)
+    sch = Scheduler(be, step_block=50, reserve_bytes=0, clock=FakeClock())
+    big = make(0, (64, 64, 64), 400)
+    small = make(1, (1024,), 400, arrival=0.0)
+    mid = make(2, (64, 64), 300, arrival=0.0)
+    for r in (big, small, mid):
+        sch.submit(r)
+    st = sch.run()
+    assert st["requests_done"] == 3
+    for r in (big, small, mid):
+        assert be.steps[r.rid] == r.n_steps
+    order = [r.rid for r in sorted(sch.finished, key=lambda r: r.done)]
+    assert order.index(0) == 2                      # the 3D request finishes last
+    for b in be.blocks:                             # batch members move in lockstep
+        shared = {b[k] for k in (1, 2) if k in b}
+        assert len(shared) <= 1
