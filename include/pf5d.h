@@ -230,6 +230,9 @@ pf5d_status pf5d_stepper_autotune(pf5d_stepper *h, int32_t *variant, float *best
                                   void *stream);
 /* Select a rate-kernel variant explicitly (index from a previous autotune). */
 pf5d_status pf5d_stepper_set_variant(pf5d_stepper *h, int32_t variant);
+/* Number of rate-kernel variants of this stepper's form (valid indices for
+ * pf5d_stepper_set_variant are 0 .. count-1); 0 for a null stepper. */
+int32_t pf5d_stepper_variant_count(const pf5d_stepper *h);
 /* Re-derive internal state after the caller modified X (e.g. a restart). */
 pf5d_status pf5d_stepper_reset(pf5d_stepper *h, double dt, double time, void *stream);
 pf5d_status pf5d_stepper_destroy(pf5d_stepper *h);

@@ -285,4 +285,70 @@ __device__ __forceinline__ double block_max(double v, double *red) {
   return v;
 }
 
+// Locality key of the table cell of a composition, for ordering points by
+// cell: a hash of the four cell indices floor(u_a), u = x / resolution,
+// estimated in FP32 (only the order of work depends on it, never a value).
+// The 16 cells of any 2x2x2x2 block of cells get distinct keys.
+__device__ __forceinline__ int cell_hash_u(const float u[S]) {
+  const unsigned w[S] = {41u, 13u, 5u, 1u};
+  unsigned h = 0;
+#pragma unroll
+  for (int a = 0; a < S; ++a) h += (unsigned)(int)floorf(u[a]) * w[a];
+  return (int)(h & 255u);
+}
+
+__device__ __forceinline__ int cell_hash(const double x[S], float inv_step) {
+  float u[S];
+#pragma unroll
+  for (int a = 0; a < S; ++a) u[a] = (float)x[a] * inv_step;
+  return cell_hash_u(u);
+}
+
+// Block-wide exclusive prefix sum of bins[0..NB) by all NT threads of the
+// block (consecutive bins per thread); wsum holds NT/32 + 1 ints.  Returns
+// the total and ends with a barrier.
+template <int NB, int NT>
+__device__ __forceinline__ int block_exclusive_scan(int *bins, int *wsum, int tid) {
+  constexpr int BPT = (NB + NT - 1) / NT;
+  const int lane = tid & 31, w = tid >> 5;
+  int loc[BPT];
+  int v = 0;
+#pragma unroll
+  for (int j = 0; j < BPT; ++j) {
+    const int b = tid * BPT + j;
+    loc[j] = b < NB ? bins[b] : 0;
+    v += loc[j];
+  }
+  int inc = v;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const int t = __shfl_up_sync(0xffffffffu, inc, o);
+    if (lane >= o) inc += t;
+  }
+  if (lane == 31) wsum[w] = inc;
+  __syncthreads();
+  if (w == 0) {
+    const int t = lane < NT / 32 ? wsum[lane] : 0;
+    int sc = t;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const int u = __shfl_up_sync(0xffffffffu, sc, o);
+      if (lane >= o) sc += u;
+    }
+    if (lane < NT / 32) wsum[lane] = sc - t;
+    if (lane == NT / 32 - 1) wsum[NT / 32] = sc;
+  }
+  __syncthreads();
+  int base = inc - v + wsum[w];
+#pragma unroll
+  for (int j = 0; j < BPT; ++j) {
+    const int b = tid * BPT + j;
+    if (b < NB) bins[b] = base;
+    base += loc[j];
+  }
+  const int total = wsum[NT / 32];
+  __syncthreads();
+  return total;
+}
+
 }  // namespace pf5d

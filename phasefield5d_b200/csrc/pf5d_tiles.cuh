@@ -10,11 +10,14 @@
 
 namespace pf5d {
 
-template <int TX, int TY>
+// NTH: threads of the block (default one per tile point); a block may have
+// more threads than tile points so that the halo positions need no second
+// pass.
+template <int TX, int TY, int NTH = TX * TY>
 struct PlaneGeom {
   static constexpr int HX = TX + 4, HY = TY + 4, PX = HX * HY;
   static constexpr int MX = TX + 2, MY = TY + 2, PM = MX * MY;
-  static constexpr int NT = TX * TY;
+  static constexpr int NT = NTH;
   static constexpr int NFX = TY * (TX + 1), NFY = (TY + 1) * TX;
 };
 

@@ -703,6 +703,8 @@ pf5d_status s32_mass(Stepper32 *h, double *mean_out, void *stream) {
   return PF5D_OK;
 }
 
+int32_t s32_variant_count() { return (int32_t)variants32().size(); }
+
 pf5d_status s32_set_variant(Stepper32 *h, int32_t variant) {
   pf5d_status st = configure32(h, variant);
   if (st == PF5D_OK) drop_graphs(h);

@@ -59,6 +59,8 @@ struct RateParams {
   double ctld, t_cfl, lower, upper, factor;
   int adaptive;
   StepState *st;
+  double *mm;                  // split rate: mu_1..4, M_Fe, M_1..4 per point, SoA [NP][npts]
+  int64_t npts;
 };
 
 // ------------------------------------------------------------------------
@@ -154,15 +156,31 @@ __device__ __forceinline__ void interp_win64(const Table &T, const double x[S], 
     out[p] = r.node < 0 ? __longlong_as_double(0x7ff8000000000000LL) : __ldg(row + p);
 }
 
+// Shared-memory scratch of a per-tile cell sort: hist[256], wsum[NT/32+1],
+// order/rank/key per mu/M position.
+struct SortScratch {
+  int *hist;
+  int *wsum;
+  unsigned short *order;
+  unsigned short *rank;
+  unsigned char *key;
+};
+
+constexpr unsigned short kNoRank = 0xFFFFu;
+
 // mu/M of one plane (tile + 1-cell halo, or tile only) into dst, making the
 // table window in `win` current first (win_lo: origin + valid flag).  Xm/Xp: axis-0 neighbour planes (3D) or
-// nullptr (2D).  Laplacian neighbour order as operators.py:49-76.
-template <int TX, int TY, int DIM, bool VEC, bool WIN>
+// nullptr (2D).  Laplacian neighbour order as operators.py:49-76.  SORT:
+// the positions are first put in table-cell order (cell_hash counting
+// sort) so the lanes of a warp gather the same table nodes; which thread
+// evaluates a position changes, the values do not.
+template <int TX, int TY, int DIM, bool VEC, bool WIN, int NTH = TX * TY, bool SORT = false>
 __device__ __forceinline__ void mu_plane64(const RateParams &P, const double *Xm, const double *Xc,
                                            const double *Xp, double *dst, int64_t zoff,
                                            const int *wx, const int *wy, bool interior_only,
-                                           double2 *win, int *win_lo, unsigned *flags, int tid) {
-  using G = PlaneGeom<TX, TY>;
+                                           double2 *win, int *win_lo, unsigned *flags, int tid,
+                                           SortScratch ss = {}) {
+  using G = PlaneGeom<TX, TY, NTH>;
   auto skip = [&](int mx, int my) {
     const bool ex = (mx == 0 || mx == G::MX - 1), ey = (my == 0 || my == G::MY - 1);
     return interior_only ? (ex || ey) : (ex && ey);
@@ -183,9 +201,34 @@ __device__ __forceinline__ void mu_plane64(const RateParams &P, const double *Xm
                                                        P.T.n, o, win, win_lo, tid);
     }
   }
-  for (int pos = tid; pos < G::PM; pos += G::NT) {
+  int nwork = G::PM;
+  if constexpr (SORT) {
+    for (int i = tid; i < 256; i += NTH) ss.hist[i] = 0;
+    __syncthreads();
+    for (int pos = tid; pos < G::PM; pos += NTH) {
+      const int my = pos / G::MX, mx = pos - my * G::MX;
+      if (skip(mx, my)) {
+        ss.rank[pos] = kNoRank;
+        continue;
+      }
+      const int px = (my + 1) * G::HX + (mx + 1);
+      double xk[S];
+#pragma unroll
+      for (int c = 0; c < S; ++c) xk[c] = Xc[c * G::PX + px];
+      const int k = cell_hash(xk, (float)P.T.inv_step);
+      ss.key[pos] = (unsigned char)k;
+      ss.rank[pos] = (unsigned short)atomicAdd(&ss.hist[k], 1);
+    }
+    __syncthreads();
+    nwork = block_exclusive_scan<256, NTH>(ss.hist, ss.wsum, tid);
+    for (int pos = tid; pos < G::PM; pos += NTH)
+      if (ss.rank[pos] != kNoRank) ss.order[ss.hist[ss.key[pos]] + ss.rank[pos]] = (unsigned short)pos;
+    __syncthreads();
+  }
+  for (int w = tid; w < nwork; w += NTH) {
+    const int pos = SORT ? (int)ss.order[w] : w;
     const int my = pos / G::MX, mx = pos - my * G::MX;
-    if (skip(mx, my)) continue;
+    if (!SORT && skip(mx, my)) continue;
     const int px = (my + 1) * G::HX + (mx + 1);
     double x[S], lap[S];
 #pragma unroll
@@ -211,6 +254,132 @@ __device__ __forceinline__ void mu_plane64(const RateParams &P, const double *Xm
 #pragma unroll
     for (int c = 0; c < NM; ++c) dst[(S + c) * G::PM + pos] = v[S + c];
   }
+}
+
+// mu/M of one plane (tile + 1-cell halo, or tile only) read from the split
+// buffer P.mm (written by k_chem64) into dst, in mu_plane64's layout.
+template <int TX, int TY, int NTH = TX * TY>
+__device__ __forceinline__ void load_mu_plane(const RateParams &P, int64_t zoff, const int *wx,
+                                              const int *wy, bool interior_only, double *dst,
+                                              int tid) {
+  using G = PlaneGeom<TX, TY, NTH>;
+  for (int pos = tid; pos < G::PM; pos += G::NT) {
+    const int my = pos / G::MX, mx = pos - my * G::MX;
+    const bool ex = (mx == 0 || mx == G::MX - 1), ey = (my == 0 || my == G::MY - 1);
+    if (interior_only ? (ex || ey) : (ex && ey)) continue;
+    const double *src = P.mm + zoff + (int64_t)wy[my + 1] * P.nx + wx[mx + 1];
+#pragma unroll
+    for (int c = 0; c < NP; ++c) dst[c * G::PM + pos] = __ldg(src + c * P.npts);
+  }
+}
+
+// Split rate evaluation, first kernel: chemical potential and mobility at
+// every point of a 2D/3D field into P.mm, one point per thread, a 32 x 8
+// tile of a plane per block.  Same arithmetic as mu_plane64: Laplacian
+// neighbour order (operators.py:49-76) +axis0, -axis0, +axis1, -axis1
+// (, +axis2, -axis2), then mu = v - lap*kappa (+ s' * l).
+//
+// Before interpolating, the block orders its points by table cell
+// (counting sort on cell_hash), so the lanes of a warp gather the same
+// table nodes: a warp-wide corner load then touches one or two cache lines
+// instead of one per lane.  Every point is evaluated exactly once (no halo)
+// and the order only changes which thread evaluates a point.
+template <int DIM, bool VEC, int MINB>
+__global__ void __launch_bounds__(256, MINB) k_chem64(RateParams P) {
+  constexpr int NT = 256;
+  __shared__ double io[NP][NT];          // inputs (x, lap, s'), then outputs (mu, M)
+  __shared__ int hist[NT];
+  __shared__ int wsum[NT / 32 + 1];
+  __shared__ unsigned short order[NT];
+  if (P.st->halt) return;
+  const int tid = threadIdx.y * 32 + threadIdx.x;
+  const int x = blockIdx.x * 32 + threadIdx.x;
+  const int y = blockIdx.y * 8 + threadIdx.y;
+  const int z = blockIdx.z;
+  const bool valid = x < P.nx && y < P.ny;
+  const int64_t plane = (int64_t)P.ny * P.nx;
+  const int64_t zo = (int64_t)z * plane;
+  const int64_t g = zo + (int64_t)y * P.nx + x;
+  hist[tid] = 0;
+  int key = 0, rank = 0;
+  __syncthreads();
+  if (valid) {
+    auto ld = [&](int64_t gi, double v[S]) {
+      const double2 a = __ldg(reinterpret_cast<const double2 *>(P.X + 4 * gi));
+      const double2 b = __ldg(reinterpret_cast<const double2 *>(P.X + 4 * gi) + 1);
+      v[0] = a.x; v[1] = a.y; v[2] = b.x; v[3] = b.y;
+    };
+    const int xp = x + 1 == P.nx ? 0 : x + 1, xm = x == 0 ? P.nx - 1 : x - 1;
+    const int yp = y + 1 == P.ny ? 0 : y + 1, ym = y == 0 ? P.ny - 1 : y - 1;
+    double xc[S], lap[S], n0[S], n1[S];
+    ld(g, xc);
+    if (DIM == 3) {
+      const int zp = z + 1 == P.nz ? 0 : z + 1, zm = z == 0 ? P.nz - 1 : z - 1;
+      ld((int64_t)zp * plane + (int64_t)y * P.nx + x, n0);
+      ld((int64_t)zm * plane + (int64_t)y * P.nx + x, n1);
+#pragma unroll
+      for (int c = 0; c < S; ++c) lap[c] = n0[c] + n1[c];
+      ld(zo + (int64_t)yp * P.nx + x, n0);
+      ld(zo + (int64_t)ym * P.nx + x, n1);
+#pragma unroll
+      for (int c = 0; c < S; ++c) lap[c] = (lap[c] + n0[c]) + n1[c];
+    } else {
+      ld(zo + (int64_t)yp * P.nx + x, n0);
+      ld(zo + (int64_t)ym * P.nx + x, n1);
+#pragma unroll
+      for (int c = 0; c < S; ++c) lap[c] = n0[c] + n1[c];
+    }
+    ld(zo + (int64_t)y * P.nx + xp, n0);
+    ld(zo + (int64_t)y * P.nx + xm, n1);
+#pragma unroll
+    for (int c = 0; c < S; ++c) {
+      lap[c] = (((lap[c] + n0[c]) + n1[c]) - (DIM == 3 ? 6.0 : 4.0) * xc[c]) * P.inv_dx2;
+      io[c][tid] = xc[c];
+      io[S + c][tid] = lap[c];
+    }
+    io[2 * S][tid] = P.sp ? __ldg(P.sp + g) : 0.0;
+    key = cell_hash(xc, (float)P.T.inv_step);
+    rank = atomicAdd(&hist[key], 1);
+  }
+  __syncthreads();
+  const int count = block_exclusive_scan<NT, NT>(hist, wsum, tid);
+  if (valid) order[hist[key] + rank] = (unsigned short)tid;
+  __syncthreads();
+  unsigned flags = 0;
+  double v[NP], mu[S];
+  int q = -1;
+  if (tid < count) {
+    q = order[tid];
+    double xq[S], lq[S];
+#pragma unroll
+    for (int c = 0; c < S; ++c) {
+      xq[c] = io[c][q];
+      lq[c] = io[S + c][q];
+    }
+    const double spv = io[2 * S][q];
+    const int o[S] = {0, 0, 0, 0};
+    interp_win64<VEC>(P.T, xq, nullptr, o, v, &flags);
+#pragma unroll
+    for (int c = 0; c < S; ++c) {
+      const double lk = lq[c] * P.kappa.v[c];
+      double m = v[c] - lk;
+      if (P.sp) m = m + spv * P.lvec.v[c];
+      mu[c] = m;
+    }
+  }
+  __syncthreads();                       // all inputs read: io now takes the outputs
+  if (q >= 0) {
+#pragma unroll
+    for (int c = 0; c < S; ++c) io[c][q] = mu[c];
+#pragma unroll
+    for (int c = 0; c < NM; ++c) io[S + c][q] = v[S + c];
+  }
+  __syncthreads();
+  if (valid) {
+#pragma unroll
+    for (int c = 0; c < NP; ++c) P.mm[c * P.npts + g] = io[c][tid];
+  }
+  if (flags) atomicOr(&P.st->flags, flags);
 }
 
 // Fold this thread's max |dX/dt| into the block, then into the device
@@ -269,10 +438,10 @@ __device__ __forceinline__ void face_between(const double *XL, const double *ML,
 
 // All x- and y-faces of one plane tile into Fx / Fy (flat loop: every
 // thread takes faces in turn).
-template <int TX, int TY>
+template <int TX, int TY, int NTH = TX * TY>
 __device__ __forceinline__ void plane_faces(const double *Xp, const double *Mp, double *Fx,
                                             double *Fy, double inv_dx, int tid) {
-  using G = PlaneGeom<TX, TY>;
+  using G = PlaneGeom<TX, TY, NTH>;
   for (int f = tid; f < G::NFX + G::NFY; f += G::NT) {
     double J[S];
     if (f < G::NFX) {
@@ -293,11 +462,11 @@ __device__ __forceinline__ void plane_faces(const double *Xp, const double *Mp, 
 }
 
 // Stage one X plane (tile + 2-cell halo) into SoA shared memory.
-template <int TX, int TY>
+template <int TX, int TY, int NTH = TX * TY>
 __device__ __forceinline__ void load_plane(const double *__restrict__ X, int64_t plane_off,
                                            const int *wx, const int *wy, int nx, double *dst,
                                            int tid) {
-  using G = PlaneGeom<TX, TY>;
+  using G = PlaneGeom<TX, TY, NTH>;
   for (int pos = tid; pos < G::PX; pos += G::NT) {
     const int hy = pos / G::HX, hx = pos - hy * G::HX;
     const int64_t g = plane_off + (int64_t)wy[hy] * nx + wx[hx];
@@ -316,9 +485,14 @@ __device__ __forceinline__ void load_plane(const double *__restrict__ X, int64_t
 // Axis 0 of the (n0, n1) field is the tile's y, axis 1 its x.  Laplacian
 // (operators.py:49-60) and divergence (fluxes.py:349) keep the reference's
 // axis order: axis-0 terms first.
-template <int TX, int TY, int MINB, bool VEC, bool WIN>
-__global__ void __launch_bounds__(TX * TY, MINB) k_rate_tile2d(RateParams P) {
-  using G = PlaneGeom<TX, TY>;
+// A block is NTH threads in one dimension (at least one per tile point; with
+// NTH >= the mu/M position count every position takes one pass).  SORT:
+// mu/M positions evaluated in table-cell order.
+template <int TX, int TY, int MINB, bool VEC, bool WIN, bool SPLIT = false, int NTH = TX * TY,
+          bool SORT = false>
+__global__ void __launch_bounds__(NTH, MINB) k_rate_tile2d(RateParams P) {
+  using G = PlaneGeom<TX, TY, NTH>;
+  static_assert(NTH >= TX * TY && NTH % 32 == 0, "one thread per tile point at least");
   if (P.st->halt) return;
   extern __shared__ double sm[];
   double *Xs = sm;                       // [S][PX]
@@ -329,7 +503,15 @@ __global__ void __launch_bounds__(TX * TY, MINB) k_rate_tile2d(RateParams P) {
   int *wx = reinterpret_cast<int *>(red + G::NT / 32);   // [HX]
   int *wy = wx + G::HX;                                  // [HY]
   int *win_lo = wy + G::HY;                              // [S+1] window origin, valid
-  const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * TX + tx;
+  SortScratch ss{};
+  if constexpr (SORT) {
+    ss.hist = win_lo + S + 1;                            // [256]
+    ss.wsum = ss.hist + 256;                             // [NT/32 + 1]
+    ss.order = reinterpret_cast<unsigned short *>(ss.wsum + G::NT / 32 + 1);   // [PM]
+    ss.rank = ss.order + G::PM;                          // [PM]
+    ss.key = reinterpret_cast<unsigned char *>(ss.rank + G::PM);               // [PM]
+  }
+  const int tid = threadIdx.x, tx = tid % TX, ty = tid / TX;
   const int x0 = blockIdx.x * TX, y0 = blockIdx.y * TY;
   unsigned flags = 0;
   if (tid == 0) win_lo[S] = 0;
@@ -339,15 +521,19 @@ __global__ void __launch_bounds__(TX * TY, MINB) k_rate_tile2d(RateParams P) {
     else wy[i - G::HX] = wrap_any(y0 + (i - G::HX) - 2, P.ny);
   }
   __syncthreads();
-  load_plane<TX, TY>(P.X, 0, wx, wy, P.nx, Xs, tid);
+  load_plane<TX, TY, NTH>(P.X, 0, wx, wy, P.nx, Xs, tid);
   __syncthreads();
-  mu_plane64<TX, TY, 2, VEC, WIN>(P, nullptr, Xs, nullptr, Ms, 0, wx, wy, false,
-                             reinterpret_cast<double2 *>(Fx), win_lo, &flags, tid);
+  if constexpr (SPLIT)
+    load_mu_plane<TX, TY, NTH>(P, 0, wx, wy, false, Ms, tid);
+  else
+    mu_plane64<TX, TY, 2, VEC, WIN, NTH, SORT>(P, nullptr, Xs, nullptr, Ms, 0, wx, wy, false,
+                                               reinterpret_cast<double2 *>(Fx), win_lo, &flags,
+                                               tid, ss);
   __syncthreads();
-  plane_faces<TX, TY>(Xs, Ms, Fx, Fy, P.inv_dx, tid);
+  plane_faces<TX, TY, NTH>(Xs, Ms, Fx, Fy, P.inv_dx, tid);
   __syncthreads();
   double vmax = 0.0;
-  if (x0 + tx < P.nx && y0 + ty < P.ny) {
+  if (tid < TX * TY && x0 + tx < P.nx && y0 + ty < P.ny) {
     double out[S];
 #pragma unroll
     for (int c = 0; c < S; ++c) {
@@ -367,13 +553,14 @@ __global__ void __launch_bounds__(TX * TY, MINB) k_rate_tile2d(RateParams P) {
   finish_rate(P, vmax, red);
 }
 
-template <int TX, int TY>
+template <int TX, int TY, int NTH = TX * TY, bool SORT = false>
 constexpr size_t tile2d_smem() {
-  using G = PlaneGeom<TX, TY>;
+  using G = PlaneGeom<TX, TY, NTH>;
   static_assert(S * (G::NFX + G::NFY) * sizeof(double) >= kWinNodes64 * kNodeV64 * sizeof(double2),
                 "face buffers must hold the table window");
+  const size_t sort = SORT ? (256 + G::NT / 32 + 1) * sizeof(int) + G::PM * (2 * 2 + 1) : 0;
   return (S * G::PX + NP * G::PM + S * G::NFX + S * G::NFY + G::NT / 32) * sizeof(double) +
-         (G::HX + G::HY + S + 1) * sizeof(int);
+         (G::HX + G::HY + S + 1) * sizeof(int) + sort;
 }
 
 // ------------------------------------------------------------------------
@@ -417,7 +604,7 @@ struct March64Geom {
   static constexpr int NFMAX = G::NFX > G::NFY ? G::NFX : G::NFY;
 };
 
-template <int TX, int TY, int MINB, bool VEC, bool WIN>
+template <int TX, int TY, int MINB, bool VEC, bool WIN, bool SPLIT = false>
 __global__ void __launch_bounds__(TX * TY, MINB) k_rate_march3d(RateParams P, int zc) {
   using G = PlaneGeom<TX, TY>;
   if (P.st->halt) return;
@@ -448,24 +635,35 @@ __global__ void __launch_bounds__(TX * TY, MINB) k_rate_march3d(RateParams P, in
     load_plane<TX, TY>(P.X, (int64_t)wrap_any(z, P.nz) * plane, wx, wy, P.nx, xplane(z), tid);
   };
   auto compute_mu = [&](int z, bool interior_only) {
-    mu_plane64<TX, TY, 3, VEC, WIN>(P, xplane(z - 1), xplane(z), xplane(z + 1), mplane(z),
-                               (int64_t)wrap_any(z, P.nz) * plane, wx, wy, interior_only, win,
-                               win_lo, &flags, tid);
+    if constexpr (SPLIT)
+      load_mu_plane<TX, TY>(P, (int64_t)wrap_any(z, P.nz) * plane, wx, wy, interior_only,
+                            mplane(z), tid);
+    else
+      mu_plane64<TX, TY, 3, VEC, WIN>(P, xplane(z - 1), xplane(z), xplane(z + 1), mplane(z),
+                                      (int64_t)wrap_any(z, P.nz) * plane, wx, wy, interior_only,
+                                      win, win_lo, &flags, tid);
   };
   const int pX = (ty + 2) * G::HX + (tx + 2);
   const int pM = (ty + 1) * G::MX + (tx + 1);
   const bool in_tile = (x0 + tx < P.nx) && (y0 + ty < P.ny);
 
   __syncthreads();
-  load_x(zb - 2);
-  load_x(zb - 1);
-  load_x(zb);
-  __syncthreads();
-  compute_mu(zb - 1, true);
-  __syncthreads();
-  load_x(zb + 1);
-  __syncthreads();
-  compute_mu(zb, false);
+  if constexpr (SPLIT) {          // faces need X and mu/M of planes z and z+1 only
+    load_x(zb - 1);
+    load_x(zb);
+    compute_mu(zb - 1, true);
+    compute_mu(zb, false);
+  } else {
+    load_x(zb - 2);
+    load_x(zb - 1);
+    load_x(zb);
+    __syncthreads();
+    compute_mu(zb - 1, true);
+    __syncthreads();
+    load_x(zb + 1);
+    __syncthreads();
+    compute_mu(zb, false);
+  }
   __syncthreads();
   double Jm[S];
   face_between<G::PX, G::PM>(xplane(zb - 1), mplane(zb - 1), pX, pM, xplane(zb), mplane(zb), pX,
@@ -473,9 +671,14 @@ __global__ void __launch_bounds__(TX * TY, MINB) k_rate_march3d(RateParams P, in
   double vmax = 0.0;
   for (int z = zb; z < ze; ++z) {
     __syncthreads();
-    load_x(z + 2);
-    __syncthreads();
-    compute_mu(z + 1, false);
+    if constexpr (SPLIT) {
+      load_x(z + 1);
+      compute_mu(z + 1, false);
+    } else {
+      load_x(z + 2);
+      __syncthreads();
+      compute_mu(z + 1, false);
+    }
     __syncthreads();
     double a[S];
     face_between<G::PX, G::PM>(xplane(z), mplane(z), pX, pM, xplane(z + 1), mplane(z + 1), pX,
@@ -744,6 +947,7 @@ struct pf5d_stepper {
   int variant = 0;
   Stepper32 *s32 = nullptr;      // FP32C form (all calls delegate)
   double *mass_ws = nullptr;     // FP64 mean reduction workspace
+  double *mm = nullptr;          // split-rate mu/M buffer (2D/3D)
 };
 
 namespace {
@@ -752,10 +956,14 @@ constexpr int kTX1 = 128;            // 1D tile
 constexpr int kGraphSteps = 50;      // steps per captured graph
 
 // Rate-kernel variants the autotuner chooses from: plane tile (TX x TY
-// threads) and the minimum resident blocks per SM (which caps registers).
+// threads) and the minimum resident blocks per SM (which caps registers);
+// fused (one kernel) or split (k_chem64 over all points, then the tile
+// kernel reading mu/M back).  All variants compute every value the same way.
 struct RateVariant {
   int tx, ty, minb;
+  int nth;          // threads of a 2D block (1D block; >= tx * ty)
   bool win;
+  bool split;
   size_t smem2d, smem3d;
   void (*set_attrs)(bool vec);
   void (*launch2d)(bool vec, dim3 g, dim3 b, size_t sm, cudaStream_t s, const RateParams &P);
@@ -763,29 +971,33 @@ struct RateVariant {
                    int zc);
 };
 
-template <int TX, int TY, int MINB, bool WIN = true>
+// NTH / SORT shape the 2D kernel only; in 3D such a variant runs the
+// marching kernel of the same tile.
+template <int TX, int TY, int MINB, bool WIN = true, int NTH = TX * TY, bool SORT = false>
 RateVariant make_variant() {
   RateVariant v;
   v.tx = TX;
   v.ty = TY;
   v.minb = MINB;
+  v.nth = NTH;
   v.win = WIN;
-  v.smem2d = tile2d_smem<TX, TY>();
+  v.split = false;
+  v.smem2d = tile2d_smem<TX, TY, NTH, SORT>();
   v.smem3d = march3d_smem<TX, TY>();
   v.set_attrs = [](bool vec) {
-    const int s2 = (int)tile2d_smem<TX, TY>(), s3 = (int)march3d_smem<TX, TY>();
+    const int s2 = (int)tile2d_smem<TX, TY, NTH, SORT>(), s3 = (int)march3d_smem<TX, TY>();
     const auto a = cudaFuncAttributeMaxDynamicSharedMemorySize;
     if (vec) {
-      cudaFuncSetAttribute(k_rate_tile2d<TX, TY, MINB, true, WIN>, a, s2);
+      cudaFuncSetAttribute(k_rate_tile2d<TX, TY, MINB, true, WIN, false, NTH, SORT>, a, s2);
       cudaFuncSetAttribute(k_rate_march3d<TX, TY, MINB, true, WIN>, a, s3);
     } else {
-      cudaFuncSetAttribute(k_rate_tile2d<TX, TY, MINB, false, WIN>, a, s2);
+      cudaFuncSetAttribute(k_rate_tile2d<TX, TY, MINB, false, WIN, false, NTH, SORT>, a, s2);
       cudaFuncSetAttribute(k_rate_march3d<TX, TY, MINB, false, WIN>, a, s3);
     }
   };
   v.launch2d = [](bool vec, dim3 g, dim3 b, size_t sm, cudaStream_t s, const RateParams &P) {
-    if (vec) k_rate_tile2d<TX, TY, MINB, true, WIN><<<g, b, sm, s>>>(P);
-    else k_rate_tile2d<TX, TY, MINB, false, WIN><<<g, b, sm, s>>>(P);
+    if (vec) k_rate_tile2d<TX, TY, MINB, true, WIN, false, NTH, SORT><<<g, b, sm, s>>>(P);
+    else k_rate_tile2d<TX, TY, MINB, false, WIN, false, NTH, SORT><<<g, b, sm, s>>>(P);
   };
   v.launch3d = [](bool vec, dim3 g, dim3 b, size_t sm, cudaStream_t s, const RateParams &P,
                   int zc) {
@@ -795,11 +1007,55 @@ RateVariant make_variant() {
   return v;
 }
 
+template <int DIM, int KMINB>
+void launch_chem(bool vec, cudaStream_t s, const RateParams &P) {
+  const dim3 b(32, 8), g((unsigned)((P.nx + 31) / 32), (unsigned)((P.ny + 7) / 8),
+                         (unsigned)P.nz);
+  if (vec) k_chem64<DIM, true, KMINB><<<g, b, 0, s>>>(P);
+  else k_chem64<DIM, false, KMINB><<<g, b, 0, s>>>(P);
+}
+
+template <int TX, int TY, int MINB, int KMINB>
+RateVariant make_split_variant() {
+  RateVariant v;
+  v.tx = TX;
+  v.ty = TY;
+  v.minb = MINB;
+  v.nth = TX * TY;
+  v.win = false;
+  v.split = true;
+  v.smem2d = tile2d_smem<TX, TY>();
+  v.smem3d = march3d_smem<TX, TY>();
+  v.set_attrs = [](bool) {
+    const auto a = cudaFuncAttributeMaxDynamicSharedMemorySize;
+    cudaFuncSetAttribute(k_rate_tile2d<TX, TY, MINB, true, false, true>, a,
+                         (int)tile2d_smem<TX, TY>());
+    cudaFuncSetAttribute(k_rate_march3d<TX, TY, MINB, true, false, true>, a,
+                         (int)march3d_smem<TX, TY>());
+  };
+  v.launch2d = [](bool vec, dim3 g, dim3 b, size_t sm, cudaStream_t s, const RateParams &P) {
+    launch_chem<2, KMINB>(vec, s, P);
+    k_rate_tile2d<TX, TY, MINB, true, false, true><<<g, b, sm, s>>>(P);
+  };
+  v.launch3d = [](bool vec, dim3 g, dim3 b, size_t sm, cudaStream_t s, const RateParams &P,
+                  int zc) {
+    launch_chem<3, KMINB>(vec, s, P);
+    k_rate_march3d<TX, TY, MINB, true, false, true><<<g, b, sm, s>>>(P, zc);
+  };
+  return v;
+}
+
 const std::vector<RateVariant> &rate_variants() {
   static const std::vector<RateVariant> v = {
       make_variant<32, 8, 2>(), make_variant<32, 8, 3>(), make_variant<32, 4, 4>(),
       make_variant<16, 8, 4>(), make_variant<64, 4, 2>(), make_variant<32, 4, 6>(),
-      make_variant<32, 8, 2, false>(), make_variant<32, 8, 3, false>()};
+      make_variant<32, 8, 2, false>(), make_variant<32, 8, 3, false>(),
+      make_split_variant<32, 8, 3, 2>(), make_split_variant<32, 8, 3, 3>(),
+      make_split_variant<32, 4, 4, 2>(), make_split_variant<32, 4, 4, 3>(),
+      make_split_variant<32, 8, 3, 4>(), make_split_variant<32, 4, 4, 4>(),
+      make_variant<32, 8, 2, true, 352, true>(), make_variant<32, 8, 2, false, 352, true>(),
+      make_variant<32, 8, 2, true, 352, false>(), make_variant<32, 4, 4, true, 224, true>(),
+      make_variant<32, 4, 4, false, 224, true>(), make_variant<32, 16, 1, false, 608, true>()};
   return v;
 }
 
@@ -822,6 +1078,7 @@ pf5d_status configure_rate(pf5d_stepper *h, int variant) {
   v.set_attrs(h->vec);
   PF5D_LAUNCHED();
   h->rate_block = dim3(v.tx, v.ty);
+  if (dim == 2) h->rate_block = dim3(v.nth);
   const unsigned gx = (unsigned)((P.nx + v.tx - 1) / v.tx), gy = (unsigned)((P.ny + v.ty - 1) / v.ty);
   if (dim == 2) {
     h->rate_smem = v.smem2d;
@@ -1004,6 +1261,10 @@ pf5d_status pf5d_stepper_create(const pf5d_stepper_desc *desc, double *X, void *
     set_error("device allocation failed");
     return fail(PF5D_ERR_CUDA);
   }
+  if (desc->dim >= 2 && cudaMalloc(&h->mm, (size_t)npts * NP * sizeof(double)) != cudaSuccess) {
+    set_error("device allocation failed");
+    return fail(PF5D_ERR_CUDA);
+  }
   if (desc->elastic) {
     if ((st = fft_create(desc->dim, h->shape, &h->fft)) != PF5D_OK) return fail(st);
     if ((st = upload_bk_scaled(desc->bk, h->fft.nk, npts, &h->bk)) != PF5D_OK) return fail(st);
@@ -1045,6 +1306,8 @@ pf5d_status pf5d_stepper_create(const pf5d_stepper_desc *desc, double *X, void *
   P.factor = desc->max_change_factor;
   P.adaptive = desc->adaptive;
   P.st = h->st;
+  P.mm = h->mm;
+  P.npts = npts;
   UpdateParams &U = h->up;
   U.X = X;
   U.dX = h->dX;
@@ -1171,6 +1434,11 @@ pf5d_status pf5d_stepper_set_variant(pf5d_stepper *h, int32_t variant) {
   return PF5D_OK;
 }
 
+int32_t pf5d_stepper_variant_count(const pf5d_stepper *h) {
+  if (!h) return 0;
+  return h->s32 ? s32_variant_count() : (int32_t)rate_variants().size();
+}
+
 pf5d_status pf5d_stepper_launch_stage(pf5d_stepper *h, int32_t stage, void *stream) {
   PF5D_REQUIRE(h, PF5D_ERR_ARG, "null stepper");
   if (h->s32) return s32_launch_stage(h->s32, stage, stream);
@@ -1201,6 +1469,7 @@ pf5d_status pf5d_stepper_destroy(pf5d_stepper *h) {
   if (!h) return PF5D_OK;
   if (h->s32) s32_destroy(h->s32);
   cudaFree(h->mass_ws);
+  cudaFree(h->mm);
   for (auto &kv : h->graphs) cudaGraphExecDestroy(kv.second);
   fft_destroy(&h->fft);
   cudaFree(h->dX);

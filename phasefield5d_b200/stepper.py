@@ -150,6 +150,11 @@ class Stepper:
                                                 self._s()), "autotune")
         return int(v.value), float(ms.value)
 
+    @property
+    def n_variants(self):
+        """Number of rate-kernel variants the autotuner chooses from."""
+        return int(self.L.pf5d_stepper_variant_count(self.h))
+
     def set_variant(self, variant):
         _lib.check(self.L.pf5d_stepper_set_variant(self.h, int(variant)), "set_variant")
 

@@ -223,7 +223,10 @@ def test_rate_variants_bitwise_identical(torch_cuda):
                             adaptive=True, n_k=2000, fluctuation=2e-2)
         prob = W.build_problem(cfg)
         ref = None
-        for v in range(8):
+        st0 = Stepper.from_problem(prob, autotune=False)
+        n_variants = st0.n_variants
+        st0.close()
+        for v in range(n_variants):
             st = Stepper.from_problem(prob, autotune=False)
             st.set_variant(v)
             st.run(7)
