@@ -284,6 +284,8 @@ pf5d_status pf5d_batch_field(pf5d_batch *h, int32_t i, double *X_out, void *stre
 pf5d_status pf5d_batch_export(pf5d_batch *h, int32_t i, float *hi_out, float *lo_out, void *stream);
 pf5d_status pf5d_batch_autotune(pf5d_batch *h, int32_t *variant, float *best_ms, void *stream);
 pf5d_status pf5d_batch_set_variant(pf5d_batch *h, int32_t variant);
+/* Number of batched rate-kernel variants (valid indices 0 .. count-1). */
+int32_t pf5d_batch_variant_count(void);
 pf5d_status pf5d_batch_destroy(pf5d_batch *h);
 
 #if defined(__GNUC__)

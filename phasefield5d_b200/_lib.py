@@ -104,6 +104,7 @@ _SIGS = {
                                      _vp]),
     "pf5d_stepper_set_variant": (_i32, [_vp, _i32]),
     "pf5d_stepper_variant_count": (_i32, [_vp]),
+    "pf5d_batch_variant_count": (_i32, []),
     "pf5d_stepper_reset": (_i32, [_vp, _f64, _f64, _vp]),
     "pf5d_stepper_destroy": (_i32, [_vp]),
     "pf5d_batch_create": (_i32, [ctypes.POINTER(BatchSolve), _i32, ctypes.POINTER(_vp), _i32,

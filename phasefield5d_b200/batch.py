@@ -159,6 +159,11 @@ class BatchStepper:
                    "autotune")
         return int(v.value), float(ms.value)
 
+    @property
+    def n_variants(self):
+        """Number of batched rate-kernel variants the autotuner chooses from."""
+        return int(self.L.pf5d_batch_variant_count())
+
     def set_variant(self, v):
         _lib.check(self.L.pf5d_batch_set_variant(self.h, int(v)), "set_variant")
 

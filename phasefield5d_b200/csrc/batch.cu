@@ -138,23 +138,23 @@ __device__ __forceinline__ float tile1d32_body(const BSolve &B, const Rate32 &P,
   return vmax;
 }
 
-template <int TX, int TY>
+template <int TX, int TY, bool SORT = false>
 struct BatchSmem {
   static constexpr int NT = TX * TY;
   static constexpr size_t s1d = (S * (NT + 4) + NP * (NT + 2) + S * (NT + 1)) * sizeof(float);
-  static constexpr size_t s2d = Tile2dSmem32<TX, TY>::bytes;
+  static constexpr size_t s2d = Tile2dSmem32<TX, TY, SORT>::bytes;
   // Rate32 copy, rounded up to whole float4 plus one spare float4, then the tile work area.
   static constexpr size_t head = 16 * ((sizeof(Rate32) + 15) / 16 + 1);
   static constexpr size_t rate = head + (s2d > s1d ? s2d : s1d);
 };
 
-template <int TX, int TY, int MINB, bool WIN>
+template <int TX, int TY, int MINB, bool WIN, bool SORT = false>
 __global__ void __launch_bounds__(TX * TY, MINB)
     kb_rate(const BSolve *__restrict__ solves, int nsolves, int total_tiles) {
   constexpr int NT = TX * TY;
   extern __shared__ float4 sm4[];
   Rate32 *Rs = reinterpret_cast<Rate32 *>(sm4);
-  float4 *work = sm4 + BatchSmem<TX, TY>::head / 16;
+  float4 *work = sm4 + BatchSmem<TX, TY, SORT>::head / 16;
   const int tid = threadIdx.y * TX + threadIdx.x;
   for (int t = blockIdx.x; t < total_tiles; t += gridDim.x) {
     const int si = find_solve_tile(solves, nsolves, t);
@@ -172,7 +172,7 @@ __global__ void __launch_bounds__(TX * TY, MINB)
     unsigned flags = 0;
     float vmax;
     if (B.dim == 2)
-      vmax = tile2d32_body<TX, TY, WIN>(P, local % B.ntx, local / B.ntx, work, &flags, tid);
+      vmax = tile2d32_body<TX, TY, WIN, SORT>(P, local % B.ntx, local / B.ntx, work, &flags, tid);
     else
       vmax = tile1d32_body<NT>(B, P, local, reinterpret_cast<float *>(work), &flags, tid);
     if (flags) atomicOr(&P.st->flags, flags);
@@ -374,25 +374,26 @@ struct BatchVariant {
   int (*occupancy)();
 };
 
-template <int TX, int TY, int MINB, bool WIN>
+template <int TX, int TY, int MINB, bool WIN, bool SORT = false>
 BatchVariant make_bvariant() {
+  using SM = BatchSmem<TX, TY, SORT>;
   BatchVariant v;
   v.tx = TX;
   v.ty = TY;
   v.minb = MINB;
   v.win = WIN;
-  v.smem = BatchSmem<TX, TY>::rate;
+  v.smem = SM::rate;
   v.set_attrs = []() {
-    cudaFuncSetAttribute(kb_rate<TX, TY, MINB, WIN>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                         (int)BatchSmem<TX, TY>::rate);
+    cudaFuncSetAttribute(kb_rate<TX, TY, MINB, WIN, SORT>,
+                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SM::rate);
   };
   v.launch = [](int grid, cudaStream_t s, const BSolve *solves, int n, int tiles) {
-    kb_rate<TX, TY, MINB, WIN><<<grid, dim3(TX, TY), BatchSmem<TX, TY>::rate, s>>>(solves, n, tiles);
+    kb_rate<TX, TY, MINB, WIN, SORT><<<grid, dim3(TX, TY), SM::rate, s>>>(solves, n, tiles);
   };
   v.occupancy = []() {
     int nb = 0;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, kb_rate<TX, TY, MINB, WIN>, TX * TY,
-                                                  BatchSmem<TX, TY>::rate);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, kb_rate<TX, TY, MINB, WIN, SORT>, TX * TY,
+                                                  SM::rate);
     return nb;
   };
   return v;
@@ -402,7 +403,9 @@ const std::vector<BatchVariant> &batch_variants() {
   static const std::vector<BatchVariant> v = {
       make_bvariant<32, 8, 2, true>(), make_bvariant<32, 8, 3, true>(),
       make_bvariant<32, 8, 2, false>(), make_bvariant<32, 8, 3, false>(),
-      make_bvariant<32, 4, 4, true>(), make_bvariant<64, 4, 2, true>()};
+      make_bvariant<32, 4, 4, true>(), make_bvariant<64, 4, 2, true>(),
+      make_bvariant<32, 8, 2, false, true>(), make_bvariant<32, 8, 3, false, true>(),
+      make_bvariant<32, 16, 2, false, true>()};
   return v;
 }
 
@@ -832,6 +835,8 @@ pf5d_status pf5d_batch_set_variant(pf5d_batch *h, int32_t variant) {
   if (st == PF5D_OK) drop_graphs(h);
   return st;
 }
+
+int32_t pf5d_batch_variant_count(void) { return (int32_t)batch_variants().size(); }
 
 pf5d_status pf5d_batch_autotune(pf5d_batch *h, int32_t *variant, float *best_ms, void *stream) {
   PF5D_REQUIRE(h, PF5D_ERR_ARG, "null batch");

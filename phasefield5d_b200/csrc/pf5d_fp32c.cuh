@@ -291,15 +291,43 @@ __device__ __forceinline__ bool skip_pos(int mx, int my, bool interior_only) {
   return interior_only ? (ex || ey) : (ex && ey);
 }
 
+// Shared-memory scratch of a per-tile cell sort: hist[256], wsum[NT/32+1],
+// order/rank/key per mu/M position.
+struct SortScratch32 {
+  int *hist;
+  int *wsum;
+  unsigned short *order;
+  unsigned short *rank;
+  unsigned char *key;
+};
+
+template <int TX, int TY>
+struct SortBytes32 {
+  using G = PlaneGeom<TX, TY>;
+  static constexpr size_t bytes = (256 + G::NT / 32 + 1) * sizeof(int) + G::PM * (2 * 2 + 1);
+  static __device__ __forceinline__ SortScratch32 carve(void *base) {
+    SortScratch32 s;
+    s.hist = reinterpret_cast<int *>(base);
+    s.wsum = s.hist + 256;
+    s.order = reinterpret_cast<unsigned short *>(s.wsum + G::NT / 32 + 1);
+    s.rank = s.order + G::PM;
+    s.key = reinterpret_cast<unsigned char *>(s.rank + G::PM);
+    return s;
+  }
+};
+
 // mu/M of one plane (tile + 1-cell halo, or the tile only) into dst.  Xm/Xp
 // are the neighbouring planes along axis 0 in 3D (nullptr in 2D, where the
 // y-neighbours sit in the same plane).  Stages the table window first.
-template <int TX, int TY, int DIM, bool WIN>
+// SORT: positions evaluated in table-cell order (cell_hash counting sort),
+// so the lanes of a warp gather the same table nodes; only the thread that
+// evaluates a position changes.
+template <int TX, int TY, int DIM, bool WIN, bool SORT = false>
 __device__ __forceinline__ void mu_plane32(const Rate32 &P, const float *Xm, const float *Xc,
                                            const float *Xp, float *dst, int64_t zoff,
                                            const int *wx, const int *wy, bool interior_only,
                                            float4 *win, int *red, int *win_lo, unsigned *flags,
-                                           int tid) {
+                                           int tid, SortScratch32 ss = {}) {
   using G = PlaneGeom<TX, TY>;
   // 1. table window around the tile centre's cell (reloaded if it moved).
   int rep[S];
@@ -315,10 +343,37 @@ __device__ __forceinline__ void mu_plane32(const Rate32 &P, const float *Xm, con
     ensure_window<kWin32, 3, float4, G::NT>(reinterpret_cast<const float4 *>(P.T.grid), P.T.n, o,
                                             win, win_lo, tid);
   }
-  // 2. interpolation + Laplacian + mu assembly.
-  for (int pos = tid; pos < G::PM; pos += G::NT) {
+  // 2. (SORT) table-cell order of the positions.
+  int nwork = G::PM;
+  if constexpr (SORT) {
+    for (int i = tid; i < 256; i += G::NT) ss.hist[i] = 0;
+    __syncthreads();
+    for (int pos = tid; pos < G::PM; pos += G::NT) {
+      const int my = pos / G::MX, mx = pos - my * G::MX;
+      if (skip_pos<G::MX, G::MY>(mx, my, interior_only)) {
+        ss.rank[pos] = 0xFFFFu;
+        continue;
+      }
+      const int px = (my + 1) * G::HX + (mx + 1);
+      float u[S];
+#pragma unroll
+      for (int c = 0; c < S; ++c)
+        u[c] = fmaf(Xc[c * G::PX + px], P.T.inv_step_f, P.T.fb[c]) + (float)P.T.ib[c];
+      const int k = cell_hash_u(u);
+      ss.key[pos] = (unsigned char)k;
+      ss.rank[pos] = (unsigned short)atomicAdd(&ss.hist[k], 1);
+    }
+    __syncthreads();
+    nwork = block_exclusive_scan<256, G::NT>(ss.hist, ss.wsum, tid);
+    for (int pos = tid; pos < G::PM; pos += G::NT)
+      if (ss.rank[pos] != 0xFFFFu) ss.order[ss.hist[ss.key[pos]] + ss.rank[pos]] = (unsigned short)pos;
+    __syncthreads();
+  }
+  // 3. interpolation + Laplacian + mu assembly.
+  for (int w = tid; w < nwork; w += G::NT) {
+    const int pos = SORT ? (int)ss.order[w] : w;
     const int my = pos / G::MX, mx = pos - my * G::MX;
-    if (skip_pos<G::MX, G::MY>(mx, my, interior_only)) continue;
+    if (!SORT && skip_pos<G::MX, G::MY>(mx, my, interior_only)) continue;
     const int px = (my + 1) * G::HX + (mx + 1);
     float d[S], lap[S];
 #pragma unroll
@@ -393,11 +448,12 @@ __device__ __forceinline__ void raise32(StepState32 *st, unsigned f) {
 // scratch, X (tile + 2 halo), mu/M (tile + 1 halo), x- and y-face fluxes,
 // window scratch/origin, halo index tables.
 // ------------------------------------------------------------------------
-template <int TX, int TY>
+template <int TX, int TY, bool SORT = false>
 struct Tile2dSmem32 {
   using G = PlaneGeom<TX, TY>;
   static constexpr size_t bytes = Smem32Tail<TX, TY>::bytes +
-      (S * G::PX + NP * G::PM + S * G::NFX + S * G::NFY) * sizeof(float);
+      (S * G::PX + NP * G::PM + S * G::NFX + S * G::NFY) * sizeof(float) +
+      (SORT ? SortBytes32<TX, TY>::bytes : 0);
   static __device__ __forceinline__ double *red(float4 *sm4) {
     return reinterpret_cast<double *>(sm4 + kWinNodes32 * 3);
   }
@@ -405,7 +461,7 @@ struct Tile2dSmem32 {
 
 // Evaluates tile (bx, by) of solve P and writes its dX/dt; returns this
 // thread's max |dX/dt|.  Ends with all threads past a barrier.
-template <int TX, int TY, bool WIN>
+template <int TX, int TY, bool WIN, bool SORT = false>
 __device__ __forceinline__ float tile2d32_body(const Rate32 &P, int bx, int by, float4 *sm4,
                                                unsigned *flags, int tid) {
   using G = PlaneGeom<TX, TY>;
@@ -419,6 +475,8 @@ __device__ __forceinline__ float tile2d32_body(const Rate32 &P, int bx, int by, 
   int *win_lo = wred + S * (G::NT / 32);
   int *wx = win_lo + S + 1;
   int *wy = wx + G::HX;
+  SortScratch32 ss{};
+  if constexpr (SORT) ss = SortBytes32<TX, TY>::carve(wy + G::HY);
   const int tx = tid % TX, ty = tid / TX;
   const int x0 = bx * TX, y0 = by * TY;
   if (tid == 0) win_lo[S] = 0;
@@ -429,8 +487,8 @@ __device__ __forceinline__ float tile2d32_body(const Rate32 &P, int bx, int by, 
   __syncthreads();
   load_plane32<TX, TY>(P.D, 0, wx, wy, P.nx, Xs, tid);
   __syncthreads();
-  mu_plane32<TX, TY, 2, WIN>(P, nullptr, Xs, nullptr, Ms, 0, wx, wy, false, win, wred, win_lo,
-                             flags, tid);
+  mu_plane32<TX, TY, 2, WIN, SORT>(P, nullptr, Xs, nullptr, Ms, 0, wx, wy, false, win, wred,
+                                   win_lo, flags, tid, ss);
   __syncthreads();
   plane_faces32<TX, TY>(P, Xs, Ms, Fx, Fy, tid);
   __syncthreads();

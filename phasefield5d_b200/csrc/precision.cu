@@ -39,23 +39,24 @@ namespace pf5d {
 // Rate kernels (same tiling as the FP64 kernels)
 // ------------------------------------------------------------------------
 
-template <int TX, int TY, int MINB, bool WIN>
+template <int TX, int TY, int MINB, bool WIN, bool SORT = false>
 __global__ void __launch_bounds__(TX * TY, MINB) k32_rate_tile2d(Rate32 P) {
   if (P.st->halt) return;
   extern __shared__ float4 sm4[];
   const int tid = threadIdx.y * TX + threadIdx.x;
   unsigned flags = 0;
-  const float vmax = tile2d32_body<TX, TY, WIN>(P, blockIdx.x, blockIdx.y, sm4, &flags, tid);
+  const float vmax =
+      tile2d32_body<TX, TY, WIN, SORT>(P, blockIdx.x, blockIdx.y, sm4, &flags, tid);
   if (flags) atomicOr(&P.st->flags, flags);
-  finish_rate32(P, vmax, Tile2dSmem32<TX, TY>::red(sm4));
+  finish_rate32(P, vmax, Tile2dSmem32<TX, TY, SORT>::red(sm4));
 }
 
-template <int TX, int TY>
+template <int TX, int TY, bool SORT = false>
 constexpr size_t tile2d32_smem() {
-  return Tile2dSmem32<TX, TY>::bytes;
+  return Tile2dSmem32<TX, TY, SORT>::bytes;
 }
 
-template <int TX, int TY, int MINB, bool WIN>
+template <int TX, int TY, int MINB, bool WIN, bool SORT = false>
 __global__ void __launch_bounds__(TX * TY, MINB) k32_rate_march3d(Rate32 P, int zc) {
   using G = PlaneGeom<TX, TY>;
   if (P.st->halt) return;
@@ -70,6 +71,8 @@ __global__ void __launch_bounds__(TX * TY, MINB) k32_rate_march3d(Rate32 P, int 
   int *win_lo = wred + S * (G::NT / 32);
   int *wx = win_lo + S + 1;
   int *wy = wx + G::HX;
+  SortScratch32 ss{};
+  if constexpr (SORT) ss = SortBytes32<TX, TY>::carve(wy + G::HY);
   const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * TX + tx;
   const int x0 = blockIdx.x * TX, y0 = blockIdx.y * TY;
   const int zb = blockIdx.z * zc;
@@ -87,9 +90,9 @@ __global__ void __launch_bounds__(TX * TY, MINB) k32_rate_march3d(Rate32 P, int 
     load_plane32<TX, TY>(P.D, (int64_t)wrap_any(z, P.nz) * plane, wx, wy, P.nx, xplane(z), tid);
   };
   auto compute_mu = [&](int z, bool interior_only) {
-    mu_plane32<TX, TY, 3, WIN>(P, xplane(z - 1), xplane(z), xplane(z + 1), mplane(z),
-                          (int64_t)wrap_any(z, P.nz) * plane, wx, wy, interior_only, win, wred,
-                          win_lo, &flags, tid);
+    mu_plane32<TX, TY, 3, WIN, SORT>(P, xplane(z - 1), xplane(z), xplane(z + 1), mplane(z),
+                                     (int64_t)wrap_any(z, P.nz) * plane, wx, wy, interior_only,
+                                     win, wred, win_lo, &flags, tid, ss);
   };
   const int pX = (ty + 2) * G::HX + (tx + 2);
   const int pM = (ty + 1) * G::MX + (tx + 1);
@@ -138,11 +141,12 @@ __global__ void __launch_bounds__(TX * TY, MINB) k32_rate_march3d(Rate32 P, int 
   finish_rate32(P, vmax, red);
 }
 
-template <int TX, int TY>
+template <int TX, int TY, bool SORT = false>
 constexpr size_t march3d32_smem() {
   using G = PlaneGeom<TX, TY>;
   return Smem32Tail<TX, TY>::bytes +
-         (3 * S * G::PX + 2 * NP * G::PM + S * G::NFX + S * G::NFY) * sizeof(float);
+         (3 * S * G::PX + 2 * NP * G::PM + S * G::NFX + S * G::NFY) * sizeof(float) +
+         (SORT ? SortBytes32<TX, TY>::bytes : 0);
 }
 
 template <int TX>
@@ -375,24 +379,26 @@ struct Variant32 {
   void (*launch3d)(dim3, dim3, size_t, cudaStream_t, const Rate32 &, int);
 };
 
-template <int TX, int TY, int MINB, bool WIN = true>
+template <int TX, int TY, int MINB, bool WIN = true, bool SORT = false>
 Variant32 make_variant32() {
   Variant32 v;
   v.tx = TX;
   v.ty = TY;
   v.minb = MINB;
-  v.smem2d = tile2d32_smem<TX, TY>();
-  v.smem3d = march3d32_smem<TX, TY>();
+  v.smem2d = tile2d32_smem<TX, TY, SORT>();
+  v.smem3d = march3d32_smem<TX, TY, SORT>();
   v.set_attrs = []() {
     const auto a = cudaFuncAttributeMaxDynamicSharedMemorySize;
-    cudaFuncSetAttribute(k32_rate_tile2d<TX, TY, MINB, WIN>, a, (int)tile2d32_smem<TX, TY>());
-    cudaFuncSetAttribute(k32_rate_march3d<TX, TY, MINB, WIN>, a, (int)march3d32_smem<TX, TY>());
+    cudaFuncSetAttribute(k32_rate_tile2d<TX, TY, MINB, WIN, SORT>, a,
+                         (int)tile2d32_smem<TX, TY, SORT>());
+    cudaFuncSetAttribute(k32_rate_march3d<TX, TY, MINB, WIN, SORT>, a,
+                         (int)march3d32_smem<TX, TY, SORT>());
   };
   v.launch2d = [](dim3 g, dim3 b, size_t sm, cudaStream_t s, const Rate32 &P) {
-    k32_rate_tile2d<TX, TY, MINB, WIN><<<g, b, sm, s>>>(P);
+    k32_rate_tile2d<TX, TY, MINB, WIN, SORT><<<g, b, sm, s>>>(P);
   };
   v.launch3d = [](dim3 g, dim3 b, size_t sm, cudaStream_t s, const Rate32 &P, int zc) {
-    k32_rate_march3d<TX, TY, MINB, WIN><<<g, b, sm, s>>>(P, zc);
+    k32_rate_march3d<TX, TY, MINB, WIN, SORT><<<g, b, sm, s>>>(P, zc);
   };
   return v;
 }
@@ -401,7 +407,9 @@ const std::vector<Variant32> &variants32() {
   static const std::vector<Variant32> v = {
       make_variant32<32, 8, 2>(), make_variant32<32, 8, 3>(), make_variant32<32, 8, 4>(),
       make_variant32<32, 4, 6>(), make_variant32<64, 4, 3>(), make_variant32<32, 16, 2>(),
-      make_variant32<32, 8, 2, false>(), make_variant32<32, 16, 2, false>()};
+      make_variant32<32, 8, 2, false>(), make_variant32<32, 16, 2, false>(),
+      make_variant32<32, 8, 2, true, true>(), make_variant32<32, 8, 3, false, true>(),
+      make_variant32<32, 16, 2, false, true>(), make_variant32<32, 8, 2, false, true>()};
   return v;
 }
 

@@ -604,7 +604,7 @@ struct March64Geom {
   static constexpr int NFMAX = G::NFX > G::NFY ? G::NFX : G::NFY;
 };
 
-template <int TX, int TY, int MINB, bool VEC, bool WIN, bool SPLIT = false>
+template <int TX, int TY, int MINB, bool VEC, bool WIN, bool SPLIT = false, bool SORT = false>
 __global__ void __launch_bounds__(TX * TY, MINB) k_rate_march3d(RateParams P, int zc) {
   using G = PlaneGeom<TX, TY>;
   if (P.st->halt) return;
@@ -617,6 +617,14 @@ __global__ void __launch_bounds__(TX * TY, MINB) k_rate_march3d(RateParams P, in
   int *wx = reinterpret_cast<int *>(red + G::NT / 32);
   int *wy = wx + G::HX;
   int *win_lo = wy + G::HY;                                  // [S+1]
+  SortScratch ss{};
+  if constexpr (SORT) {
+    ss.hist = win_lo + S + 1;                                // [256]
+    ss.wsum = ss.hist + 256;                                 // [NT/32 + 1]
+    ss.order = reinterpret_cast<unsigned short *>(ss.wsum + G::NT / 32 + 1);   // [PM]
+    ss.rank = ss.order + G::PM;                              // [PM]
+    ss.key = reinterpret_cast<unsigned char *>(ss.rank + G::PM);               // [PM]
+  }
   const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * TX + tx;
   const int x0 = blockIdx.x * TX, y0 = blockIdx.y * TY;
   const int zb = blockIdx.z * zc;
@@ -639,9 +647,10 @@ __global__ void __launch_bounds__(TX * TY, MINB) k_rate_march3d(RateParams P, in
       load_mu_plane<TX, TY>(P, (int64_t)wrap_any(z, P.nz) * plane, wx, wy, interior_only,
                             mplane(z), tid);
     else
-      mu_plane64<TX, TY, 3, VEC, WIN>(P, xplane(z - 1), xplane(z), xplane(z + 1), mplane(z),
-                                      (int64_t)wrap_any(z, P.nz) * plane, wx, wy, interior_only,
-                                      win, win_lo, &flags, tid);
+      mu_plane64<TX, TY, 3, VEC, WIN, TX * TY, SORT>(P, xplane(z - 1), xplane(z), xplane(z + 1),
+                                                     mplane(z), (int64_t)wrap_any(z, P.nz) * plane,
+                                                     wx, wy, interior_only, win, win_lo, &flags,
+                                                     tid, ss);
   };
   const int pX = (ty + 2) * G::HX + (tx + 2);
   const int pM = (ty + 1) * G::MX + (tx + 1);
@@ -719,12 +728,13 @@ __global__ void __launch_bounds__(TX * TY, MINB) k_rate_march3d(RateParams P, in
   finish_rate(P, vmax, red);
 }
 
-template <int TX, int TY>
+template <int TX, int TY, bool SORT = false>
 constexpr size_t march3d_smem() {
   using G = PlaneGeom<TX, TY>;
+  const size_t sort = SORT ? (256 + G::NT / 32 + 1) * sizeof(int) + G::PM * (2 * 2 + 1) : 0;
   return (3 * S * G::PX + 2 * NP * G::PM + S * March64Geom<TX, TY>::NFMAX + G::NT / 32) *
              sizeof(double) +
-         kWinNodes64 * kNodeV64 * sizeof(double2) + (G::HX + G::HY + S + 1) * sizeof(int);
+         kWinNodes64 * kNodeV64 * sizeof(double2) + (G::HX + G::HY + S + 1) * sizeof(int) + sort;
 }
 
 // ------------------------------------------------------------------------
@@ -971,8 +981,8 @@ struct RateVariant {
                    int zc);
 };
 
-// NTH / SORT shape the 2D kernel only; in 3D such a variant runs the
-// marching kernel of the same tile.
+// NTH shapes the 2D kernel only (the 3D marching kernel has one thread per
+// tile point); SORT applies to both.
 template <int TX, int TY, int MINB, bool WIN = true, int NTH = TX * TY, bool SORT = false>
 RateVariant make_variant() {
   RateVariant v;
@@ -983,16 +993,16 @@ RateVariant make_variant() {
   v.win = WIN;
   v.split = false;
   v.smem2d = tile2d_smem<TX, TY, NTH, SORT>();
-  v.smem3d = march3d_smem<TX, TY>();
+  v.smem3d = march3d_smem<TX, TY, SORT>();
   v.set_attrs = [](bool vec) {
-    const int s2 = (int)tile2d_smem<TX, TY, NTH, SORT>(), s3 = (int)march3d_smem<TX, TY>();
+    const int s2 = (int)tile2d_smem<TX, TY, NTH, SORT>(), s3 = (int)march3d_smem<TX, TY, SORT>();
     const auto a = cudaFuncAttributeMaxDynamicSharedMemorySize;
     if (vec) {
       cudaFuncSetAttribute(k_rate_tile2d<TX, TY, MINB, true, WIN, false, NTH, SORT>, a, s2);
-      cudaFuncSetAttribute(k_rate_march3d<TX, TY, MINB, true, WIN>, a, s3);
+      cudaFuncSetAttribute(k_rate_march3d<TX, TY, MINB, true, WIN, false, SORT>, a, s3);
     } else {
       cudaFuncSetAttribute(k_rate_tile2d<TX, TY, MINB, false, WIN, false, NTH, SORT>, a, s2);
-      cudaFuncSetAttribute(k_rate_march3d<TX, TY, MINB, false, WIN>, a, s3);
+      cudaFuncSetAttribute(k_rate_march3d<TX, TY, MINB, false, WIN, false, SORT>, a, s3);
     }
   };
   v.launch2d = [](bool vec, dim3 g, dim3 b, size_t sm, cudaStream_t s, const RateParams &P) {
@@ -1001,8 +1011,8 @@ RateVariant make_variant() {
   };
   v.launch3d = [](bool vec, dim3 g, dim3 b, size_t sm, cudaStream_t s, const RateParams &P,
                   int zc) {
-    if (vec) k_rate_march3d<TX, TY, MINB, true, WIN><<<g, b, sm, s>>>(P, zc);
-    else k_rate_march3d<TX, TY, MINB, false, WIN><<<g, b, sm, s>>>(P, zc);
+    if (vec) k_rate_march3d<TX, TY, MINB, true, WIN, false, SORT><<<g, b, sm, s>>>(P, zc);
+    else k_rate_march3d<TX, TY, MINB, false, WIN, false, SORT><<<g, b, sm, s>>>(P, zc);
   };
   return v;
 }

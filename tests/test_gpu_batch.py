@@ -86,7 +86,8 @@ def test_variants_agree(small_probs):
     """Every batch-kernel variant computes each point the same way."""
     from phasefield5d_b200.batch import BatchStepper
     ref = None
-    for v in range(6):
+    from phasefield5d_b200 import _lib
+    for v in range(int(_lib.load().pf5d_batch_variant_count())):
         b = BatchStepper(small_probs[:4], autotune=False)
         b.set_variant(v)
         b.advance(9)
