@@ -94,11 +94,12 @@ def measured_peak():
         return FALLBACK_HBM_GBS, "fallback"
 
 
-def committed_traffic(kernel, workload):
-    """dram bytes per launch of ``kernel`` from the committed ncu summary."""
+def committed_traffic(kernel, workload, precision):
+    """DRAM bytes per launch of ``kernel`` on this workload from the committed
+    ncu capture (profiles/traffic.json), or None when none was taken."""
     try:
         with open(os.path.join(HERE, "profiles", "traffic.json")) as f:
-            ent = json.load(f)[kernel][workload]
+            ent = json.load(f)[kernel][f"{workload}_{precision}"]
         return float(ent["dram_bytes_per_launch"])
     except Exception:
         return None
@@ -536,7 +537,7 @@ def run_ours(args, rank, world, local_rank):
         "roofline": {"bound": "hbm", "kernel": "k_rate_march (fused chemical potential + flux "
                                                "divergence)" if prob.dim > 1 else "k_rate_1d",
                      "achieved": achieved, "peak": peak, "peak_kind": peak_kind, "unit": "GB/s",
-                     "frac": achieved / peak, "traffic": committed_traffic("rate", args.workload),
+                     "frac": achieved / peak, "traffic": committed_traffic("rate", args.workload, args.precision),
                      "algorithmic_bytes_per_launch": rate_bytes,
                      "ms_per_launch": stage_ms["rate"]},
         "step_roofline": {"bytes_per_grid_point_step": per_step,

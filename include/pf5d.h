@@ -230,6 +230,34 @@ pf5d_status pf5d_stepper_autotune(pf5d_stepper *h, int32_t *variant, float *best
                                   void *stream);
 /* Select a rate-kernel variant explicitly (index from a previous autotune). */
 pf5d_status pf5d_stepper_set_variant(pf5d_stepper *h, int32_t variant);
+/* Save-step diagnostics of one step (examples/simulate.py:299-354): the
+ * values the reference records in its traces at a save step.  "Before" values
+ * use the step's dX/dt before it is scaled by dt; "after" values use the
+ * field after the update and clamp. */
+typedef struct {
+  double net[4];            /* before: sum over space of dX/dt */
+  double max_change[4];     /* before: max over space of |dX/dt| per component */
+  double total_flux[4];     /* before: sum over space and axes of flux_p - flux_m */
+  double mass[4];           /* after: sum over space of X */
+  double comp_min[4];       /* after: min over space of X */
+  double comp_max[4];       /* after: max over space of X */
+  double comp_fe_min;       /* after: 1 - max over space of sum_s X_s */
+  double comp_var[4];       /* after: variance over space of X (population) */
+  double f_grad;            /* after: -(dx^dim / 2) sum X . kappa lap X */
+  double xdotmax;           /* the step's max |dX/dt| (abs_max) */
+  double dt;                /* the step's time increment */
+  double time;              /* time after the step */
+  int64_t step;             /* index of this step (count before it) */
+  int32_t halted;           /* 1: the stepper was halted before; nothing ran */
+  int32_t pad;
+} pf5d_save_diag;
+
+/* One step, exactly as pf5d_stepper_advance(h, 1), plus the save-step
+ * diagnostics of that step; synchronises the stream.  Replaces the save
+ * branch of examples/simulate.py:299-354 (calculate_gradients_pm,
+ * compute_fluxes and the numpy reductions).  Plain FP64 form only
+ * (PF5D_ERR_ARG for the FP32C form). */
+pf5d_status pf5d_stepper_step_save(pf5d_stepper *h, pf5d_save_diag *out, void *stream);
 /* Number of rate-kernel variants of this stepper's form (valid indices for
  * pf5d_stepper_set_variant are 0 .. count-1); 0 for a null stepper. */
 int32_t pf5d_stepper_variant_count(const pf5d_stepper *h);

@@ -230,6 +230,38 @@ def make_elastic_updater(X0, lvec, elastic_kernel_r, field_shape, fft_workers=-1
 # Step loop (examples/simulate.py:230-320, saves off)
 # ---------------------------------------------------------------------------
 
+def run_simulation(ost, total_steps, path, *, ctld, t_cfl, early_stage_frames=100,
+                   late_burst_duration_ctld=100, late_burst_frames=700, late_tail_frames=300,
+                   oob_interval=100):
+    """The main loop of examples/simulate.py:200-365 on an ``OracleStepper``:
+    the out-of-bounds check every ``oob_interval`` steps, ``should_save``
+    called every step with the time after it, state files and traces at
+    data saves, the final state.  Returns (traces, files)."""
+    from phasefield5d_b200.solver.io import (finalize_traces, init_traces,
+                                             save_current_state, should_save, update_traces)
+    kw = dict(early_frames=early_stage_frames, burst_duration_ctld=late_burst_duration_ctld,
+              burst_frames=late_burst_frames, tail_dt_ctld=late_tail_frames, snapshot_factor=10)
+    files = [save_current_state(path, 0, 0, 0.0, ost.X, postfix="_initial")]
+    traces = init_traces(4)
+    should_save._state = None
+    timestep = 0
+    for timestep in range(total_steps):
+        if timestep % oob_interval == 0 and out_of_bounds(ost.X):
+            files.append(save_current_state(path, timestep, ost.dt, ost.time, ost.X,
+                                            postfix="_out_of_bound"))
+            break
+        d = ost.step_save()
+        save_data, _ = should_save(timestep, ctld, d["time"], total_steps, **kw)
+        if save_data:
+            files.append(save_current_state(path, timestep, d["dt"], d["time"], ost.X))
+            update_traces(traces, timestep, d["time"], d["dt"], t_cfl, d["net"], d["xdotmax"],
+                          d["max_change"], d["mass"], d["total_flux"], d["comp_min"],
+                          d["comp_max"], d["comp_fe_min"], d["comp_var"], d["f_grad"])
+    files.append(save_current_state(path, timestep, ost.dt, ost.time, ost.X))
+    finalize_traces(path, traces)
+    return traces, files
+
+
 class OracleStepper:
     """Explicit Euler loop of the reference driver on host arrays.
 
@@ -302,6 +334,43 @@ class OracleStepper:
         lib().orc_update(_p(self.X), _p(self.dXdt), self.X.size, self.dt)
         clamp_simplex(self.X)
         self.step_index += 1
+
+    def step_save(self):
+        """One step with the save-step diagnostics of examples/simulate.py:299-354
+        (numpy reductions in the reference's form).  ``flux_abs`` (the sum of
+        |flux_p| + |flux_m|) is the scale of the total-flux rounding noise."""
+        ax = tuple(range(self.dim))
+        self.compute_rate()
+        if self.adaptive:
+            self.dt = apply_adaptive_time(self.dt, self.xdotmax, self.ctld, self.t_cfl,
+                                          composition_change_lower_limit=self.lower,
+                                          composition_change_upper_limit=self.upper)
+        net = np.sum(self.dXdt, axis=ax)
+        max_change = np.max(np.abs(self.dXdt), axis=ax)
+        mu = np.ascontiguousarray(self.interp[..., :4])
+        M = self.interp[..., 4:]
+        gp, gm = calculate_gradients_pm(mu, self.dx)
+        fp = np.empty_like(gp)
+        fm = np.empty_like(gm)
+        compute_fluxes(self.X, M, gp, gm, fp, fm)
+        step = self.step_index
+        self.time += self.dt
+        lib().orc_update(_p(self.X), _p(self.dXdt), self.X.size, self.dt)
+        clamp_simplex(self.X)
+        self.step_index += 1
+        lap = np.empty_like(self.X)
+        calculate_laplacian(self.X, self.dx, lap)
+        lap *= self.kappa
+        return dict(
+            net=net, max_change=max_change,
+            total_flux=np.sum(fp - fm, axis=tuple(range(self.dim + 1))),
+            flux_abs=float(np.sum(np.abs(fp)) + np.sum(np.abs(fm))),
+            mass=np.sum(self.X, axis=ax), comp_min=np.min(self.X, axis=ax),
+            comp_max=np.max(self.X, axis=ax),
+            comp_fe_min=1.0 - float(np.max(self.X.sum(axis=-1))),
+            comp_var=np.var(self.X, axis=ax),
+            f_grad=-0.5 * (self.dx ** self.dim) * float(np.sum(self.X * lap)),
+            xdotmax=self.xdotmax, dt=self.dt, time=self.time, step=step, halted=False)
 
     def run(self, n_steps, oob_interval=100):
         """Advance n_steps; stops early (returns False) on a hard OOB check,

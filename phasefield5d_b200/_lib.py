@@ -73,6 +73,15 @@ class StepState(ctypes.Structure):
                 ("flags", ctypes.c_uint32), ("halted", ctypes.c_uint32)]
 
 
+class SaveDiag(ctypes.Structure):
+    """pf5d_save_diag (include/pf5d.h)."""
+    _fields_ = [("net", _f64 * 4), ("max_change", _f64 * 4), ("total_flux", _f64 * 4),
+                ("mass", _f64 * 4), ("comp_min", _f64 * 4), ("comp_max", _f64 * 4),
+                ("comp_fe_min", _f64), ("comp_var", _f64 * 4), ("f_grad", _f64),
+                ("xdotmax", _f64), ("dt", _f64), ("time", _f64), ("step", _i64),
+                ("halted", _i32), ("pad", _i32)]
+
+
 _SIGS = {
     "pf5d_last_error": (ctypes.c_char_p, []),
     "pf5d_version": (_i32, []),
@@ -104,6 +113,7 @@ _SIGS = {
                                      _vp]),
     "pf5d_stepper_set_variant": (_i32, [_vp, _i32]),
     "pf5d_stepper_variant_count": (_i32, [_vp]),
+    "pf5d_stepper_step_save": (_i32, [_vp, ctypes.POINTER(SaveDiag), _vp]),
     "pf5d_batch_variant_count": (_i32, []),
     "pf5d_stepper_reset": (_i32, [_vp, _f64, _f64, _vp]),
     "pf5d_stepper_destroy": (_i32, [_vp]),

@@ -25,6 +25,7 @@
 // with -fmad=false, so apart from the FFT (cuFFT vs pocketfft rounding) the
 // trajectory equals the reference's bit for bit.
 #include <algorithm>
+#include <cstring>
 #include <map>
 #include <vector>
 
@@ -33,6 +34,7 @@
 #include "pf5d_fp32c.h"
 #include "pf5d_tiles.cuh"
 #include "pf5d_window.cuh"
+#include "pf5d_diag.cuh"
 
 namespace pf5d {
 
@@ -313,7 +315,10 @@ __global__ void __launch_bounds__(256, MINB) k_chem64(RateParams P) {
     const int yp = y + 1 == P.ny ? 0 : y + 1, ym = y == 0 ? P.ny - 1 : y - 1;
     double xc[S], lap[S], n0[S], n1[S];
     ld(g, xc);
-    if (DIM == 3) {
+    if (DIM == 1) {
+#pragma unroll
+      for (int c = 0; c < S; ++c) lap[c] = 0.0;
+    } else if (DIM == 3) {
       const int zp = z + 1 == P.nz ? 0 : z + 1, zm = z == 0 ? P.nz - 1 : z - 1;
       ld((int64_t)zp * plane + (int64_t)y * P.nx + x, n0);
       ld((int64_t)zm * plane + (int64_t)y * P.nx + x, n1);
@@ -333,7 +338,10 @@ __global__ void __launch_bounds__(256, MINB) k_chem64(RateParams P) {
     ld(zo + (int64_t)y * P.nx + xm, n1);
 #pragma unroll
     for (int c = 0; c < S; ++c) {
-      lap[c] = (((lap[c] + n0[c]) + n1[c]) - (DIM == 3 ? 6.0 : 4.0) * xc[c]) * P.inv_dx2;
+      if (DIM == 1)
+        lap[c] = ((n0[c] + n1[c]) - 2.0 * xc[c]) * P.inv_dx2;
+      else
+        lap[c] = (((lap[c] + n0[c]) + n1[c]) - (DIM == 3 ? 6.0 : 4.0) * xc[c]) * P.inv_dx2;
       io[c][tid] = xc[c];
       io[S + c][tid] = lap[c];
     }
@@ -957,7 +965,8 @@ struct pf5d_stepper {
   int variant = 0;
   Stepper32 *s32 = nullptr;      // FP32C form (all calls delegate)
   double *mass_ws = nullptr;     // FP64 mean reduction workspace
-  double *mm = nullptr;          // split-rate mu/M buffer (2D/3D)
+  double *mm = nullptr;          // split-rate mu/M buffer (also save-step diagnostics)
+  double *diag_ws = nullptr;     // save-step partial rows + mean
 };
 
 namespace {
@@ -1271,7 +1280,7 @@ pf5d_status pf5d_stepper_create(const pf5d_stepper_desc *desc, double *X, void *
     set_error("device allocation failed");
     return fail(PF5D_ERR_CUDA);
   }
-  if (desc->dim >= 2 && cudaMalloc(&h->mm, (size_t)npts * NP * sizeof(double)) != cudaSuccess) {
+  if (cudaMalloc(&h->mm, (size_t)npts * NP * sizeof(double)) != cudaSuccess) {
     set_error("device allocation failed");
     return fail(PF5D_ERR_CUDA);
   }
@@ -1444,6 +1453,110 @@ pf5d_status pf5d_stepper_set_variant(pf5d_stepper *h, int32_t variant) {
   return PF5D_OK;
 }
 
+pf5d_status pf5d_stepper_step_save(pf5d_stepper *h, pf5d_save_diag *out, void *stream) {
+  PF5D_REQUIRE(h && out, PF5D_ERR_ARG, "bad arguments");
+  PF5D_REQUIRE(!h->s32, PF5D_ERR_ARG, "save-step diagnostics are computed by the FP64 form");
+  cudaStream_t s = as_stream(stream);
+  std::memset(out, 0, sizeof(*out));
+  StepState before;
+  PF5D_CUDA(cudaMemcpyAsync(&before, h->st, sizeof(before), cudaMemcpyDeviceToHost, s));
+  PF5D_CUDA(cudaStreamSynchronize(s));
+  out->step = before.step;
+  if (before.halt) {
+    out->halted = 1;
+    out->dt = before.dt;
+    out->time = before.time;
+    return PF5D_OK;
+  }
+  const int rows = kDiagBlocks;
+  if (!h->diag_ws)
+    PF5D_CUDA(cudaMalloc(&h->diag_ws, (size_t)(rows * (kDiagPre + kDiagPost + kDiagVar) + S) *
+                                          sizeof(double)));
+  double *pre = h->diag_ws, *post = pre + rows * kDiagPre, *var = post + rows * kDiagPost;
+  double *mean = var + rows * kDiagVar;
+  DiagGeom G;
+  G.nz = h->rp.nz;
+  G.ny = h->rp.ny;
+  G.nx = h->rp.nx;
+  G.dim = h->d.dim;
+  G.npts = h->npts;
+  G.inv_dx = h->rp.inv_dx;
+  G.inv_dx2 = h->rp.inv_dx2;
+  for (int c = 0; c < S; ++c) G.kappa[c] = h->rp.kappa.v[c];
+  const unsigned nb = std::min<unsigned>(rows, grid_for(h->npts, kDiagThreads, 1));
+  // the step up to its rate evaluation, as enqueue_step
+  pf5d_status st;
+  if (h->d.elastic) {
+    if ((st = fft_forward(&h->fft, h->s, h->k, s)) != PF5D_OK) return st;
+    if ((st = launch_bmul(h->k, h->bk, h->fft.nk, &h->st->halt, s)) != PF5D_OK) return st;
+    if ((st = fft_inverse(&h->fft, h->k, h->s, s)) != PF5D_OK) return st;
+  }
+  if ((st = launch_rate(h, s)) != PF5D_OK) return st;
+  // mu and M of this step at every point, then the "before" reductions
+  switch (h->d.dim) {
+    case 1: launch_chem<1, 3>(h->vec, s, h->rp); break;
+    case 2: launch_chem<2, 3>(h->vec, s, h->rp); break;
+    default: launch_chem<3, 3>(h->vec, s, h->rp);
+  }
+  PF5D_LAUNCHED();
+  k_diag_pre<<<nb, kDiagThreads, 0, s>>>(G, h->X, h->dX, h->mm, pre);
+  PF5D_LAUNCHED();
+  k_update_step<<<grid_for(h->npts, 256, 4), 256, 0, s>>>(h->up);
+  PF5D_LAUNCHED();
+  k_diag_post<<<nb, kDiagThreads, 0, s>>>(G, h->X, post);
+  PF5D_LAUNCHED();
+  std::vector<double> hp((size_t)nb * kDiagPre), hq((size_t)nb * kDiagPost);
+  PF5D_CUDA(cudaMemcpyAsync(hp.data(), pre, hp.size() * sizeof(double), cudaMemcpyDeviceToHost, s));
+  PF5D_CUDA(cudaMemcpyAsync(hq.data(), post, hq.size() * sizeof(double), cudaMemcpyDeviceToHost, s));
+  StepState after;
+  PF5D_CUDA(cudaMemcpyAsync(&after, h->st, sizeof(after), cudaMemcpyDeviceToHost, s));
+  PF5D_CUDA(cudaStreamSynchronize(s));
+  for (int c = 0; c < S; ++c) {
+    double net = 0.0, mx = 0.0, tf = 0.0, mass = 0.0, nmn = -INFINITY, mxx = -INFINITY;
+    for (unsigned b = 0; b < nb; ++b) {
+      net += hp[b * kDiagPre + c];
+      mx = std::max(mx, hp[b * kDiagPre + S + c]);
+      tf += hp[b * kDiagPre + 2 * S + c];
+      mass += hq[b * kDiagPost + c];
+      nmn = std::max(nmn, hq[b * kDiagPost + S + c]);
+      mxx = std::max(mxx, hq[b * kDiagPost + 2 * S + c]);
+    }
+    out->net[c] = net;
+    out->max_change[c] = mx;
+    out->total_flux[c] = tf;
+    out->mass[c] = mass;
+    out->comp_min[c] = -nmn;
+    out->comp_max[c] = mxx;
+  }
+  double msum = -INFINITY, fg = 0.0;
+  for (unsigned b = 0; b < nb; ++b) {
+    msum = std::max(msum, hq[b * kDiagPost + 3 * S]);
+    fg += hq[b * kDiagPost + 3 * S + 1];
+  }
+  out->comp_fe_min = 1.0 - msum;
+  double cell = 1.0;
+  for (int d = 0; d < h->d.dim; ++d) cell *= h->d.dx;
+  out->f_grad = -0.5 * cell * fg;
+  double m[S];
+  for (int c = 0; c < S; ++c) m[c] = out->mass[c] / (double)h->npts;
+  PF5D_CUDA(cudaMemcpyAsync(mean, m, sizeof(m), cudaMemcpyHostToDevice, s));
+  k_diag_var<<<nb, kDiagThreads, 0, s>>>(G, h->X, mean, var);
+  PF5D_LAUNCHED();
+  std::vector<double> hv((size_t)nb * kDiagVar);
+  PF5D_CUDA(cudaMemcpyAsync(hv.data(), var, hv.size() * sizeof(double), cudaMemcpyDeviceToHost, s));
+  PF5D_CUDA(cudaStreamSynchronize(s));
+  for (int c = 0; c < S; ++c) {
+    double v = 0.0;
+    for (unsigned b = 0; b < nb; ++b) v += hv[b * kDiagVar + c];
+    out->comp_var[c] = v / (double)h->npts;
+  }
+  out->xdotmax = after.xdotmax;
+  out->dt = after.dt;
+  out->time = after.time;
+  out->halted = 0;          // the step ran; a halt it raised shows in the next state
+  return PF5D_OK;
+}
+
 int32_t pf5d_stepper_variant_count(const pf5d_stepper *h) {
   if (!h) return 0;
   return h->s32 ? s32_variant_count() : (int32_t)rate_variants().size();
@@ -1480,6 +1593,7 @@ pf5d_status pf5d_stepper_destroy(pf5d_stepper *h) {
   if (h->s32) s32_destroy(h->s32);
   cudaFree(h->mass_ws);
   cudaFree(h->mm);
+  cudaFree(h->diag_ws);
   for (auto &kv : h->graphs) cudaGraphExecDestroy(kv.second);
   fft_destroy(&h->fft);
   cudaFree(h->dX);

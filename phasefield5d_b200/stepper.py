@@ -150,6 +150,20 @@ class Stepper:
                                                 self._s()), "autotune")
         return int(v.value), float(ms.value)
 
+    def step_save(self):
+        """One step plus its save-step diagnostics (examples/simulate.py:299-354),
+        plain FP64 form: a dict with net, max_change, total_flux, mass,
+        comp_min, comp_max, comp_var (arrays of 4), comp_fe_min, f_grad,
+        xdotmax, dt, time (after the step), step (its index) and halted."""
+        d = _lib.SaveDiag()
+        _lib.check(self.L.pf5d_stepper_step_save(self.h, ctypes.byref(d), self._s()), "step_save")
+        self.steps_enqueued += 0 if d.halted else 1
+        out = {k: np.array(list(getattr(d, k))) for k in
+               ("net", "max_change", "total_flux", "mass", "comp_min", "comp_max", "comp_var")}
+        out.update(comp_fe_min=d.comp_fe_min, f_grad=d.f_grad, xdotmax=d.xdotmax, dt=d.dt,
+                   time=d.time, step=int(d.step), halted=bool(d.halted))
+        return out
+
     @property
     def n_variants(self):
         """Number of rate-kernel variants the autotuner chooses from."""

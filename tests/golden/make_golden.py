@@ -308,11 +308,79 @@ def gen_fullres(R):
     return out
 
 
+def schedule_times(n, ctld, dt0, growth, cap):
+    """A time series with geometric dt growth up to a cap (as the adaptive
+    rule produces), used to exercise every stage of the save schedule."""
+    t, dt, out = 0.0, dt0, []
+    for _ in range(n):
+        dt = min(dt * growth, cap)
+        t = t + dt
+        out.append(t)
+    return out
+
+
+SCHEDULE_CASES = [
+    # (n steps, ctld, dt0, growth, cap, should_save kwargs)
+    (3000, 1e-6, 1e-12, 1.01, 0.005e-6, dict(early_frames=7, burst_duration_ctld=3.0,
+                                              burst_frames=11, tail_dt_ctld=0.2,
+                                              snapshot_factor=10, save_every_n_steps_data=700,
+                                              save_every_n_steps_snap=1500)),
+    (30000, 2e-7, 1e-14, 1.05, 1e-9, dict(early_frames=100, burst_duration_ctld=100,
+                                          burst_frames=700, tail_dt_ctld=300,
+                                          snapshot_factor=10)),
+]
+
+
+def gen_save(ref, out_path):
+    """Save-step host logic of the reference (phasefield5d/solver/io.py):
+    should_save decisions over seeded time series, the state-file keys and
+    dtypes, and the trace columns."""
+    import tempfile
+    import phasefield5d.solver.io as IO
+    cases = []
+    for n, ctld, dt0, growth, cap, kw in SCHEDULE_CASES:
+        times = schedule_times(n, ctld, dt0, growth, cap)
+        data, snap = [], []
+        for step, t in enumerate(times):
+            d, sn = IO.should_save(step, ctld, t, n, **kw)
+            if d:
+                data.append(step)
+            if sn:
+                snap.append(step)
+        cases.append(dict(n=n, ctld=ctld, dt0=dt0, growth=growth, cap=cap, kwargs=kw,
+                          data_steps=data, snap_steps=snap))
+    with tempfile.TemporaryDirectory() as tmp:
+        os.makedirs(os.path.join(tmp, "data"))
+        X = np.arange(24, dtype=np.float64).reshape(3, 2, 4) / 100.0
+        IO.save_current_state(tmp, 12, 1e-9, 3e-7, X)
+        name = os.listdir(os.path.join(tmp, "data"))[0]
+        z = np.load(os.path.join(tmp, "data", name))
+        npz = dict(name=name, keys=sorted(z.files),
+                   dtypes={k: str(z[k].dtype) for k in z.files},
+                   shapes={k: list(z[k].shape) for k in z.files})
+        tr = IO.init_traces(4)
+        IO.update_traces(tr, 5, 1e-7, 1e-9, 2e-9, np.arange(4) * 1e-3, 0.5, np.arange(4) * 0.1,
+                         np.arange(4) + 1.0, np.arange(4) * 1e-18, np.arange(4) * 0.01,
+                         np.arange(4) * 0.02 + 0.1, 0.3, np.arange(4) * 1e-6, -2e-20)
+        IO.finalize_traces(tmp, tr)
+        with open(os.path.join(tmp, "timeseries_info.csv")) as f:
+            csv_text = f.read()
+        with open(os.path.join(tmp, "timeseries_info.json")) as f:
+            info = json.load(f)
+    with open(out_path, "w") as f:
+        json.dump(dict(schedule=cases, npz=npz, trace_csv=csv_text, trace_info=info), f, indent=1)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--ref", default="/root/reference")
+    ap.add_argument("--only-save", action="store_true",
+                    help="regenerate only the save-step host logic fixture")
     args = ap.parse_args()
     R = import_reference(args.ref)
+    gen_save(args.ref, os.path.join(HERE, "save_io.json"))
+    if args.only_save:
+        return
     table = W.find_unstable_table(small_cfg(2, (12, 10)))[0]
     np.savez_compressed(os.path.join(HERE, "table_small.npz"), data=table.data,
                         resolution=table.resolution, temperature=table.temperature,
