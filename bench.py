@@ -170,6 +170,23 @@ class ClockSampler:
                 "samples": len(rows), "window": "samples bracketing the timed region"}
 
 
+def reduce_max_over_ranks(values, world, device=None):
+    """Max over ranks of each value (per-rank device times); identity at N=1.
+    Every rank must call it, in the same order."""
+    import torch
+    t = torch.tensor(list(values), dtype=torch.float64, device=device)
+    if world > 1:
+        import torch.distributed as dist
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return [float(v) for v in t.tolist()]
+
+
+def replica_throughput(points, steps, world, max_ms):
+    """Whole-job grid-point steps/s of `world` independent replicas of one
+    solve, timed by the slowest rank."""
+    return world * points * steps / (max_ms * 1e-3)
+
+
 def cpu_threads():
     from oracle import oracle as O
     return O.num_threads()
@@ -503,14 +520,12 @@ def run_ours(args, rank, world, local_rank):
     e2e_st.close()
 
     # ---- max over ranks -----------------------------------------------------
-    t = torch.tensor([total_ms, e2e_ms, resident_ms], dtype=torch.float64, device=dev)
-    if world > 1:
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    total_ms, e2e_ms, resident_ms = (float(v) for v in t.tolist())
+    total_ms, e2e_ms, resident_ms = reduce_max_over_ranks([total_ms, e2e_ms, resident_ms], world,
+                                                          device=dev)
     if rank != 0:
         return
 
-    value = world * P * args.steps / (total_ms * 1e-3)
+    value = replica_throughput(P, args.steps, world, total_ms)
     peak, peak_kind = measured_peak()
     per_rate = RATE_BYTES_FP32C if fp32c else RATE_BYTES_FP64
     per_step = STEP_BYTES_FP32C if fp32c else STEP_BYTES_FP64
