@@ -150,7 +150,7 @@ struct BatchSmem {
 
 template <int TX, int TY, int MINB, bool WIN, bool SORT = false>
 __global__ void __launch_bounds__(TX * TY, MINB)
-    kb_rate(const BSolve *__restrict__ solves, int nsolves, int total_tiles) {
+    kb_rate(const BSolve *__restrict__ solves, int nsolves, int total_tiles, double *tile_max) {
   constexpr int NT = TX * TY;
   extern __shared__ float4 sm4[];
   Rate32 *Rs = reinterpret_cast<Rate32 *>(sm4);
@@ -178,7 +178,7 @@ __global__ void __launch_bounds__(TX * TY, MINB)
     if (flags) atomicOr(&P.st->flags, flags);
     double *red = reinterpret_cast<double *>(work);    // free after the body's last barrier
     __syncthreads();
-    finish_tiles32(P, vmax, red, (unsigned)B.ntiles);
+    finish_slot32(vmax, red, tile_max + t);
   }
 }
 
@@ -365,12 +365,23 @@ __global__ void kb_bmul(cufftComplex *__restrict__ k, const float *__restrict__ 
 // ------------------------------------------------------------------------
 // Host side
 // ------------------------------------------------------------------------
+// The dt controllers of all solves after a rate launch: one warp per solve
+// reduces its tiles' maxima and advances its dt / time / step.
+__global__ void kb_dt(const BSolve *__restrict__ solves, int nsolves, const double *tile_max) {
+  const int i = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+  if (i >= nsolves) return;
+  const BSolve &B = solves[i];
+  if (B.R.st->halt) return;
+  dt_from_slots32(B.R, tile_max + B.tile0, B.ntiles);
+}
+
 struct BatchVariant {
   int tx, ty, minb;
   bool win;
   size_t smem;
   void (*set_attrs)();
-  void (*launch)(int grid, cudaStream_t s, const BSolve *solves, int n, int tiles);
+  void (*launch)(int grid, cudaStream_t s, const BSolve *solves, int n, int tiles,
+                 double *tile_max);
   int (*occupancy)();
 };
 
@@ -387,8 +398,10 @@ BatchVariant make_bvariant() {
     cudaFuncSetAttribute(kb_rate<TX, TY, MINB, WIN, SORT>,
                          cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SM::rate);
   };
-  v.launch = [](int grid, cudaStream_t s, const BSolve *solves, int n, int tiles) {
-    kb_rate<TX, TY, MINB, WIN, SORT><<<grid, dim3(TX, TY), SM::rate, s>>>(solves, n, tiles);
+  v.launch = [](int grid, cudaStream_t s, const BSolve *solves, int n, int tiles,
+                double *tile_max) {
+    kb_rate<TX, TY, MINB, WIN, SORT><<<grid, dim3(TX, TY), SM::rate, s>>>(solves, n, tiles,
+                                                                          tile_max);
   };
   v.occupancy = []() {
     int nb = 0;
@@ -436,6 +449,7 @@ struct pf5d_batch {
   int total_tiles = 0, total_chunks = 0;
   int variant = 0, rate_grid = 1, upd_grid = 1;
   cudaStream_t cap = nullptr;
+  double *tile_max = nullptr;       // per-tile max |dX/dt| of the last rate launch
   // Shape groups' FFT chains run as parallel branches of the step graph:
   // forked from the capture stream onto `aux`, joined back before the rate
   // kernel.  `order` lists the groups largest first, dealt round-robin.
@@ -448,6 +462,17 @@ struct pf5d_batch {
 };
 
 namespace {
+
+// Tiles of all solves under `variant` (configure_batch's tiling).
+int batch_tiles_of(const pf5d_batch *h, int variant) {
+  const BatchVariant &v = batch_variants()[variant];
+  const int nt = v.tx * v.ty;
+  int tiles = 0;
+  for (const auto &b : h->solves)
+    tiles += b.dim == 2 ? ((b.R.nx + v.tx - 1) / v.tx) * ((b.R.ny + v.ty - 1) / v.ty)
+                        : (b.R.nx + nt - 1) / nt;
+  return tiles;
+}
 
 pf5d_status configure_batch(pf5d_batch *h, int variant) {
   const auto &vars = batch_variants();
@@ -507,7 +532,10 @@ pf5d_status enqueue_batch_step(pf5d_batch *h, cudaStream_t s) {
     PF5D_CUDA(cudaStreamWaitEvent(s, h->join[a], 0));
   }
   batch_variants()[h->variant].launch(h->rate_grid, s, h->d_solves, (int)h->solves.size(),
-                                      h->total_tiles);
+                                      h->total_tiles, h->tile_max);
+  PF5D_LAUNCHED();
+  kb_dt<<<(unsigned)((h->solves.size() + 7) / 8), 256, 0, s>>>(h->d_solves, (int)h->solves.size(),
+                                                                h->tile_max);
   PF5D_LAUNCHED();
   kb_update<<<h->upd_grid, kUpdThreads, 0, s>>>(h->d_solves, (int)h->solves.size(),
                                                 h->total_chunks);
@@ -755,6 +783,13 @@ pf5d_status pf5d_batch_create(const pf5d_batch_solve *solves, int32_t nsolves,
     set_error("state upload failed");
     return fail(PF5D_ERR_CUDA);
   }
+  int max_tiles = 1;
+  for (int v = 0; v < (int)batch_variants().size(); ++v)
+    max_tiles = std::max(max_tiles, batch_tiles_of(h, v));
+  if (cudaMalloc(&h->tile_max, (size_t)max_tiles * sizeof(double)) != cudaSuccess) {
+    set_error("device allocation failed");
+    return fail(PF5D_ERR_CUDA);
+  }
   pf5d_status st = configure_batch(h, 0);
   if (st != PF5D_OK) return fail(st);
   for (int i = 0; i < nsolves; ++i) {
@@ -852,11 +887,11 @@ pf5d_status pf5d_batch_autotune(pf5d_batch *h, int32_t *variant, float *best_ms,
   float best_t = 1e30f;
   for (int v = 0; v < (int)batch_variants().size(); ++v) {
     if (configure_batch(h, v) != PF5D_OK) continue;
-    batch_variants()[v].launch(h->rate_grid, s, h->d_solves, (int)n, h->total_tiles);
+    batch_variants()[v].launch(h->rate_grid, s, h->d_solves, (int)n, h->total_tiles, h->tile_max);
     if (cudaGetLastError() != cudaSuccess) continue;
     PF5D_CUDA(cudaEventRecord(e0, s));
     for (int r = 0; r < 3; ++r)
-      batch_variants()[v].launch(h->rate_grid, s, h->d_solves, (int)n, h->total_tiles);
+      batch_variants()[v].launch(h->rate_grid, s, h->d_solves, (int)n, h->total_tiles, h->tile_max);
     PF5D_CUDA(cudaEventRecord(e1, s));
     PF5D_CUDA(cudaEventSynchronize(e1));
     float ms = 0.f;
@@ -894,6 +929,7 @@ pf5d_status pf5d_batch_destroy(pf5d_batch *h) {
   cudaFree(h->spart);
   cudaFree(h->st);
   cudaFree(h->d_solves);
+  cudaFree(h->tile_max);
   if (h->cap) cudaStreamDestroy(h->cap);
   for (auto as : h->aux) cudaStreamDestroy(as);
   for (auto ev : h->join) cudaEventDestroy(ev);

@@ -54,6 +54,7 @@ struct Rate32 {
   double ctld, t_cfl, lower, upper, factor;
   int adaptive;
   StepState32 *st;
+  double *partial;     // block maxima of |dX/dt| of the last rate launch
 };
 
 // ------------------------------------------------------------------------
@@ -181,11 +182,10 @@ __device__ __forceinline__ void face_flux32(const Rate32 &P, const float Dc[S], 
   for (int a = 0; a < S; ++a) J[a] = w_fe * xm[a] * dot + xm[a] * mm[1 + a] * dk[a] - xm[a] * swk;
 }
 
-// Fold this thread's max |dX/dt| into the block and the solve's device
-// accumulator; the block completing the solve's `total` tiles runs the FP64
-// dt controller and advances dt / time / step.
-__device__ __forceinline__ void finish_tiles32(const Rate32 &P, float m32, double *red,
-                                               unsigned total) {
+// Fold this thread's max |dX/dt| into the block and store the block's max
+// in `slot` (a plain store: no same-address atomics, no fences); a separate
+// one-block kernel reduces the slots and runs the FP64 dt controller.
+__device__ __forceinline__ void finish_slot32(float m32, double *red, double *slot) {
   double m = (double)m32;
 #pragma unroll
   for (int o = 16; o > 0; o >>= 1) m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
@@ -196,27 +196,31 @@ __device__ __forceinline__ void finish_tiles32(const Rate32 &P, float m32, doubl
   __syncthreads();
   if (tid == 0) {
     for (int w = 1; w < nw; ++w) m = fmax(m, red[w]);
-    StepState32 *st = P.st;
-    atomic_max_nonneg(&st->xacc, m);
-    __threadfence();
-    if (atomicAdd(&st->blocks_done, 1u) == total - 1) {
-      __threadfence();
-      const double xmax = __longlong_as_double(
-          (long long)atomicAdd(reinterpret_cast<unsigned long long *>(&st->xacc), 0ULL));
-      double dt = st->dt;
-      if (P.adaptive) dt = adaptive_dt(dt, xmax, P.ctld, P.t_cfl, P.lower, P.upper, P.factor);
-      st->dt = dt;
-      st->time = st->time + dt;
-      st->xdotmax = xmax;
-      st->step = st->step + 1;
-      st->xacc = 0.0;
-      st->blocks_done = 0;
-    }
+    *slot = m;
   }
 }
 
 __device__ __forceinline__ void finish_rate32(const Rate32 &P, float m32, double *red) {
-  finish_tiles32(P, m32, red, gridDim.x * gridDim.y * gridDim.z);
+  finish_slot32(m32, red, P.partial + (blockIdx.z * gridDim.y + blockIdx.y) * gridDim.x + blockIdx.x);
+}
+
+// The dt controller of one solve from the block maxima slots[0..n): max
+// |dX/dt|, the adaptive-dt rule (system.py:90-112), dt / time / step.  Called
+// by one warp; lane 0 writes the state.
+__device__ __forceinline__ void dt_from_slots32(const Rate32 &P, const double *slots, int n) {
+  StepState32 *st = P.st;
+  double m = 0.0;
+  for (int i = threadIdx.x & 31; i < n; i += 32) m = fmax(m, slots[i]);
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
+  if ((threadIdx.x & 31) == 0) {
+    double dt = st->dt;
+    if (P.adaptive) dt = adaptive_dt(dt, m, P.ctld, P.t_cfl, P.lower, P.upper, P.factor);
+    st->dt = dt;
+    st->time = st->time + dt;
+    st->xdotmax = m;
+    st->step = st->step + 1;
+  }
 }
 
 template <int PX, int PM>

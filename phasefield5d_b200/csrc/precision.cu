@@ -352,6 +352,30 @@ __global__ void k32_mass_final(const double *partial, int nparts, double *out) {
   }
 }
 
+// The dt controller after a rate launch of `nparts` blocks: a block-wide
+// max over the slots, then the FP64 rule in thread 0.
+constexpr int kDt32Threads = 1024;
+__global__ void __launch_bounds__(kDt32Threads) k32_dt(Rate32 P, int nparts) {
+  __shared__ double red[kDt32Threads / 32];
+  StepState32 *st = P.st;
+  if (st->halt) return;
+  double m = 0.0;
+  for (int i = threadIdx.x; i < nparts; i += kDt32Threads) m = fmax(m, P.partial[i]);
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = m;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    for (int w = 1; w < kDt32Threads / 32; ++w) m = fmax(m, red[w]);
+    double dt = st->dt;
+    if (P.adaptive) dt = adaptive_dt(dt, m, P.ctld, P.t_cfl, P.lower, P.upper, P.factor);
+    st->dt = dt;
+    st->time = st->time + dt;
+    st->xdotmax = m;
+    st->step = st->step + 1;
+  }
+}
+
 __global__ void k32_bmul(cufftComplex *__restrict__ k, const float *__restrict__ bk, int64_t nk,
                          const unsigned *halt) {
   if (halt && *halt) return;
@@ -423,6 +447,7 @@ struct Stepper32 {
   cufftHandle fwd = 0, inv = 0;
   bool plans = false;
   double *mass_ws = nullptr;
+  double *partial = nullptr;     // rate kernel block maxima
   StepState32 *st = nullptr;
   Rate32 rp{};
   Update32 up{};
@@ -443,11 +468,39 @@ struct Stepper32 {
     }                                                                              \
   } while (0)
 
-static pf5d_status configure32(Stepper32 *h, int variant) {
+// Grid of the rate kernel of `variant` (and the 3D axis-0 chunk).
+static dim3 grid32_of(const Stepper32 *h, int variant, int *zc_out) {
   const Rate32 &P = h->rp;
+  *zc_out = 1;
+  if (h->d.dim == 1) return dim3((unsigned)((P.nx + kTX1_32 - 1) / kTX1_32));
+  const Variant32 &v = variants32()[variant];
+  const unsigned gx = (unsigned)((P.nx + v.tx - 1) / v.tx), gy = (unsigned)((P.ny + v.ty - 1) / v.ty);
+  if (h->d.dim == 2) return dim3(gx, gy, 1);
+  const int64_t tiles = (int64_t)gx * gy;
+  const int64_t target = (int64_t)sm_count() * v.minb * 4;
+  int64_t zc = (tiles * P.nz + target - 1) / target;
+  zc = std::max<int64_t>(4, std::min<int64_t>(zc, 64));
+  zc = std::min<int64_t>(zc, P.nz);
+  *zc_out = (int)zc;
+  return dim3(gx, gy, (unsigned)((P.nz + zc - 1) / zc));
+}
+
+// Block slots needed by the largest rate grid over all variants.
+static int64_t max_blocks32(const Stepper32 *h) {
+  int64_t m = 1;
+  const int nv = h->d.dim == 1 ? 1 : (int)variants32().size();
+  for (int v = 0; v < nv; ++v) {
+    int zc = 1;
+    const dim3 g = grid32_of(h, v, &zc);
+    m = std::max<int64_t>(m, (int64_t)g.x * g.y * g.z);
+  }
+  return m;
+}
+
+static pf5d_status configure32(Stepper32 *h, int variant) {
   if (h->d.dim == 1) {
     h->block = dim3(kTX1_32);
-    h->grid = dim3((unsigned)((P.nx + kTX1_32 - 1) / kTX1_32));
+    h->grid = grid32_of(h, 0, &h->zc);
     h->smem = 0;
     return PF5D_OK;
   }
@@ -459,20 +512,8 @@ static pf5d_status configure32(Stepper32 *h, int variant) {
   v.set_attrs();
   PF5D_LAUNCHED();
   h->block = dim3(v.tx, v.ty);
-  const unsigned gx = (unsigned)((P.nx + v.tx - 1) / v.tx), gy = (unsigned)((P.ny + v.ty - 1) / v.ty);
-  if (h->d.dim == 2) {
-    h->smem = v.smem2d;
-    h->grid = dim3(gx, gy, 1);
-    return PF5D_OK;
-  }
-  h->smem = v.smem3d;
-  const int64_t tiles = (int64_t)gx * gy;
-  const int64_t target = (int64_t)sm_count() * v.minb * 4;
-  int64_t zc = (tiles * P.nz + target - 1) / target;
-  zc = std::max<int64_t>(4, std::min<int64_t>(zc, 64));
-  zc = std::min<int64_t>(zc, P.nz);
-  h->zc = (int)zc;
-  h->grid = dim3(gx, gy, (unsigned)((P.nz + zc - 1) / zc));
+  h->smem = h->d.dim == 2 ? v.smem2d : v.smem3d;
+  h->grid = grid32_of(h, variant, &h->zc);
   return PF5D_OK;
 }
 
@@ -482,6 +523,8 @@ static pf5d_status launch_rate32(Stepper32 *h, cudaStream_t s) {
     case 2: variants32()[h->variant].launch2d(h->grid, h->block, h->smem, s, h->rp); break;
     default: variants32()[h->variant].launch3d(h->grid, h->block, h->smem, s, h->rp, h->zc);
   }
+  PF5D_LAUNCHED();
+  k32_dt<<<1, kDt32Threads, 0, s>>>(h->rp, (int)(h->grid.x * h->grid.y * h->grid.z));
   PF5D_LAUNCHED();
   return PF5D_OK;
 }
@@ -628,6 +671,11 @@ pf5d_status s32_create(const pf5d_stepper_desc *desc, const double *X_init, void
   P.factor = desc->max_change_factor;
   P.adaptive = desc->adaptive;
   P.st = h->st;
+  if (cudaMalloc(&h->partial, (size_t)max_blocks32(h) * sizeof(double)) != cudaSuccess) {
+    set_error("device allocation failed");
+    return fail(PF5D_ERR_CUDA);
+  }
+  P.partial = h->partial;
   Update32 &U = h->up;
   U.hi = h->hi;
   U.lo = h->lo;
@@ -811,6 +859,7 @@ void s32_destroy(Stepper32 *h) {
   cudaFree(h->k);
   cudaFree(h->st);
   cudaFree(h->mass_ws);
+  cudaFree(h->partial);
   if (h->cap) cudaStreamDestroy(h->cap);
   delete h;
 }

@@ -63,6 +63,7 @@ struct RateParams {
   StepState *st;
   double *mm;                  // split rate: mu_1..4, M_Fe, M_1..4 per point, SoA [NP][npts]
   int64_t npts;
+  double *partial;             // per-block max |dX/dt| of the last rate launch
 };
 
 // ------------------------------------------------------------------------
@@ -390,8 +391,9 @@ __global__ void __launch_bounds__(256, MINB) k_chem64(RateParams P) {
   if (flags) atomicOr(&P.st->flags, flags);
 }
 
-// Fold this thread's max |dX/dt| into the block, then into the device
-// accumulator; the last block of the launch runs the dt controller.
+// Fold this thread's max |dX/dt| into the block and store the block's max
+// in its own slot of P.partial (a plain store: no same-address atomics, no
+// fences); k_dt_finish reduces the slots and runs the dt controller.
 __device__ __forceinline__ void finish_rate(const RateParams &P, double m, double *red) {
 #pragma unroll
   for (int o = 16; o > 0; o >>= 1) m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
@@ -402,24 +404,32 @@ __device__ __forceinline__ void finish_rate(const RateParams &P, double m, doubl
   __syncthreads();
   if (tid == 0) {
     for (int w = 1; w < nw; ++w) m = fmax(m, red[w]);
-    StepState *st = P.st;
-    atomic_max_nonneg(&st->xacc, m);
-    __threadfence();
-    const unsigned total = gridDim.x * gridDim.y * gridDim.z;
-    const unsigned prev = atomicAdd(&st->blocks_done, 1u);
-    if (prev == total - 1) {
-      __threadfence();
-      const double xmax = __longlong_as_double(
-          (long long)atomicAdd(reinterpret_cast<unsigned long long *>(&st->xacc), 0ULL));
-      double dt = st->dt;
-      if (P.adaptive) dt = adaptive_dt(dt, xmax, P.ctld, P.t_cfl, P.lower, P.upper, P.factor);
-      st->dt = dt;
-      st->time = st->time + dt;
-      st->xdotmax = xmax;
-      st->step = st->step + 1;
-      st->xacc = 0.0;
-      st->blocks_done = 0;
-    }
+    P.partial[(blockIdx.z * gridDim.y + blockIdx.y) * gridDim.x + blockIdx.x] = m;
+  }
+}
+
+// After a rate launch of `nparts` blocks: max |dX/dt| over the block slots,
+// then the adaptive-dt rule (system.py:90-112) and dt / time / step on the
+// device.  One block.
+constexpr int kDtThreads = 1024;
+__global__ void __launch_bounds__(kDtThreads) k_dt_finish(RateParams P, int nparts) {
+  __shared__ double red[kDtThreads / 32];
+  StepState *st = P.st;
+  if (st->halt) return;
+  double m = 0.0;
+  for (int i = threadIdx.x; i < nparts; i += kDtThreads) m = fmax(m, P.partial[i]);
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = m;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    for (int w = 1; w < kDtThreads / 32; ++w) m = fmax(m, red[w]);
+    double dt = st->dt;
+    if (P.adaptive) dt = adaptive_dt(dt, m, P.ctld, P.t_cfl, P.lower, P.upper, P.factor);
+    st->dt = dt;
+    st->time = st->time + dt;
+    st->xdotmax = m;
+    st->step = st->step + 1;
   }
 }
 
@@ -967,6 +977,7 @@ struct pf5d_stepper {
   double *mass_ws = nullptr;     // FP64 mean reduction workspace
   double *mm = nullptr;          // split-rate mu/M buffer (also save-step diagnostics)
   double *diag_ws = nullptr;     // save-step partial rows + mean
+  double *partial = nullptr;     // rate kernel block maxima
 };
 
 namespace {
@@ -1078,14 +1089,44 @@ const std::vector<RateVariant> &rate_variants() {
   return v;
 }
 
+// Grid of the rate kernel of `variant` on this solve (and the axis-0 chunk
+// of the 3D marching kernel).
+dim3 rate_grid_of(const pf5d_stepper *h, int variant, int *zc_out) {
+  const RateParams &P = h->rp;
+  *zc_out = 1;
+  if (h->d.dim == 1) return dim3((unsigned)((P.nx + kTX1 - 1) / kTX1));
+  const RateVariant &v = rate_variants()[variant];
+  const unsigned gx = (unsigned)((P.nx + v.tx - 1) / v.tx), gy = (unsigned)((P.ny + v.ty - 1) / v.ty);
+  if (h->d.dim == 2) return dim3(gx, gy, 1);
+  // Chunk of axis-0 planes per block: ~8 resident-block waves, >= 4 planes.
+  const int64_t tiles = (int64_t)gx * gy;
+  const int64_t target = (int64_t)sm_count() * v.minb * 4;
+  int64_t zc = (tiles * P.nz + target - 1) / target;
+  zc = std::max<int64_t>(4, std::min<int64_t>(zc, 64));
+  zc = std::min<int64_t>(zc, P.nz);
+  *zc_out = (int)zc;
+  return dim3(gx, gy, (unsigned)((P.nz + zc - 1) / zc));
+}
+
+// Block slots needed by the largest rate grid over all variants.
+int64_t max_rate_blocks(const pf5d_stepper *h) {
+  int64_t m = 1;
+  const int nv = h->d.dim == 1 ? 1 : (int)rate_variants().size();
+  for (int v = 0; v < nv; ++v) {
+    int zc = 1;
+    const dim3 g = rate_grid_of(h, v, &zc);
+    m = std::max<int64_t>(m, (int64_t)g.x * g.y * g.z);
+  }
+  return m;
+}
+
 pf5d_status configure_rate(pf5d_stepper *h, int variant) {
   const int dim = h->d.dim;
-  const int nsm = sm_count();
   const RateParams &P = h->rp;
   h->vec = (P.T.stride % 2 == 0) && (((uintptr_t)P.T.grid & 15) == 0);
   if (dim == 1) {
     h->rate_block = dim3(kTX1);
-    h->rate_grid = dim3((unsigned)((P.nx + kTX1 - 1) / kTX1));
+    h->rate_grid = rate_grid_of(h, 0, &h->zc);
     h->rate_smem = 0;
     return PF5D_OK;
   }
@@ -1098,21 +1139,8 @@ pf5d_status configure_rate(pf5d_stepper *h, int variant) {
   PF5D_LAUNCHED();
   h->rate_block = dim3(v.tx, v.ty);
   if (dim == 2) h->rate_block = dim3(v.nth);
-  const unsigned gx = (unsigned)((P.nx + v.tx - 1) / v.tx), gy = (unsigned)((P.ny + v.ty - 1) / v.ty);
-  if (dim == 2) {
-    h->rate_smem = v.smem2d;
-    h->rate_grid = dim3(gx, gy, 1);
-    return PF5D_OK;
-  }
-  h->rate_smem = v.smem3d;
-  // Chunk of axis-0 planes per block: ~8 resident-block waves, >= 4 planes.
-  const int64_t tiles = (int64_t)gx * gy;
-  const int64_t target = (int64_t)nsm * v.minb * 4;
-  int64_t zc = (tiles * P.nz + target - 1) / target;
-  zc = std::max<int64_t>(4, std::min<int64_t>(zc, 64));
-  zc = std::min<int64_t>(zc, P.nz);
-  h->zc = (int)zc;
-  h->rate_grid = dim3(gx, gy, (unsigned)((P.nz + zc - 1) / zc));
+  h->rate_smem = dim == 2 ? v.smem2d : v.smem3d;
+  h->rate_grid = rate_grid_of(h, variant, &h->zc);
   return PF5D_OK;
 }
 
@@ -1130,6 +1158,8 @@ pf5d_status launch_rate(pf5d_stepper *h, cudaStream_t s) {
     default:
       rate_variants()[h->variant].launch3d(h->vec, g, b, sm, s, h->rp, h->zc);
   }
+  PF5D_LAUNCHED();
+  k_dt_finish<<<1, kDtThreads, 0, s>>>(h->rp, (int)(g.x * g.y * g.z));
   PF5D_LAUNCHED();
   return PF5D_OK;
 }
@@ -1327,6 +1357,11 @@ pf5d_status pf5d_stepper_create(const pf5d_stepper_desc *desc, double *X, void *
   P.st = h->st;
   P.mm = h->mm;
   P.npts = npts;
+  if (cudaMalloc(&h->partial, (size_t)max_rate_blocks(h) * sizeof(double)) != cudaSuccess) {
+    set_error("device allocation failed");
+    return fail(PF5D_ERR_CUDA);
+  }
+  P.partial = h->partial;
   UpdateParams &U = h->up;
   U.X = X;
   U.dX = h->dX;
@@ -1594,6 +1629,7 @@ pf5d_status pf5d_stepper_destroy(pf5d_stepper *h) {
   cudaFree(h->mass_ws);
   cudaFree(h->mm);
   cudaFree(h->diag_ws);
+  cudaFree(h->partial);
   for (auto &kv : h->graphs) cudaGraphExecDestroy(kv.second);
   fft_destroy(&h->fft);
   cudaFree(h->dX);
