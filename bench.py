@@ -452,6 +452,7 @@ def run_ours(args, rank, world, local_rank):
     clock_info = clocks.stop()
     step_ms = [e0.elapsed_time(e1) for e0, e1 in ev]
     total_ms = sum(step_ms)
+    launches_per_step = st.launches_per_step
     state = st.state()
     if state["halted"]:
         raise RuntimeError(f"stepper halted during the benchmark: {state}")
@@ -569,7 +570,7 @@ def run_ours(args, rank, world, local_rank):
                 "d2h_bytes_per_step": int(host.numel() * 8),
                 "path": "pinned host X -> H2D -> pf5d_stepper_advance(1) -> D2H, per step"},
         "clocks": clock_info,
-        "gpu_launches": args.steps * (3 if prob.lvec is not None else 2),
+        "gpu_launches": args.steps * launches_per_step,
         "state_after": {"step": state["step"], "dt": state["dt"], "time": state["time"]},
     }
     if fp32c and args.accuracy_steps > 0:

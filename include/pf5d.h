@@ -261,6 +261,10 @@ pf5d_status pf5d_stepper_step_save(pf5d_stepper *h, pf5d_save_diag *out, void *s
 /* Number of rate-kernel variants of this stepper's form (valid indices for
  * pf5d_stepper_set_variant are 0 .. count-1); 0 for a null stepper. */
 int32_t pf5d_stepper_variant_count(const pf5d_stepper *h);
+/* Kernels of this library that one step launches with the current variant
+ * (rate kernel(s), dt controller, update, and the B(k) multiply when
+ * elasticity is on; cuFFT's own kernels not counted); 0 for a null stepper. */
+int32_t pf5d_stepper_launches_per_step(const pf5d_stepper *h);
 /* Re-derive internal state after the caller modified X (e.g. a restart). */
 pf5d_status pf5d_stepper_reset(pf5d_stepper *h, double dt, double time, void *stream);
 pf5d_status pf5d_stepper_destroy(pf5d_stepper *h);

@@ -113,6 +113,7 @@ _SIGS = {
                                      _vp]),
     "pf5d_stepper_set_variant": (_i32, [_vp, _i32]),
     "pf5d_stepper_variant_count": (_i32, [_vp]),
+    "pf5d_stepper_launches_per_step": (_i32, [_vp]),
     "pf5d_stepper_step_save": (_i32, [_vp, ctypes.POINTER(SaveDiag), _vp]),
     "pf5d_batch_variant_count": (_i32, []),
     "pf5d_stepper_reset": (_i32, [_vp, _f64, _f64, _vp]),

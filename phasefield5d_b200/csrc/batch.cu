@@ -97,7 +97,8 @@ __device__ __forceinline__ float tile1d32_body(const BSolve &B, const Rate32 &P,
 #pragma unroll
     for (int c = 0; c < S; ++c) {
       d[c] = Xs[c * HX + px];
-      lap[c] = (Xs[c * HX + px + 1] + Xs[c * HX + px - 1] - 2.f * d[c]) * P.inv_dx2;
+      const float nb[2] = {Xs[c * HX + px + 1], Xs[c * HX + px - 1]};
+      lap[c] = lap32<2>(nb, d[c], P.inv_dx2);
     }
     float spv = 0.f;
     if (B.emode == 1)

@@ -55,11 +55,25 @@ struct Rate32 {
   int adaptive;
   StepState32 *st;
   double *partial;     // block maxima of |dX/dt| of the last rate launch
+  float *mm;           // split rate: mu_1..4, M_Fe, M_1..4 per point, SoA [NP][npts]
+  int64_t npts;
 };
 
 // ------------------------------------------------------------------------
 // Device numerics
 // ------------------------------------------------------------------------
+
+// FP32 Laplacian of one component: the N neighbour values in the
+// reference's order (+axis0, -axis0, +axis1, ...), minus N * centre, times
+// 1/dx^2 (operators.py:33-76).  Every operation is separately rounded, so
+// the fused, split and batched kernels agree bit for bit.
+template <int N>
+__device__ __forceinline__ float lap32(const float nb[N], float c, float inv_dx2) {
+  float sum = nb[0];
+#pragma unroll
+  for (int i = 1; i < N; ++i) sum = __fadd_rn(sum, nb[i]);
+  return __fmul_rn(__fsub_rn(sum, __fmul_rn((float)N, c)), inv_dx2);
+}
 
 // Table cell and fractional coordinates of X = X0 + d (interpolation.py:103-121
 // clamping).  Returns false when the point is outside the linear region
@@ -384,11 +398,14 @@ __device__ __forceinline__ void mu_plane32(const Rate32 &P, const float *Xm, con
     for (int c = 0; c < S; ++c) {
       const float *q = Xc + c * G::PX;
       d[c] = q[px];
-      if (DIM == 3)
-        lap[c] = (Xp[c * G::PX + px] + Xm[c * G::PX + px] + q[px + G::HX] + q[px - G::HX] +
-                  q[px + 1] + q[px - 1] - 6.f * d[c]) * P.inv_dx2;
-      else
-        lap[c] = (q[px + G::HX] + q[px - G::HX] + q[px + 1] + q[px - 1] - 4.f * d[c]) * P.inv_dx2;
+      if (DIM == 3) {
+        const float nb[6] = {Xp[c * G::PX + px], Xm[c * G::PX + px], q[px + G::HX], q[px - G::HX],
+                             q[px + 1], q[px - 1]};
+        lap[c] = lap32<6>(nb, d[c], P.inv_dx2);
+      } else {
+        const float nb[4] = {q[px + G::HX], q[px - G::HX], q[px + 1], q[px - 1]};
+        lap[c] = lap32<4>(nb, d[c], P.inv_dx2);
+      }
     }
     const float spv = P.sp ? __ldg(P.sp + zoff + (int64_t)wy[my + 1] * P.nx + wx[mx + 1]) : 0.f;
     float mu[S], M[NM];
@@ -397,6 +414,22 @@ __device__ __forceinline__ void mu_plane32(const Rate32 &P, const float *Xm, con
     for (int c = 0; c < S; ++c) dst[c * G::PM + pos] = mu[c];
 #pragma unroll
     for (int c = 0; c < NM; ++c) dst[(S + c) * G::PM + pos] = M[c];
+  }
+}
+
+// mu/M of one plane (tile + 1-cell halo, or the tile only) read from the
+// split buffer P.mm (written by k32_chem) into dst, in mu_plane32's layout.
+template <int TX, int TY>
+__device__ __forceinline__ void load_mu_plane32(const Rate32 &P, int64_t zoff, const int *wx,
+                                                const int *wy, bool interior_only, float *dst,
+                                                int tid) {
+  using G = PlaneGeom<TX, TY>;
+  for (int pos = tid; pos < G::PM; pos += G::NT) {
+    const int my = pos / G::MX, mx = pos - my * G::MX;
+    if (skip_pos<G::MX, G::MY>(mx, my, interior_only)) continue;
+    const float *src = P.mm + zoff + (int64_t)wy[my + 1] * P.nx + wx[mx + 1];
+#pragma unroll
+    for (int c = 0; c < NP; ++c) dst[c * G::PM + pos] = __ldg(src + c * P.npts);
   }
 }
 
@@ -465,7 +498,7 @@ struct Tile2dSmem32 {
 
 // Evaluates tile (bx, by) of solve P and writes its dX/dt; returns this
 // thread's max |dX/dt|.  Ends with all threads past a barrier.
-template <int TX, int TY, bool WIN, bool SORT = false>
+template <int TX, int TY, bool WIN, bool SORT = false, bool SPLIT = false>
 __device__ __forceinline__ float tile2d32_body(const Rate32 &P, int bx, int by, float4 *sm4,
                                                unsigned *flags, int tid) {
   using G = PlaneGeom<TX, TY>;
@@ -491,8 +524,11 @@ __device__ __forceinline__ float tile2d32_body(const Rate32 &P, int bx, int by, 
   __syncthreads();
   load_plane32<TX, TY>(P.D, 0, wx, wy, P.nx, Xs, tid);
   __syncthreads();
-  mu_plane32<TX, TY, 2, WIN, SORT>(P, nullptr, Xs, nullptr, Ms, 0, wx, wy, false, win, wred,
-                                   win_lo, flags, tid, ss);
+  if constexpr (SPLIT)
+    load_mu_plane32<TX, TY>(P, 0, wx, wy, false, Ms, tid);
+  else
+    mu_plane32<TX, TY, 2, WIN, SORT>(P, nullptr, Xs, nullptr, Ms, 0, wx, wy, false, win, wred,
+                                     win_lo, flags, tid, ss);
   __syncthreads();
   plane_faces32<TX, TY>(P, Xs, Ms, Fx, Fy, tid);
   __syncthreads();

@@ -25,6 +25,7 @@ pf5d_status s32_mass(Stepper32 *h, double *mean_out, void *stream);
 pf5d_status s32_autotune(Stepper32 *h, int32_t *variant, float *best_ms, void *stream);
 pf5d_status s32_set_variant(Stepper32 *h, int32_t variant);
 int32_t s32_variant_count();
+int32_t s32_launches_per_step(const Stepper32 *h);
 pf5d_status s32_launch_stage(Stepper32 *h, int32_t stage, void *stream);
 pf5d_status s32_reset(Stepper32 *h, const double *X, double dt, double time, void *stream);
 float *s32_rate(Stepper32 *h);

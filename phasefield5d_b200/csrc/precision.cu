@@ -39,14 +39,14 @@ namespace pf5d {
 // Rate kernels (same tiling as the FP64 kernels)
 // ------------------------------------------------------------------------
 
-template <int TX, int TY, int MINB, bool WIN, bool SORT = false>
+template <int TX, int TY, int MINB, bool WIN, bool SORT = false, bool SPLIT = false>
 __global__ void __launch_bounds__(TX * TY, MINB) k32_rate_tile2d(Rate32 P) {
   if (P.st->halt) return;
   extern __shared__ float4 sm4[];
   const int tid = threadIdx.y * TX + threadIdx.x;
   unsigned flags = 0;
   const float vmax =
-      tile2d32_body<TX, TY, WIN, SORT>(P, blockIdx.x, blockIdx.y, sm4, &flags, tid);
+      tile2d32_body<TX, TY, WIN, SORT, SPLIT>(P, blockIdx.x, blockIdx.y, sm4, &flags, tid);
   if (flags) atomicOr(&P.st->flags, flags);
   finish_rate32(P, vmax, Tile2dSmem32<TX, TY, SORT>::red(sm4));
 }
@@ -56,7 +56,7 @@ constexpr size_t tile2d32_smem() {
   return Tile2dSmem32<TX, TY, SORT>::bytes;
 }
 
-template <int TX, int TY, int MINB, bool WIN, bool SORT = false>
+template <int TX, int TY, int MINB, bool WIN, bool SORT = false, bool SPLIT = false>
 __global__ void __launch_bounds__(TX * TY, MINB) k32_rate_march3d(Rate32 P, int zc) {
   using G = PlaneGeom<TX, TY>;
   if (P.st->halt) return;
@@ -90,23 +90,34 @@ __global__ void __launch_bounds__(TX * TY, MINB) k32_rate_march3d(Rate32 P, int 
     load_plane32<TX, TY>(P.D, (int64_t)wrap_any(z, P.nz) * plane, wx, wy, P.nx, xplane(z), tid);
   };
   auto compute_mu = [&](int z, bool interior_only) {
-    mu_plane32<TX, TY, 3, WIN, SORT>(P, xplane(z - 1), xplane(z), xplane(z + 1), mplane(z),
-                                     (int64_t)wrap_any(z, P.nz) * plane, wx, wy, interior_only,
-                                     win, wred, win_lo, &flags, tid, ss);
+    if constexpr (SPLIT)
+      load_mu_plane32<TX, TY>(P, (int64_t)wrap_any(z, P.nz) * plane, wx, wy, interior_only,
+                              mplane(z), tid);
+    else
+      mu_plane32<TX, TY, 3, WIN, SORT>(P, xplane(z - 1), xplane(z), xplane(z + 1), mplane(z),
+                                       (int64_t)wrap_any(z, P.nz) * plane, wx, wy, interior_only,
+                                       win, wred, win_lo, &flags, tid, ss);
   };
   const int pX = (ty + 2) * G::HX + (tx + 2);
   const int pM = (ty + 1) * G::MX + (tx + 1);
   const bool in_tile = (x0 + tx < P.nx) && (y0 + ty < P.ny);
   __syncthreads();
-  load_x(zb - 2);
-  load_x(zb - 1);
-  load_x(zb);
-  __syncthreads();
-  compute_mu(zb - 1, true);
-  __syncthreads();
-  load_x(zb + 1);
-  __syncthreads();
-  compute_mu(zb, false);
+  if constexpr (SPLIT) {          // faces need X and mu/M of planes z and z+1 only
+    load_x(zb - 1);
+    load_x(zb);
+    compute_mu(zb - 1, true);
+    compute_mu(zb, false);
+  } else {
+    load_x(zb - 2);
+    load_x(zb - 1);
+    load_x(zb);
+    __syncthreads();
+    compute_mu(zb - 1, true);
+    __syncthreads();
+    load_x(zb + 1);
+    __syncthreads();
+    compute_mu(zb, false);
+  }
   __syncthreads();
   float Jm[S];
   face32_between<G::PX, G::PM>(P, xplane(zb - 1), mplane(zb - 1), pX, pM, xplane(zb), mplane(zb),
@@ -114,9 +125,14 @@ __global__ void __launch_bounds__(TX * TY, MINB) k32_rate_march3d(Rate32 P, int 
   float vmax = 0.f;
   for (int z = zb; z < ze; ++z) {
     __syncthreads();
-    load_x(z + 2);
-    __syncthreads();
-    compute_mu(z + 1, false);
+    if constexpr (SPLIT) {
+      load_x(z + 1);
+      compute_mu(z + 1, false);
+    } else {
+      load_x(z + 2);
+      __syncthreads();
+      compute_mu(z + 1, false);
+    }
     __syncthreads();
     float Jz[S];
     face32_between<G::PX, G::PM>(P, xplane(z), mplane(z), pX, pM, xplane(z + 1), mplane(z + 1),
@@ -175,7 +191,8 @@ __global__ void __launch_bounds__(TX) k32_rate_1d(Rate32 P) {
 #pragma unroll
     for (int c = 0; c < S; ++c) {
       d[c] = Xs[c][px];
-      lap[c] = (Xs[c][px + 1] + Xs[c][px - 1] - 2.f * d[c]) * P.inv_dx2;
+      const float nb[2] = {Xs[c][px + 1], Xs[c][px - 1]};
+      lap[c] = lap32<2>(nb, d[c], P.inv_dx2);
     }
     const float spv = P.sp ? __ldg(P.sp + wrap_any(x0 + pos - 1, n)) : 0.f;
     float mu[S], M[NM];
@@ -352,6 +369,104 @@ __global__ void k32_mass_final(const double *partial, int nparts, double *out) {
   }
 }
 
+// Split rate evaluation, first kernel: mu/M at every point of a 2D/3D field
+// into P.mm, one point per thread, a 32 x 8 tile of a plane per block.  The
+// block orders its points by table cell (cell_hash counting sort) before
+// interpolating, so the lanes of a warp gather the same table nodes.  Same
+// Laplacian (lap32, neighbour order +axis0, -axis0, ...) and mu assembly
+// (chem32) as the fused kernels.
+template <int DIM, int MINB>
+__global__ void __launch_bounds__(256, MINB) k32_chem(Rate32 P) {
+  constexpr int NT = 256;
+  __shared__ float io[NP][NT];              // inputs (d, lap, s'), then outputs (mu, M)
+  __shared__ int hist[NT];
+  __shared__ int wsum[NT / 32 + 1];
+  __shared__ unsigned short order[NT];
+  if (P.st->halt) return;
+  const int tid = threadIdx.y * 32 + threadIdx.x;
+  const int x = blockIdx.x * 32 + threadIdx.x;
+  const int y = blockIdx.y * 8 + threadIdx.y;
+  const int z = blockIdx.z;
+  const bool valid = x < P.nx && y < P.ny;
+  const int64_t plane = (int64_t)P.ny * P.nx;
+  const int64_t zo = (int64_t)z * plane;
+  const int64_t g = zo + (int64_t)y * P.nx + x;
+  hist[tid] = 0;
+  int key = 0, rank = 0;
+  __syncthreads();
+  if (valid) {
+    auto ld = [&](int64_t gi, float v[S]) {
+      const float4 a = __ldg(P.D + gi);
+      v[0] = a.x; v[1] = a.y; v[2] = a.z; v[3] = a.w;
+    };
+    const int xp = x + 1 == P.nx ? 0 : x + 1, xm = x == 0 ? P.nx - 1 : x - 1;
+    const int yp = y + 1 == P.ny ? 0 : y + 1, ym = y == 0 ? P.ny - 1 : y - 1;
+    constexpr int NB = DIM == 3 ? 6 : 4;
+    float d[S], nb[NB][S];
+    ld(g, d);
+    int k = 0;
+    if (DIM == 3) {
+      const int zp = z + 1 == P.nz ? 0 : z + 1, zm = z == 0 ? P.nz - 1 : z - 1;
+      ld((int64_t)zp * plane + (int64_t)y * P.nx + x, nb[k++]);
+      ld((int64_t)zm * plane + (int64_t)y * P.nx + x, nb[k++]);
+    }
+    ld(zo + (int64_t)yp * P.nx + x, nb[k++]);
+    ld(zo + (int64_t)ym * P.nx + x, nb[k++]);
+    ld(zo + (int64_t)y * P.nx + xp, nb[k++]);
+    ld(zo + (int64_t)y * P.nx + xm, nb[k]);
+    float u[S];
+#pragma unroll
+    for (int c = 0; c < S; ++c) {
+      float n[NB];
+#pragma unroll
+      for (int i = 0; i < NB; ++i) n[i] = nb[i][c];
+      io[c][tid] = d[c];
+      io[S + c][tid] = lap32<NB>(n, d[c], P.inv_dx2);
+      u[c] = fmaf(d[c], P.T.inv_step_f, P.T.fb[c]) + (float)P.T.ib[c];
+    }
+    io[2 * S][tid] = P.sp ? __ldg(P.sp + g) : 0.f;
+    key = cell_hash_u(u);
+    rank = atomicAdd(&hist[key], 1);
+  }
+  __syncthreads();
+  const int count = block_exclusive_scan<NT, NT>(hist, wsum, tid);
+  if (valid) order[hist[key] + rank] = (unsigned short)tid;
+  __syncthreads();
+  unsigned flags = 0;
+  float mu[S], M[NM];
+  int q = -1;
+  if (tid < count) {
+    q = order[tid];
+    float dq[S], lq[S];
+#pragma unroll
+    for (int c = 0; c < S; ++c) {
+      dq[c] = io[c][q];
+      lq[c] = io[S + c][q];
+    }
+    const int o[S] = {0, 0, 0, 0};
+    chem32(P, dq, lq, io[2 * S][q], nullptr, o, mu, M, &flags);
+  }
+  __syncthreads();                          // all inputs read: io now takes the outputs
+  if (q >= 0) {
+#pragma unroll
+    for (int c = 0; c < S; ++c) io[c][q] = mu[c];
+#pragma unroll
+    for (int c = 0; c < NM; ++c) io[S + c][q] = M[c];
+  }
+  __syncthreads();
+  if (valid) {
+#pragma unroll
+    for (int c = 0; c < NP; ++c) P.mm[c * P.npts + g] = io[c][tid];
+  }
+  if (flags) atomicOr(&P.st->flags, flags);
+}
+
+template <int DIM, int KMINB>
+void launch_chem32(cudaStream_t s, const Rate32 &P) {
+  const dim3 b(32, 8), g((unsigned)((P.nx + 31) / 32), (unsigned)((P.ny + 7) / 8), (unsigned)P.nz);
+  k32_chem<DIM, KMINB><<<g, b, 0, s>>>(P);
+}
+
 // The dt controller after a rate launch of `nparts` blocks: a block-wide
 // max over the slots, then the FP64 rule in thread 0.
 constexpr int kDt32Threads = 1024;
@@ -397,6 +512,7 @@ constexpr int kGraphSteps32 = 50;
 
 struct Variant32 {
   int tx, ty, minb;
+  bool split;
   size_t smem2d, smem3d;
   void (*set_attrs)();
   void (*launch2d)(dim3, dim3, size_t, cudaStream_t, const Rate32 &);
@@ -409,6 +525,7 @@ Variant32 make_variant32() {
   v.tx = TX;
   v.ty = TY;
   v.minb = MINB;
+  v.split = false;
   v.smem2d = tile2d32_smem<TX, TY, SORT>();
   v.smem3d = march3d32_smem<TX, TY, SORT>();
   v.set_attrs = []() {
@@ -427,13 +544,44 @@ Variant32 make_variant32() {
   return v;
 }
 
+// Split variant: k32_chem over all points, then the tile / marching kernel
+// reading mu/M back.
+template <int TX, int TY, int MINB, int KMINB>
+Variant32 make_split_variant32() {
+  Variant32 v;
+  v.tx = TX;
+  v.ty = TY;
+  v.minb = MINB;
+  v.split = true;
+  v.smem2d = tile2d32_smem<TX, TY>();
+  v.smem3d = march3d32_smem<TX, TY>();
+  v.set_attrs = []() {
+    const auto a = cudaFuncAttributeMaxDynamicSharedMemorySize;
+    cudaFuncSetAttribute(k32_rate_tile2d<TX, TY, MINB, false, false, true>, a,
+                         (int)tile2d32_smem<TX, TY>());
+    cudaFuncSetAttribute(k32_rate_march3d<TX, TY, MINB, false, false, true>, a,
+                         (int)march3d32_smem<TX, TY>());
+  };
+  v.launch2d = [](dim3 g, dim3 b, size_t sm, cudaStream_t s, const Rate32 &P) {
+    launch_chem32<2, KMINB>(s, P);
+    k32_rate_tile2d<TX, TY, MINB, false, false, true><<<g, b, sm, s>>>(P);
+  };
+  v.launch3d = [](dim3 g, dim3 b, size_t sm, cudaStream_t s, const Rate32 &P, int zc) {
+    launch_chem32<3, KMINB>(s, P);
+    k32_rate_march3d<TX, TY, MINB, false, false, true><<<g, b, sm, s>>>(P, zc);
+  };
+  return v;
+}
+
 const std::vector<Variant32> &variants32() {
   static const std::vector<Variant32> v = {
       make_variant32<32, 8, 2>(), make_variant32<32, 8, 3>(), make_variant32<32, 8, 4>(),
       make_variant32<32, 4, 6>(), make_variant32<64, 4, 3>(), make_variant32<32, 16, 2>(),
       make_variant32<32, 8, 2, false>(), make_variant32<32, 16, 2, false>(),
       make_variant32<32, 8, 2, true, true>(), make_variant32<32, 8, 3, false, true>(),
-      make_variant32<32, 16, 2, false, true>(), make_variant32<32, 8, 2, false, true>()};
+      make_variant32<32, 16, 2, false, true>(), make_variant32<32, 8, 2, false, true>(),
+      make_split_variant32<32, 8, 3, 3>(), make_split_variant32<32, 16, 2, 3>(),
+      make_split_variant32<32, 8, 4, 4>(), make_split_variant32<32, 16, 2, 4>()};
   return v;
 }
 
@@ -448,6 +596,7 @@ struct Stepper32 {
   bool plans = false;
   double *mass_ws = nullptr;
   double *partial = nullptr;     // rate kernel block maxima
+  float *mm = nullptr;           // split-rate mu/M buffer (2D/3D)
   StepState32 *st = nullptr;
   Rate32 rp{};
   Update32 up{};
@@ -676,6 +825,14 @@ pf5d_status s32_create(const pf5d_stepper_desc *desc, const double *X_init, void
     return fail(PF5D_ERR_CUDA);
   }
   P.partial = h->partial;
+  P.npts = npts;
+  if (desc->dim >= 2) {
+    if (cudaMalloc(&h->mm, (size_t)npts * NP * sizeof(float)) != cudaSuccess) {
+      set_error("device allocation failed");
+      return fail(PF5D_ERR_CUDA);
+    }
+    P.mm = h->mm;
+  }
   Update32 &U = h->up;
   U.hi = h->hi;
   U.lo = h->lo;
@@ -760,6 +917,11 @@ pf5d_status s32_mass(Stepper32 *h, double *mean_out, void *stream) {
 }
 
 int32_t s32_variant_count() { return (int32_t)variants32().size(); }
+
+int32_t s32_launches_per_step(const Stepper32 *h) {
+  const bool split = h->d.dim >= 2 && variants32()[h->variant].split;
+  return (split ? 4 : 3) + (h->d.elastic ? 1 : 0);   // rate (+chem), dt, update (+ B(k))
+}
 
 pf5d_status s32_set_variant(Stepper32 *h, int32_t variant) {
   pf5d_status st = configure32(h, variant);
@@ -860,6 +1022,7 @@ void s32_destroy(Stepper32 *h) {
   cudaFree(h->st);
   cudaFree(h->mass_ws);
   cudaFree(h->partial);
+  cudaFree(h->mm);
   if (h->cap) cudaStreamDestroy(h->cap);
   delete h;
 }

@@ -1592,6 +1592,13 @@ pf5d_status pf5d_stepper_step_save(pf5d_stepper *h, pf5d_save_diag *out, void *s
   return PF5D_OK;
 }
 
+int32_t pf5d_stepper_launches_per_step(const pf5d_stepper *h) {
+  if (!h) return 0;
+  if (h->s32) return s32_launches_per_step(h->s32);
+  const bool split = h->d.dim >= 2 && rate_variants()[h->variant].split;
+  return (split ? 2 : 1) + 2 + (h->d.elastic ? 1 : 0);   // rate (+chem), dt, update, bmul
+}
+
 int32_t pf5d_stepper_variant_count(const pf5d_stepper *h) {
   if (!h) return 0;
   return h->s32 ? s32_variant_count() : (int32_t)rate_variants().size();

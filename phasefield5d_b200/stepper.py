@@ -165,6 +165,11 @@ class Stepper:
         return out
 
     @property
+    def launches_per_step(self):
+        """Kernels of this library one step launches (cuFFT's not counted)."""
+        return int(self.L.pf5d_stepper_launches_per_step(self.h))
+
+    @property
     def n_variants(self):
         """Number of rate-kernel variants the autotuner chooses from."""
         return int(self.L.pf5d_stepper_variant_count(self.h))
