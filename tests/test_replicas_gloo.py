@@ -35,7 +35,7 @@ def _rank(rank, world, port, results):
 @pytest.mark.timeout(180)
 def test_replicas_max_over_ranks_gloo():
     world = 2
-    with mp.Manager() as m:
+    with mp.get_context("spawn").Manager() as m:
         results = m.dict()
         mp.spawn(_rank, args=(world, _free_port(), results), nprocs=world, join=True)
         res = dict(results)
