@@ -24,6 +24,7 @@
 #include <map>
 #include <vector>
 
+#include <cuda_pipeline_primitives.h>
 #include <cufft.h>
 
 #include "pf5d_device.cuh"
@@ -378,7 +379,7 @@ __global__ void k32_mass_final(const double *partial, int nparts, double *out) {
 template <int DIM, int MINB>
 __global__ void __launch_bounds__(256, MINB) k32_chem(Rate32 P) {
   constexpr int NT = 256;
-  __shared__ float io[NP][NT];              // inputs (d, lap, s'), then outputs (mu, M)
+  __shared__ float io[2 * S + 1][NT];       // inputs of each point: d, lap, s'
   __shared__ int hist[NT];
   __shared__ int wsum[NT / 32 + 1];
   __shared__ unsigned short order[NT];
@@ -434,9 +435,8 @@ __global__ void __launch_bounds__(256, MINB) k32_chem(Rate32 P) {
   __syncthreads();
   unsigned flags = 0;
   float mu[S], M[NM];
-  int q = -1;
   if (tid < count) {
-    q = order[tid];
+    const int q = order[tid];
     float dq[S], lq[S];
 #pragma unroll
     for (int c = 0; c < S; ++c) {
@@ -445,20 +445,117 @@ __global__ void __launch_bounds__(256, MINB) k32_chem(Rate32 P) {
     }
     const int o[S] = {0, 0, 0, 0};
     chem32(P, dq, lq, io[2 * S][q], nullptr, o, mu, M, &flags);
-  }
-  __syncthreads();                          // all inputs read: io now takes the outputs
-  if (q >= 0) {
+    // point q of the tile: row q / 32, column q % 32
+    const int64_t gq = zo + (int64_t)(blockIdx.y * 8 + (q >> 5)) * P.nx + blockIdx.x * 32 + (q & 31);
 #pragma unroll
-    for (int c = 0; c < S; ++c) io[c][q] = mu[c];
+    for (int c = 0; c < S; ++c) P.mm[c * P.npts + gq] = mu[c];
 #pragma unroll
-    for (int c = 0; c < NM; ++c) io[S + c][q] = M[c];
-  }
-  __syncthreads();
-  if (valid) {
-#pragma unroll
-    for (int c = 0; c < NP; ++c) P.mm[c * P.npts + g] = io[c][tid];
+    for (int c = 0; c < NM; ++c) P.mm[(S + c) * P.npts + gq] = M[c];
   }
   if (flags) atomicOr(&P.st->flags, flags);
+}
+
+// Copies (cp.async) of one plane's composition hi and mu/M at the tile and
+// its 1-cell halo (corners skipped; the tile only when interior_only) into a
+// ring slot: X in the 2-halo SoA layout of the face routines, mu/M in the
+// mu_plane32 layout.  Commit and wait are the caller's.
+template <int TX, int TY>
+__device__ __forceinline__ void copy_plane_async32(const Rate32 &P, int64_t zoff, const int *wx,
+                                                   const int *wy, bool interior_only, float *xdst,
+                                                   float *mdst, int tid) {
+  using G = PlaneGeom<TX, TY>;
+  for (int pos = tid; pos < G::PM; pos += G::NT) {
+    const int my = pos / G::MX, mx = pos - my * G::MX;
+    if (skip_pos<G::MX, G::MY>(mx, my, interior_only)) continue;
+    const int64_t g = zoff + (int64_t)wy[my + 1] * P.nx + wx[mx + 1];
+    const int px = (my + 1) * G::HX + (mx + 1);
+    const float *src = reinterpret_cast<const float *>(P.D + g);
+#pragma unroll
+    for (int c = 0; c < S; ++c) __pipeline_memcpy_async(xdst + c * G::PX + px, src + c, 4);
+#pragma unroll
+    for (int c = 0; c < NP; ++c) __pipeline_memcpy_async(mdst + c * G::PM + pos, P.mm + c * P.npts + g, 4);
+  }
+}
+
+// Split rate evaluation, second kernel in 3D: face fluxes and divergence of
+// a plane tile marching along axis 0, mu/M read from P.mm.  The copies of
+// plane z+2 are in flight while plane z is evaluated (three-slot rings for
+// X and mu/M).  Same face routine and divergence order as k32_rate_march3d.
+template <int TX, int TY, int MINB>
+__global__ void __launch_bounds__(TX * TY, MINB) k32_flux_march3d(Rate32 P, int zc) {
+  using G = PlaneGeom<TX, TY>;
+  if (P.st->halt) return;
+  extern __shared__ float4 sm4[];
+  double *red = reinterpret_cast<double *>(sm4);
+  float *Xs = reinterpret_cast<float *>(red + G::NT / 32);      // [3][S][PX]
+  float *Ms = Xs + 3 * S * G::PX;                                // [3][NP][PM]
+  float *Fx = Ms + 3 * NP * G::PM;
+  float *Fy = Fx + S * G::NFX;
+  int *wx = reinterpret_cast<int *>(Fy + S * G::NFY);
+  int *wy = wx + G::HX;
+  const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * TX + tx;
+  const int x0 = blockIdx.x * TX, y0 = blockIdx.y * TY;
+  const int zb = blockIdx.z * zc;
+  const int ze = min(zb + zc, P.nz);
+  const int64_t plane = (int64_t)P.ny * P.nx;
+  for (int i = tid; i < G::HX + G::HY; i += G::NT) {
+    if (i < G::HX) wx[i] = wrap_any(x0 + i - 2, P.nx);
+    else wy[i - G::HX] = wrap_any(y0 + (i - G::HX) - 2, P.ny);
+  }
+  __syncthreads();
+  auto slot = [&](int z) { return (z - zb + 3) % 3; };
+  auto xplane = [&](int z) { return Xs + slot(z) * S * G::PX; };
+  auto mplane = [&](int z) { return Ms + slot(z) * NP * G::PM; };
+  auto issue = [&](int z, bool interior_only) {
+    copy_plane_async32<TX, TY>(P, (int64_t)wrap_any(z, P.nz) * plane, wx, wy, interior_only,
+                               xplane(z), mplane(z), tid);
+    __pipeline_commit();
+  };
+  const int pX = (ty + 2) * G::HX + (tx + 2);
+  const int pM = (ty + 1) * G::MX + (tx + 1);
+  const bool in_tile = (x0 + tx < P.nx) && (y0 + ty < P.ny);
+  issue(zb - 1, true);
+  issue(zb, false);
+  issue(zb + 1, false);
+  __pipeline_wait_prior(1);
+  __syncthreads();
+  float Jm[S];
+  face32_between<G::PX, G::PM>(P, xplane(zb - 1), mplane(zb - 1), pX, pM, xplane(zb), mplane(zb),
+                               pX, pM, Jm);
+  float vmax = 0.f;
+  for (int z = zb; z < ze; ++z) {
+    __pipeline_wait_prior(0);          // plane z+1 copied (this thread's part)
+    __syncthreads();                   // ... and every thread's; slot of z-1 free
+    if (z + 2 <= ze) issue(z + 2, false);
+    float Jz[S];
+    face32_between<G::PX, G::PM>(P, xplane(z), mplane(z), pX, pM, xplane(z + 1), mplane(z + 1),
+                                 pX, pM, Jz);
+    plane_faces32<TX, TY>(P, xplane(z), mplane(z), Fx, Fy, tid);
+    __syncthreads();
+    if (in_tile) {
+      float out[S];
+#pragma unroll
+      for (int c = 0; c < S; ++c) {
+        const float a = (Jz[c] - Jm[c]) +
+                        (Fy[c * G::NFY + (ty + 1) * TX + tx] - Fy[c * G::NFY + ty * TX + tx]) +
+                        (Fx[c * G::NFX + ty * (TX + 1) + tx + 1] - Fx[c * G::NFX + ty * (TX + 1) + tx]);
+        out[c] = a * P.inv_dx;
+      }
+      store_rate(P.dX, (int64_t)z * plane + (int64_t)(y0 + ty) * P.nx + (x0 + tx), out, vmax);
+    }
+#pragma unroll
+    for (int c = 0; c < S; ++c) Jm[c] = Jz[c];
+  }
+  __pipeline_wait_prior(0);
+  finish_rate32(P, vmax, red);
+}
+
+template <int TX, int TY>
+constexpr size_t flux_march3d32_smem() {
+  using G = PlaneGeom<TX, TY>;
+  return (G::NT / 32) * sizeof(double) +
+         (3 * S * G::PX + 3 * NP * G::PM + S * G::NFX + S * G::NFY) * sizeof(float) +
+         (G::HX + G::HY) * sizeof(int);
 }
 
 template <int DIM, int KMINB>
@@ -554,13 +651,12 @@ Variant32 make_split_variant32() {
   v.minb = MINB;
   v.split = true;
   v.smem2d = tile2d32_smem<TX, TY>();
-  v.smem3d = march3d32_smem<TX, TY>();
+  v.smem3d = flux_march3d32_smem<TX, TY>();
   v.set_attrs = []() {
     const auto a = cudaFuncAttributeMaxDynamicSharedMemorySize;
     cudaFuncSetAttribute(k32_rate_tile2d<TX, TY, MINB, false, false, true>, a,
                          (int)tile2d32_smem<TX, TY>());
-    cudaFuncSetAttribute(k32_rate_march3d<TX, TY, MINB, false, false, true>, a,
-                         (int)march3d32_smem<TX, TY>());
+    cudaFuncSetAttribute(k32_flux_march3d<TX, TY, MINB>, a, (int)flux_march3d32_smem<TX, TY>());
   };
   v.launch2d = [](dim3 g, dim3 b, size_t sm, cudaStream_t s, const Rate32 &P) {
     launch_chem32<2, KMINB>(s, P);
@@ -568,7 +664,7 @@ Variant32 make_split_variant32() {
   };
   v.launch3d = [](dim3 g, dim3 b, size_t sm, cudaStream_t s, const Rate32 &P, int zc) {
     launch_chem32<3, KMINB>(s, P);
-    k32_rate_march3d<TX, TY, MINB, false, false, true><<<g, b, sm, s>>>(P, zc);
+    k32_flux_march3d<TX, TY, MINB><<<g, b, sm, s>>>(P, zc);
   };
   return v;
 }

@@ -290,7 +290,7 @@ __device__ __forceinline__ void load_mu_plane(const RateParams &P, int64_t zoff,
 template <int DIM, bool VEC, int MINB>
 __global__ void __launch_bounds__(256, MINB) k_chem64(RateParams P) {
   constexpr int NT = 256;
-  __shared__ double io[NP][NT];          // inputs (x, lap, s'), then outputs (mu, M)
+  __shared__ double io[2 * S + 1][NT];   // inputs of each point: x, lap, s'
   __shared__ int hist[NT];
   __shared__ int wsum[NT / 32 + 1];
   __shared__ unsigned short order[NT];
@@ -355,10 +355,9 @@ __global__ void __launch_bounds__(256, MINB) k_chem64(RateParams P) {
   if (valid) order[hist[key] + rank] = (unsigned short)tid;
   __syncthreads();
   unsigned flags = 0;
-  double v[NP], mu[S];
-  int q = -1;
+  double v[NP];
   if (tid < count) {
-    q = order[tid];
+    const int q = order[tid];
     double xq[S], lq[S];
 #pragma unroll
     for (int c = 0; c < S; ++c) {
@@ -368,25 +367,17 @@ __global__ void __launch_bounds__(256, MINB) k_chem64(RateParams P) {
     const double spv = io[2 * S][q];
     const int o[S] = {0, 0, 0, 0};
     interp_win64<VEC>(P.T, xq, nullptr, o, v, &flags);
+    // point q of the tile: row q / 32, column q % 32
+    const int64_t gq = zo + (int64_t)(blockIdx.y * 8 + (q >> 5)) * P.nx + blockIdx.x * 32 + (q & 31);
 #pragma unroll
     for (int c = 0; c < S; ++c) {
       const double lk = lq[c] * P.kappa.v[c];
       double m = v[c] - lk;
       if (P.sp) m = m + spv * P.lvec.v[c];
-      mu[c] = m;
+      P.mm[c * P.npts + gq] = m;
     }
-  }
-  __syncthreads();                       // all inputs read: io now takes the outputs
-  if (q >= 0) {
 #pragma unroll
-    for (int c = 0; c < S; ++c) io[c][q] = mu[c];
-#pragma unroll
-    for (int c = 0; c < NM; ++c) io[S + c][q] = v[S + c];
-  }
-  __syncthreads();
-  if (valid) {
-#pragma unroll
-    for (int c = 0; c < NP; ++c) P.mm[c * P.npts + g] = io[c][tid];
+    for (int c = 0; c < NM; ++c) P.mm[(S + c) * P.npts + gq] = v[S + c];
   }
   if (flags) atomicOr(&P.st->flags, flags);
 }
