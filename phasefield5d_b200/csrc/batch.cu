@@ -424,7 +424,7 @@ const std::vector<BatchVariant> &batch_variants() {
 }
 
 // Parallel FFT branches of a batch step graph (one stream per branch).
-constexpr int kFftBranches = 8;
+constexpr int kFftBranches = 16;
 
 struct ShapeGroup {
   int ny, nx, count;

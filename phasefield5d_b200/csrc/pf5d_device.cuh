@@ -351,4 +351,9 @@ __device__ __forceinline__ int block_exclusive_scan(int *bins, int *wsum, int ti
   return total;
 }
 
+// Wait for the previous kernel of the stream (and its memory) when this
+// kernel was launched with programmatic stream serialization; a no-op
+// otherwise.
+__device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+
 }  // namespace pf5d

@@ -27,6 +27,25 @@ inline unsigned grid_for(int64_t n, int threads, int waves = 8) {
   return (unsigned)(want < 1 ? 1 : (want < cap ? want : cap));
 }
 
+// Launch with programmatic stream serialization: the kernel's grid may be
+// scheduled while the previous kernel in the stream finishes; the kernel
+// must call pdl_wait() before touching memory that kernel writes.
+template <typename... KArgs, typename... Args>
+cudaError_t launch_pdl(void (*kernel)(KArgs...), dim3 grid, dim3 block, size_t smem,
+                       cudaStream_t s, Args... args) {
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = grid;
+  cfg.blockDim = block;
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = s;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  attr[0].val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  return cudaLaunchKernelEx(&cfg, kernel, args...);
+}
+
 }  // namespace pf5d
 
 #define PF5D_CUDA(call)                                                             \

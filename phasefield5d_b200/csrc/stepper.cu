@@ -294,6 +294,7 @@ __global__ void __launch_bounds__(256, MINB) k_chem64(RateParams P) {
   __shared__ int hist[NT];
   __shared__ int wsum[NT / 32 + 1];
   __shared__ unsigned short order[NT];
+  pdl_wait();
   if (P.st->halt) return;
   const int tid = threadIdx.y * 32 + threadIdx.x;
   const int x = blockIdx.x * 32 + threadIdx.x;
@@ -405,6 +406,7 @@ __device__ __forceinline__ void finish_rate(const RateParams &P, double m, doubl
 constexpr int kDtThreads = 1024;
 __global__ void __launch_bounds__(kDtThreads) k_dt_finish(RateParams P, int nparts) {
   __shared__ double red[kDtThreads / 32];
+  pdl_wait();
   StepState *st = P.st;
   if (st->halt) return;
   double m = 0.0;
@@ -502,6 +504,7 @@ template <int TX, int TY, int MINB, bool VEC, bool WIN, bool SPLIT = false, int 
 __global__ void __launch_bounds__(NTH, MINB) k_rate_tile2d(RateParams P) {
   using G = PlaneGeom<TX, TY, NTH>;
   static_assert(NTH >= TX * TY && NTH % 32 == 0, "one thread per tile point at least");
+  pdl_wait();
   if (P.st->halt) return;
   extern __shared__ double sm[];
   double *Xs = sm;                       // [S][PX]
@@ -616,6 +619,7 @@ struct March64Geom {
 template <int TX, int TY, int MINB, bool VEC, bool WIN, bool SPLIT = false, bool SORT = false>
 __global__ void __launch_bounds__(TX * TY, MINB) k_rate_march3d(RateParams P, int zc) {
   using G = PlaneGeom<TX, TY>;
+  pdl_wait();
   if (P.st->halt) return;
   extern __shared__ double sm[];
   double *Xs = sm;                                           // [3][S][PX]
@@ -751,6 +755,7 @@ constexpr size_t march3d_smem() {
 // ------------------------------------------------------------------------
 template <int TX, bool VEC>
 __global__ void __launch_bounds__(TX) k_rate_1d(RateParams P) {
+  pdl_wait();
   if (P.st->halt) return;
   constexpr int HX = TX + 4, MX = TX + 2;
   __shared__ double Xs[S][HX];
@@ -860,6 +865,7 @@ __device__ __forceinline__ void raise_flags(StepState *st, unsigned f) {
 }
 
 __global__ void k_update_step(UpdateParams U) {
+  pdl_wait();
   StepState *st = U.st;
   if (st->halt) return;
   const double dt = st->dt;
@@ -1017,13 +1023,13 @@ RateVariant make_variant() {
     }
   };
   v.launch2d = [](bool vec, dim3 g, dim3 b, size_t sm, cudaStream_t s, const RateParams &P) {
-    if (vec) k_rate_tile2d<TX, TY, MINB, true, WIN, false, NTH, SORT><<<g, b, sm, s>>>(P);
-    else k_rate_tile2d<TX, TY, MINB, false, WIN, false, NTH, SORT><<<g, b, sm, s>>>(P);
+    if (vec) launch_pdl(k_rate_tile2d<TX, TY, MINB, true, WIN, false, NTH, SORT>, g, b, sm, s, P);
+    else launch_pdl(k_rate_tile2d<TX, TY, MINB, false, WIN, false, NTH, SORT>, g, b, sm, s, P);
   };
   v.launch3d = [](bool vec, dim3 g, dim3 b, size_t sm, cudaStream_t s, const RateParams &P,
                   int zc) {
-    if (vec) k_rate_march3d<TX, TY, MINB, true, WIN, false, SORT><<<g, b, sm, s>>>(P, zc);
-    else k_rate_march3d<TX, TY, MINB, false, WIN, false, SORT><<<g, b, sm, s>>>(P, zc);
+    if (vec) launch_pdl(k_rate_march3d<TX, TY, MINB, true, WIN, false, SORT>, g, b, sm, s, P, zc);
+    else launch_pdl(k_rate_march3d<TX, TY, MINB, false, WIN, false, SORT>, g, b, sm, s, P, zc);
   };
   return v;
 }
@@ -1032,8 +1038,8 @@ template <int DIM, int KMINB>
 void launch_chem(bool vec, cudaStream_t s, const RateParams &P) {
   const dim3 b(32, 8), g((unsigned)((P.nx + 31) / 32), (unsigned)((P.ny + 7) / 8),
                          (unsigned)P.nz);
-  if (vec) k_chem64<DIM, true, KMINB><<<g, b, 0, s>>>(P);
-  else k_chem64<DIM, false, KMINB><<<g, b, 0, s>>>(P);
+  if (vec) launch_pdl(k_chem64<DIM, true, KMINB>, g, b, 0, s, P);
+  else launch_pdl(k_chem64<DIM, false, KMINB>, g, b, 0, s, P);
 }
 
 template <int TX, int TY, int MINB, int KMINB>
@@ -1056,12 +1062,12 @@ RateVariant make_split_variant() {
   };
   v.launch2d = [](bool vec, dim3 g, dim3 b, size_t sm, cudaStream_t s, const RateParams &P) {
     launch_chem<2, KMINB>(vec, s, P);
-    k_rate_tile2d<TX, TY, MINB, true, false, true><<<g, b, sm, s>>>(P);
+    launch_pdl(k_rate_tile2d<TX, TY, MINB, true, false, true>, g, b, sm, s, P);
   };
   v.launch3d = [](bool vec, dim3 g, dim3 b, size_t sm, cudaStream_t s, const RateParams &P,
                   int zc) {
     launch_chem<3, KMINB>(vec, s, P);
-    k_rate_march3d<TX, TY, MINB, true, false, true><<<g, b, sm, s>>>(P, zc);
+    launch_pdl(k_rate_march3d<TX, TY, MINB, true, false, true>, g, b, sm, s, P, zc);
   };
   return v;
 }
@@ -1140,8 +1146,8 @@ pf5d_status launch_rate(pf5d_stepper *h, cudaStream_t s) {
   const size_t sm = h->rate_smem;
   switch (h->d.dim) {
     case 1:
-      if (h->vec) k_rate_1d<kTX1, true><<<g, b, 0, s>>>(h->rp);
-      else k_rate_1d<kTX1, false><<<g, b, 0, s>>>(h->rp);
+      if (h->vec) launch_pdl(k_rate_1d<kTX1, true>, g, b, 0, s, h->rp);
+      else launch_pdl(k_rate_1d<kTX1, false>, g, b, 0, s, h->rp);
       break;
     case 2:
       rate_variants()[h->variant].launch2d(h->vec, g, b, sm, s, h->rp);
@@ -1150,8 +1156,8 @@ pf5d_status launch_rate(pf5d_stepper *h, cudaStream_t s) {
       rate_variants()[h->variant].launch3d(h->vec, g, b, sm, s, h->rp, h->zc);
   }
   PF5D_LAUNCHED();
-  k_dt_finish<<<1, kDtThreads, 0, s>>>(h->rp, (int)(g.x * g.y * g.z));
-  PF5D_LAUNCHED();
+  PF5D_CUDA(launch_pdl(k_dt_finish, dim3(1), dim3(kDtThreads), 0, s, h->rp,
+                       (int)(g.x * g.y * g.z)));
   return PF5D_OK;
 }
 
@@ -1211,8 +1217,7 @@ pf5d_status enqueue_step(pf5d_stepper *h, cudaStream_t s) {
     if ((st = fft_inverse(&h->fft, h->k, h->s, s)) != PF5D_OK) return st;
   }
   if ((st = launch_rate(h, s)) != PF5D_OK) return st;
-  k_update_step<<<grid_for(h->npts, 256, 4), 256, 0, s>>>(h->up);
-  PF5D_LAUNCHED();
+  PF5D_CUDA(launch_pdl(k_update_step, dim3(grid_for(h->npts, 256, 4)), dim3(256), 0, s, h->up));
   return PF5D_OK;
 }
 
