@@ -157,6 +157,7 @@ __global__ void __launch_bounds__(TX * TY, MINB)
   Rate32 *Rs = reinterpret_cast<Rate32 *>(sm4);
   float4 *work = sm4 + BatchSmem<TX, TY, SORT>::head / 16;
   const int tid = threadIdx.y * TX + threadIdx.x;
+  pdl_wait();
   for (int t = blockIdx.x; t < total_tiles; t += gridDim.x) {
     const int si = find_solve_tile(solves, nsolves, t);
     const BSolve &B = solves[si];
@@ -187,6 +188,7 @@ __global__ void __launch_bounds__(kUpdThreads)
     kb_update(const BSolve *__restrict__ solves, int nsolves, int total_chunks) {
   __shared__ double red[kUpdThreads / 32];
   const int tid = threadIdx.x;
+  pdl_wait();
   for (int cidx = blockIdx.x; cidx < total_chunks; cidx += gridDim.x) {
     const BSolve &B = solves[find_solve_chunk(solves, nsolves, cidx)];
     StepState32 *st = B.R.st;
@@ -369,6 +371,7 @@ __global__ void kb_bmul(cufftComplex *__restrict__ k, const float *__restrict__ 
 // The dt controllers of all solves after a rate launch: one warp per solve
 // reduces its tiles' maxima and advances its dt / time / step.
 __global__ void kb_dt(const BSolve *__restrict__ solves, int nsolves, const double *tile_max) {
+  pdl_wait();
   const int i = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
   if (i >= nsolves) return;
   const BSolve &B = solves[i];
@@ -401,8 +404,8 @@ BatchVariant make_bvariant() {
   };
   v.launch = [](int grid, cudaStream_t s, const BSolve *solves, int n, int tiles,
                 double *tile_max) {
-    kb_rate<TX, TY, MINB, WIN, SORT><<<grid, dim3(TX, TY), SM::rate, s>>>(solves, n, tiles,
-                                                                          tile_max);
+    launch_pdl(kb_rate<TX, TY, MINB, WIN, SORT>, dim3(grid), dim3(TX, TY), SM::rate, s, solves, n,
+               tiles, tile_max);
   };
   v.occupancy = []() {
     int nb = 0;
@@ -535,11 +538,11 @@ pf5d_status enqueue_batch_step(pf5d_batch *h, cudaStream_t s) {
   batch_variants()[h->variant].launch(h->rate_grid, s, h->d_solves, (int)h->solves.size(),
                                       h->total_tiles, h->tile_max);
   PF5D_LAUNCHED();
-  kb_dt<<<(unsigned)((h->solves.size() + 7) / 8), 256, 0, s>>>(h->d_solves, (int)h->solves.size(),
-                                                                h->tile_max);
-  PF5D_LAUNCHED();
-  kb_update<<<h->upd_grid, kUpdThreads, 0, s>>>(h->d_solves, (int)h->solves.size(),
-                                                h->total_chunks);
+  PF5D_CUDA(launch_pdl(kb_dt, dim3((unsigned)((h->solves.size() + 7) / 8)), dim3(256), 0, s,
+                       (const BSolve *)h->d_solves, (int)h->solves.size(),
+                       (const double *)h->tile_max));
+  PF5D_CUDA(launch_pdl(kb_update, dim3(h->upd_grid), dim3(kUpdThreads), 0, s,
+                       (const BSolve *)h->d_solves, (int)h->solves.size(), h->total_chunks));
   PF5D_LAUNCHED();
   return PF5D_OK;
 }

@@ -42,6 +42,7 @@ namespace pf5d {
 
 template <int TX, int TY, int MINB, bool WIN, bool SORT = false, bool SPLIT = false>
 __global__ void __launch_bounds__(TX * TY, MINB) k32_rate_tile2d(Rate32 P) {
+  pdl_wait();
   if (P.st->halt) return;
   extern __shared__ float4 sm4[];
   const int tid = threadIdx.y * TX + threadIdx.x;
@@ -60,6 +61,7 @@ constexpr size_t tile2d32_smem() {
 template <int TX, int TY, int MINB, bool WIN, bool SORT = false, bool SPLIT = false>
 __global__ void __launch_bounds__(TX * TY, MINB) k32_rate_march3d(Rate32 P, int zc) {
   using G = PlaneGeom<TX, TY>;
+  pdl_wait();
   if (P.st->halt) return;
   extern __shared__ float4 sm4[];
   float4 *win = sm4;
@@ -168,6 +170,7 @@ constexpr size_t march3d32_smem() {
 
 template <int TX>
 __global__ void __launch_bounds__(TX) k32_rate_1d(Rate32 P) {
+  pdl_wait();
   if (P.st->halt) return;
   constexpr int HX = TX + 4, MX = TX + 2;
   __shared__ float Xs[S][HX];
@@ -249,6 +252,7 @@ struct Update32 {
 };
 
 __global__ void k32_update(Update32 U) {
+  pdl_wait();
   StepState32 *st = U.st;
   if (st->halt) return;
   const float dtf = (float)st->dt;
@@ -383,6 +387,7 @@ __global__ void __launch_bounds__(256, MINB) k32_chem(Rate32 P) {
   __shared__ int hist[NT];
   __shared__ int wsum[NT / 32 + 1];
   __shared__ unsigned short order[NT];
+  pdl_wait();
   if (P.st->halt) return;
   const int tid = threadIdx.y * 32 + threadIdx.x;
   const int x = blockIdx.x * 32 + threadIdx.x;
@@ -484,6 +489,7 @@ __device__ __forceinline__ void copy_plane_async32(const Rate32 &P, int64_t zoff
 template <int TX, int TY, int MINB>
 __global__ void __launch_bounds__(TX * TY, MINB) k32_flux_march3d(Rate32 P, int zc) {
   using G = PlaneGeom<TX, TY>;
+  pdl_wait();
   if (P.st->halt) return;
   extern __shared__ float4 sm4[];
   double *red = reinterpret_cast<double *>(sm4);
@@ -561,7 +567,7 @@ constexpr size_t flux_march3d32_smem() {
 template <int DIM, int KMINB>
 void launch_chem32(cudaStream_t s, const Rate32 &P) {
   const dim3 b(32, 8), g((unsigned)((P.nx + 31) / 32), (unsigned)((P.ny + 7) / 8), (unsigned)P.nz);
-  k32_chem<DIM, KMINB><<<g, b, 0, s>>>(P);
+  launch_pdl(k32_chem<DIM, KMINB>, g, b, 0, s, P);
 }
 
 // The dt controller after a rate launch of `nparts` blocks: a block-wide
@@ -569,6 +575,7 @@ void launch_chem32(cudaStream_t s, const Rate32 &P) {
 constexpr int kDt32Threads = 1024;
 __global__ void __launch_bounds__(kDt32Threads) k32_dt(Rate32 P, int nparts) {
   __shared__ double red[kDt32Threads / 32];
+  pdl_wait();
   StepState32 *st = P.st;
   if (st->halt) return;
   double m = 0.0;
@@ -633,10 +640,10 @@ Variant32 make_variant32() {
                          (int)march3d32_smem<TX, TY, SORT>());
   };
   v.launch2d = [](dim3 g, dim3 b, size_t sm, cudaStream_t s, const Rate32 &P) {
-    k32_rate_tile2d<TX, TY, MINB, WIN, SORT><<<g, b, sm, s>>>(P);
+    launch_pdl(k32_rate_tile2d<TX, TY, MINB, WIN, SORT>, g, b, sm, s, P);
   };
   v.launch3d = [](dim3 g, dim3 b, size_t sm, cudaStream_t s, const Rate32 &P, int zc) {
-    k32_rate_march3d<TX, TY, MINB, WIN, SORT><<<g, b, sm, s>>>(P, zc);
+    launch_pdl(k32_rate_march3d<TX, TY, MINB, WIN, SORT>, g, b, sm, s, P, zc);
   };
   return v;
 }
@@ -660,11 +667,11 @@ Variant32 make_split_variant32() {
   };
   v.launch2d = [](dim3 g, dim3 b, size_t sm, cudaStream_t s, const Rate32 &P) {
     launch_chem32<2, KMINB>(s, P);
-    k32_rate_tile2d<TX, TY, MINB, false, false, true><<<g, b, sm, s>>>(P);
+    launch_pdl(k32_rate_tile2d<TX, TY, MINB, false, false, true>, g, b, sm, s, P);
   };
   v.launch3d = [](dim3 g, dim3 b, size_t sm, cudaStream_t s, const Rate32 &P, int zc) {
     launch_chem32<3, KMINB>(s, P);
-    k32_flux_march3d<TX, TY, MINB><<<g, b, sm, s>>>(P, zc);
+    launch_pdl(k32_flux_march3d<TX, TY, MINB>, g, b, sm, s, P, zc);
   };
   return v;
 }
@@ -764,13 +771,13 @@ static pf5d_status configure32(Stepper32 *h, int variant) {
 
 static pf5d_status launch_rate32(Stepper32 *h, cudaStream_t s) {
   switch (h->d.dim) {
-    case 1: k32_rate_1d<kTX1_32><<<h->grid, h->block, 0, s>>>(h->rp); break;
+    case 1: launch_pdl(k32_rate_1d<kTX1_32>, h->grid, h->block, 0, s, h->rp); break;
     case 2: variants32()[h->variant].launch2d(h->grid, h->block, h->smem, s, h->rp); break;
     default: variants32()[h->variant].launch3d(h->grid, h->block, h->smem, s, h->rp, h->zc);
   }
   PF5D_LAUNCHED();
-  k32_dt<<<1, kDt32Threads, 0, s>>>(h->rp, (int)(h->grid.x * h->grid.y * h->grid.z));
-  PF5D_LAUNCHED();
+  PF5D_CUDA(launch_pdl(k32_dt, dim3(1), dim3(kDt32Threads), 0, s, h->rp,
+                       (int)(h->grid.x * h->grid.y * h->grid.z)));
   return PF5D_OK;
 }
 
@@ -785,7 +792,7 @@ static pf5d_status enqueue32(Stepper32 *h, cudaStream_t s) {
   }
   pf5d_status st = launch_rate32(h, s);
   if (st != PF5D_OK) return st;
-  k32_update<<<grid_for(h->npts, 256, 4), 256, 0, s>>>(h->up);
+  PF5D_CUDA(launch_pdl(k32_update, dim3(grid_for(h->npts, 256, 4)), dim3(256), 0, s, h->up));
   PF5D_LAUNCHED();
   return PF5D_OK;
 }

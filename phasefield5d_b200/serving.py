@@ -238,9 +238,31 @@ class GpuBackend:
         self.reqs: dict[int, Request] = {}
         self.batch_stream = torch.cuda.Stream()
         self.variants: dict[tuple, int] = {}      # shape -> autotuned kernel variant
-        self.tables: dict[tuple, object] = {}     # resident FP32 tables of the batch
+        self.tables: dict[tuple, object] = {}     # resident device tables, per temperature
+        self.table_mu: dict[tuple, object] = {}   # mu reference each FP32 table subtracts
         self.pending: dict[object, object] = {}   # unit ("batch" or rid) -> event of its block
         self.fresh = False                        # batch rebuilt: report its states
+
+    def _table(self, prob):
+        """Resident device table of the request's temperature (built once):
+        FP32 mu - mu(equiatomic) for the compensated form -- the same table
+        the batch uses -- or the padded FP64 table."""
+        import numpy as np
+        from .batch import TABLE_REFERENCE_X, _table32
+        from .solver.table import host_table_eval
+        from .stepper import device_table
+        key = (prob.cfg.temperature, prob.table.seed, prob.cfg.resolution)
+        if self.precision == "fp64":
+            key = ("fp64",) + key
+            if key not in self.tables:
+                self.tables[key] = device_table(prob.grid, self.torch)
+            return self.tables[key], None
+        if key not in self.table_mu:
+            self.table_mu[key] = host_table_eval(np.asarray(TABLE_REFERENCE_X)[None, :], prob.grid,
+                                                 prob.cfg.resolution)[0, :4]
+        if key not in self.tables:
+            self.tables[key] = _table32(prob.grid, self.table_mu[key], self.torch)
+        return self.tables[key], self.table_mu[key]
 
     def shares_batch(self, req):
         """True when the request advances in the shared 1D/2D batch."""
@@ -264,9 +286,11 @@ class GpuBackend:
             if not self.shares_batch(r) and r.rid not in self.steppers:
                 s = torch.cuda.Stream()
                 key = tuple(r.problem.shape)
+                tab, mu0 = self._table(r.problem)
                 with torch.cuda.stream(s):
                     st = self.Stepper.from_problem(r.problem, precision=self.precision, stream=s,
-                                                   autotune=key not in self.variants)
+                                                   autotune=key not in self.variants, table=tab,
+                                                   table_mu0=mu0)
                     if key in self.variants:
                         st.set_variant(self.variants[key])
                     else:

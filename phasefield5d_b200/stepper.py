@@ -29,12 +29,17 @@ class Stepper:
     ``dx``; rank-1 elastic factor ``lvec`` and ``bk`` = B(k) on the rfft
     half-grid (both None: elasticity off); ``ctld``, ``t_cfl``, initial
     ``dt``; ``adaptive`` (False: dt fixed); change limits.
+
+    ``table`` (optional): the device table already in the layout of this
+    form -- (n,n,n,n,10) float64 for "fp64", (n,n,n,n,12) float32 holding
+    mu - ``table_mu0`` for "fp32c" -- so solves at the same temperature can
+    share one resident copy.
     """
 
     def __init__(self, *, grid, resolution, node_coord, X, X0, kappa, dx, lvec, bk, ctld, t_cfl,
                  dt, adaptive=True, lower_limit=1e-5, upper_limit=1e-3, max_change_factor=2.0,
                  oob_interval=100, max_nn_dist=None, stream=None, autotune=True,
-                 precision="fp64"):
+                 precision="fp64", table=None, table_mu0=None):
         import torch
         self._torch = torch
         self.L = _lib.load()
@@ -47,7 +52,14 @@ class Stepper:
         if precision not in ("fp64", "fp32c"):
             raise ValueError(f"precision must be 'fp64' or 'fp32c' (got {precision!r})")
         self.precision = precision
-        self.grid = device_table(grid, torch)
+        if table is not None and precision == "fp32c" and table_mu0 is None:
+            raise ValueError("a shared FP32 table needs the mu reference it subtracts (table_mu0)")
+        if precision == "fp64":
+            self.grid = table if table is not None else device_table(grid, torch)
+            table_n = int(self.grid.shape[0])
+        else:
+            self.grid = None
+            table_n = int(table.shape[0]) if table is not None else int(np.shape(grid)[0])
         self.node_coord = torch.from_numpy(np.ascontiguousarray(node_coord,
                                                                 dtype=np.float64)).cuda()
         if isinstance(X, torch.Tensor):
@@ -71,10 +83,10 @@ class Stepper:
         self._bk = np.ascontiguousarray(bk, dtype=np.float64) if elastic else None
         d.bk = (self._bk.ctypes.data_as(ctypes.POINTER(ctypes.c_double)) if elastic
                 else ctypes.POINTER(ctypes.c_double)())
-        d.grid = self.grid.data_ptr()
-        d.table_n = int(self.grid.shape[0])
+        d.grid = self.grid.data_ptr() if self.grid is not None else None
+        d.table_n = table_n
         d.nprops = 9
-        d.node_stride = int(self.grid.shape[-1])
+        d.node_stride = int(self.grid.shape[-1]) if self.grid is not None else NODE_STRIDE
         d.resolution = float(resolution)
         d.node_coord = self.node_coord.data_ptr()
         d.max_nn_dist = float(max_nn_dist) if max_nn_dist is not None else -1.0
@@ -88,8 +100,11 @@ class Stepper:
         d.oob_interval = int(oob_interval)
         d.precision = _lib.PRECISION_FP64 if precision == "fp64" else _lib.PRECISION_FP32C
         if precision == "fp32c":
-            mu0 = reference_mu(grid, resolution, X0)
-            self.grid32 = device_table32(grid, mu0, torch)
+            if table is not None:
+                mu0, self.grid32 = np.asarray(table_mu0, dtype=np.float64), table
+            else:
+                mu0 = reference_mu(grid, resolution, X0)
+                self.grid32 = device_table32(grid, mu0, torch)
             d.grid32 = self.grid32.data_ptr()
             d.node_stride32 = NODE_STRIDE32
             for i in range(4):
