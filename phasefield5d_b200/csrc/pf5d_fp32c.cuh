@@ -19,11 +19,8 @@ struct StepState32 {
   double dt;
   double time;
   double xdotmax;
-  double xacc;
-  unsigned blocks_done;
   unsigned flags;
   unsigned halt;
-  unsigned pad;
   long long step;
 };
 

@@ -42,11 +42,8 @@ struct StepState {
   double dt;
   double time;
   double xdotmax;      // max |dX/dt| of the last rate evaluation
-  double xacc;         // running max of the current evaluation (bit-wise atomicMax)
-  unsigned blocks_done;
   unsigned flags;      // PF5D_FLAG_* accumulated
   unsigned halt;       // non-zero: every step kernel returns at entry
-  unsigned pad;
   long long step;      // completed steps
 };
 
