@@ -255,8 +255,8 @@ typedef struct {
 /* One step, exactly as pf5d_stepper_advance(h, 1), plus the save-step
  * diagnostics of that step; synchronises the stream.  Replaces the save
  * branch of examples/simulate.py:299-354 (calculate_gradients_pm,
- * compute_fluxes and the numpy reductions).  Plain FP64 form only
- * (PF5D_ERR_ARG for the FP32C form). */
+ * compute_fluxes and the numpy reductions).  Either form; the FP32C form
+ * reduces FP64 copies of its field X0 + hi + lo, dX/dt and mu/M. */
 pf5d_status pf5d_stepper_step_save(pf5d_stepper *h, pf5d_save_diag *out, void *stream);
 /* Number of rate-kernel variants of this stepper's form (valid indices for
  * pf5d_stepper_set_variant are 0 .. count-1); 0 for a null stepper. */

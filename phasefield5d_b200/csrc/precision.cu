@@ -407,7 +407,7 @@ __global__ void __launch_bounds__(256, MINB) k32_chem(Rate32 P) {
     };
     const int xp = x + 1 == P.nx ? 0 : x + 1, xm = x == 0 ? P.nx - 1 : x - 1;
     const int yp = y + 1 == P.ny ? 0 : y + 1, ym = y == 0 ? P.ny - 1 : y - 1;
-    constexpr int NB = DIM == 3 ? 6 : 4;
+    constexpr int NB = 2 * DIM;
     float d[S], nb[NB][S];
     ld(g, d);
     int k = 0;
@@ -416,8 +416,10 @@ __global__ void __launch_bounds__(256, MINB) k32_chem(Rate32 P) {
       ld((int64_t)zp * plane + (int64_t)y * P.nx + x, nb[k++]);
       ld((int64_t)zm * plane + (int64_t)y * P.nx + x, nb[k++]);
     }
-    ld(zo + (int64_t)yp * P.nx + x, nb[k++]);
-    ld(zo + (int64_t)ym * P.nx + x, nb[k++]);
+    if (DIM >= 2) {
+      ld(zo + (int64_t)yp * P.nx + x, nb[k++]);
+      ld(zo + (int64_t)ym * P.nx + x, nb[k++]);
+    }
     ld(zo + (int64_t)y * P.nx + xp, nb[k++]);
     ld(zo + (int64_t)y * P.nx + xm, nb[k]);
     float u[S];
@@ -929,13 +931,11 @@ pf5d_status s32_create(const pf5d_stepper_desc *desc, const double *X_init, void
   }
   P.partial = h->partial;
   P.npts = npts;
-  if (desc->dim >= 2) {
-    if (cudaMalloc(&h->mm, (size_t)npts * NP * sizeof(float)) != cudaSuccess) {
-      set_error("device allocation failed");
-      return fail(PF5D_ERR_CUDA);
-    }
-    P.mm = h->mm;
+  if (cudaMalloc(&h->mm, (size_t)npts * NP * sizeof(float)) != cudaSuccess) {
+    set_error("device allocation failed");
+    return fail(PF5D_ERR_CUDA);
   }
+  P.mm = h->mm;
   Update32 &U = h->up;
   U.hi = h->hi;
   U.lo = h->lo;
@@ -994,6 +994,50 @@ pf5d_status s32_state(Stepper32 *h, pf5d_step_state *out, void *stream) {
   out->step = hs.step;
   out->flags = hs.flags | (hs.halt ? PF5D_FLAG_HALTED : 0u);
   out->halted = hs.halt;
+  return PF5D_OK;
+}
+
+// FP64 copies for the save-step reductions: dX/dt (4 per point) and mu/M
+// (SoA, 9 rows), from the FP32 buffers.
+__global__ void k32_widen(const float *__restrict__ src, int64_t n, double *__restrict__ dst) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
+       i += (int64_t)gridDim.x * blockDim.x)
+    dst[i] = (double)src[i];
+}
+
+pf5d_status s32_step_save_inputs(Stepper32 *h, double *X_out, double *dX_out, double *mm_out,
+                                 void *stream) {
+  cudaStream_t s = as_stream(stream);
+  if (h->d.elastic) {
+    PF5D_CUFFT32(cufftSetStream(h->fwd, s));
+    PF5D_CUFFT32(cufftExecR2C(h->fwd, h->s, h->k));
+    k32_bmul<<<grid_for(h->nk, 256), 256, 0, s>>>(h->k, h->bk, h->nk, &h->st->halt);
+    PF5D_LAUNCHED();
+    PF5D_CUFFT32(cufftSetStream(h->inv, s));
+    PF5D_CUFFT32(cufftExecC2R(h->inv, h->k, h->s));
+  }
+  pf5d_status st = launch_rate32(h, s);
+  if (st != PF5D_OK) return st;
+  switch (h->d.dim) {
+    case 1: launch_chem32<1, 3>(s, h->rp); break;
+    case 2: launch_chem32<2, 3>(s, h->rp); break;
+    default: launch_chem32<3, 3>(s, h->rp);
+  }
+  PF5D_LAUNCHED();
+  k32_join<<<grid_for(h->npts, 256, 4), 256, 0, s>>>(h->hi, h->lo, h->npts, h->up, X_out);
+  PF5D_LAUNCHED();
+  k32_widen<<<grid_for(4 * h->npts, 256, 4), 256, 0, s>>>(reinterpret_cast<const float *>(h->dX),
+                                                          4 * h->npts, dX_out);
+  PF5D_LAUNCHED();
+  k32_widen<<<grid_for(NP * h->npts, 256, 4), 256, 0, s>>>(h->mm, NP * h->npts, mm_out);
+  PF5D_LAUNCHED();
+  return PF5D_OK;
+}
+
+pf5d_status s32_step_update(Stepper32 *h, void *stream) {
+  cudaStream_t s = as_stream(stream);
+  k32_update<<<grid_for(h->npts, 256, 4), 256, 0, s>>>(h->up);
+  PF5D_LAUNCHED();
   return PF5D_OK;
 }
 

@@ -972,6 +972,7 @@ struct pf5d_stepper {
   double *mm = nullptr;          // split-rate mu/M buffer (also save-step diagnostics)
   double *diag_ws = nullptr;     // save-step partial rows + mean
   double *partial = nullptr;     // rate kernel block maxima
+  double *save_x = nullptr;      // FP32C save steps: FP64 field, dX/dt, mu/M
 };
 
 namespace {
@@ -1483,62 +1484,79 @@ pf5d_status pf5d_stepper_set_variant(pf5d_stepper *h, int32_t variant) {
 
 pf5d_status pf5d_stepper_step_save(pf5d_stepper *h, pf5d_save_diag *out, void *stream) {
   PF5D_REQUIRE(h && out, PF5D_ERR_ARG, "bad arguments");
-  PF5D_REQUIRE(!h->s32, PF5D_ERR_ARG, "save-step diagnostics are computed by the FP64 form");
   cudaStream_t s = as_stream(stream);
   std::memset(out, 0, sizeof(*out));
-  StepState before;
-  PF5D_CUDA(cudaMemcpyAsync(&before, h->st, sizeof(before), cudaMemcpyDeviceToHost, s));
-  PF5D_CUDA(cudaStreamSynchronize(s));
+  pf5d_step_state before, after;
+  pf5d_status st = pf5d_stepper_state(h, &before, stream);
+  if (st != PF5D_OK) return st;
   out->step = before.step;
-  if (before.halt) {
+  if (before.halted) {
     out->halted = 1;
     out->dt = before.dt;
     out->time = before.time;
     return PF5D_OK;
   }
+  DiagGeom G;
+  const int dim = h->d.dim;
+  G.nz = dim == 3 ? (int)h->d.shape[0] : 1;
+  G.ny = dim == 1 ? 1 : (int)h->d.shape[dim - 2];
+  G.nx = (int)h->d.shape[dim - 1];
+  G.dim = dim;
+  G.npts = (int64_t)G.nz * G.ny * G.nx;
+  G.inv_dx = 1.0 / h->d.dx;
+  G.inv_dx2 = 1.0 / (h->d.dx * h->d.dx);
+  for (int c = 0; c < S; ++c) G.kappa[c] = h->d.kappa[c];
   const int rows = kDiagBlocks;
   if (!h->diag_ws)
     PF5D_CUDA(cudaMalloc(&h->diag_ws, (size_t)(rows * (kDiagPre + kDiagPost + kDiagVar) + S) *
                                           sizeof(double)));
   double *pre = h->diag_ws, *post = pre + rows * kDiagPre, *var = post + rows * kDiagPost;
   double *mean = var + rows * kDiagVar;
-  DiagGeom G;
-  G.nz = h->rp.nz;
-  G.ny = h->rp.ny;
-  G.nx = h->rp.nx;
-  G.dim = h->d.dim;
-  G.npts = h->npts;
-  G.inv_dx = h->rp.inv_dx;
-  G.inv_dx2 = h->rp.inv_dx2;
-  for (int c = 0; c < S; ++c) G.kappa[c] = h->rp.kappa.v[c];
-  const unsigned nb = std::min<unsigned>(rows, grid_for(h->npts, kDiagThreads, 1));
-  // the step up to its rate evaluation, as enqueue_step
-  pf5d_status st;
-  if (h->d.elastic) {
-    if ((st = fft_forward(&h->fft, h->s, h->k, s)) != PF5D_OK) return st;
-    if ((st = launch_bmul(h->k, h->bk, h->fft.nk, &h->st->halt, s)) != PF5D_OK) return st;
-    if ((st = fft_inverse(&h->fft, h->k, h->s, s)) != PF5D_OK) return st;
+  const unsigned nb = std::min<unsigned>(rows, grid_for(G.npts, kDiagThreads, 1));
+  const double *Xpre, *dXpre, *mmpre, *Xpost;
+  if (h->s32) {
+    // FP32-compensated form: FP64 copies of the field, dX/dt and mu/M
+    if (!h->save_x) {
+      PF5D_CUDA(cudaMalloc(&h->save_x, (size_t)G.npts * (4 + 4 + NP) * sizeof(double)));
+    }
+    double *sx = h->save_x, *sdx = sx + 4 * G.npts, *smm = sdx + 4 * G.npts;
+    if ((st = s32_step_save_inputs(h->s32, sx, sdx, smm, stream)) != PF5D_OK) return st;
+    k_diag_pre<<<nb, kDiagThreads, 0, s>>>(G, sx, sdx, smm, pre);
+    PF5D_LAUNCHED();
+    if ((st = s32_step_update(h->s32, stream)) != PF5D_OK) return st;
+    if ((st = s32_field(h->s32, sx, stream)) != PF5D_OK) return st;
+    Xpost = sx;
+  } else {
+    // the step up to its rate evaluation, as enqueue_step
+    if (h->d.elastic) {
+      if ((st = fft_forward(&h->fft, h->s, h->k, s)) != PF5D_OK) return st;
+      if ((st = launch_bmul(h->k, h->bk, h->fft.nk, &h->st->halt, s)) != PF5D_OK) return st;
+      if ((st = fft_inverse(&h->fft, h->k, h->s, s)) != PF5D_OK) return st;
+    }
+    if ((st = launch_rate(h, s)) != PF5D_OK) return st;
+    // mu and M of this step at every point, then the "before" reductions
+    switch (dim) {
+      case 1: launch_chem<1, 3>(h->vec, s, h->rp); break;
+      case 2: launch_chem<2, 3>(h->vec, s, h->rp); break;
+      default: launch_chem<3, 3>(h->vec, s, h->rp);
+    }
+    PF5D_LAUNCHED();
+    Xpre = h->X;
+    dXpre = h->dX;
+    mmpre = h->mm;
+    k_diag_pre<<<nb, kDiagThreads, 0, s>>>(G, Xpre, dXpre, mmpre, pre);
+    PF5D_LAUNCHED();
+    k_update_step<<<grid_for(h->npts, 256, 4), 256, 0, s>>>(h->up);
+    PF5D_LAUNCHED();
+    Xpost = h->X;
   }
-  if ((st = launch_rate(h, s)) != PF5D_OK) return st;
-  // mu and M of this step at every point, then the "before" reductions
-  switch (h->d.dim) {
-    case 1: launch_chem<1, 3>(h->vec, s, h->rp); break;
-    case 2: launch_chem<2, 3>(h->vec, s, h->rp); break;
-    default: launch_chem<3, 3>(h->vec, s, h->rp);
-  }
-  PF5D_LAUNCHED();
-  k_diag_pre<<<nb, kDiagThreads, 0, s>>>(G, h->X, h->dX, h->mm, pre);
-  PF5D_LAUNCHED();
-  k_update_step<<<grid_for(h->npts, 256, 4), 256, 0, s>>>(h->up);
-  PF5D_LAUNCHED();
-  k_diag_post<<<nb, kDiagThreads, 0, s>>>(G, h->X, post);
+  k_diag_post<<<nb, kDiagThreads, 0, s>>>(G, Xpost, post);
   PF5D_LAUNCHED();
   std::vector<double> hp((size_t)nb * kDiagPre), hq((size_t)nb * kDiagPost);
   PF5D_CUDA(cudaMemcpyAsync(hp.data(), pre, hp.size() * sizeof(double), cudaMemcpyDeviceToHost, s));
   PF5D_CUDA(cudaMemcpyAsync(hq.data(), post, hq.size() * sizeof(double), cudaMemcpyDeviceToHost, s));
-  StepState after;
-  PF5D_CUDA(cudaMemcpyAsync(&after, h->st, sizeof(after), cudaMemcpyDeviceToHost, s));
   PF5D_CUDA(cudaStreamSynchronize(s));
+  if ((st = pf5d_stepper_state(h, &after, stream)) != PF5D_OK) return st;
   for (int c = 0; c < S; ++c) {
     double net = 0.0, mx = 0.0, tf = 0.0, mass = 0.0, nmn = -INFINITY, mxx = -INFINITY;
     for (unsigned b = 0; b < nb; ++b) {
@@ -1563,12 +1581,12 @@ pf5d_status pf5d_stepper_step_save(pf5d_stepper *h, pf5d_save_diag *out, void *s
   }
   out->comp_fe_min = 1.0 - msum;
   double cell = 1.0;
-  for (int d = 0; d < h->d.dim; ++d) cell *= h->d.dx;
+  for (int d = 0; d < dim; ++d) cell *= h->d.dx;
   out->f_grad = -0.5 * cell * fg;
   double m[S];
-  for (int c = 0; c < S; ++c) m[c] = out->mass[c] / (double)h->npts;
+  for (int c = 0; c < S; ++c) m[c] = out->mass[c] / (double)G.npts;
   PF5D_CUDA(cudaMemcpyAsync(mean, m, sizeof(m), cudaMemcpyHostToDevice, s));
-  k_diag_var<<<nb, kDiagThreads, 0, s>>>(G, h->X, mean, var);
+  k_diag_var<<<nb, kDiagThreads, 0, s>>>(G, Xpost, mean, var);
   PF5D_LAUNCHED();
   std::vector<double> hv((size_t)nb * kDiagVar);
   PF5D_CUDA(cudaMemcpyAsync(hv.data(), var, hv.size() * sizeof(double), cudaMemcpyDeviceToHost, s));
@@ -1576,7 +1594,7 @@ pf5d_status pf5d_stepper_step_save(pf5d_stepper *h, pf5d_save_diag *out, void *s
   for (int c = 0; c < S; ++c) {
     double v = 0.0;
     for (unsigned b = 0; b < nb; ++b) v += hv[b * kDiagVar + c];
-    out->comp_var[c] = v / (double)h->npts;
+    out->comp_var[c] = v / (double)G.npts;
   }
   out->xdotmax = after.xdotmax;
   out->dt = after.dt;
@@ -1630,6 +1648,7 @@ pf5d_status pf5d_stepper_destroy(pf5d_stepper *h) {
   cudaFree(h->mm);
   cudaFree(h->diag_ws);
   cudaFree(h->partial);
+  cudaFree(h->save_x);
   for (auto &kv : h->graphs) cudaGraphExecDestroy(kv.second);
   fft_destroy(&h->fft);
   cudaFree(h->dX);

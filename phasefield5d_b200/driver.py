@@ -36,7 +36,7 @@ def run_simulation(stepper, total_steps, path, *, ctld, t_cfl, adaptive=True,
                    early_stage_frames=100, late_burst_duration_ctld=100, late_burst_frames=700,
                    late_tail_frames=300, save_every_n_steps_data=50_000,
                    save_every_n_steps_snap=100_000, max_block=50):
-    """Run ``total_steps`` steps of ``stepper`` (plain FP64 form) writing the
+    """Run ``total_steps`` steps of ``stepper`` (either form) writing the
     reference's state files and traces under ``path``.  Returns the traces
     dict and the list of state files written."""
     kw = dict(early_frames=early_stage_frames, burst_duration_ctld=late_burst_duration_ctld,

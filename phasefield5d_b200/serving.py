@@ -32,12 +32,13 @@ from dataclasses import dataclass, field
 import numpy as np
 
 # Device bytes per grid point of an admitted FP32-compensated solve: hi, lo
-# and dX/dt (3 x 16), the misfit scalar and its half spectrum (~4 + 8), and
-# working room for cuFFT (16).
-BYTES_PER_POINT = 96
-# The plain FP64 form: X and dX/dt (2 x 32), the FP64 misfit scalar and its
-# half spectrum (8 + 16), cuFFT working room (32).
-BYTES_PER_POINT_FP64 = 120
+# and dX/dt (3 x 16), the mu/M buffer of the split rate kernels (36), the
+# misfit scalar and its half spectrum (~4 + 8), and working room for cuFFT
+# (16).
+BYTES_PER_POINT = 132
+# The plain FP64 form: X and dX/dt (2 x 32), the mu/M buffer (72), the FP64
+# misfit scalar and its half spectrum (8 + 16), cuFFT working room (32).
+BYTES_PER_POINT_FP64 = 192
 FIXED_BYTES_PER_SOLVE = 4 << 20
 
 

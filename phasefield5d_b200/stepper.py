@@ -167,7 +167,8 @@ class Stepper:
 
     def step_save(self):
         """One step plus its save-step diagnostics (examples/simulate.py:299-354),
-        plain FP64 form: a dict with net, max_change, total_flux, mass,
+        either form (the FP32-compensated one reduces its field X0 + hi + lo,
+        dX/dt and mu/M in FP64): a dict with net, max_change, total_flux, mass,
         comp_min, comp_max, comp_var (arrays of 4), comp_fe_min, f_grad,
         xdotmax, dt, time (after the step), step (its index) and halted."""
         d = _lib.SaveDiag()

@@ -90,3 +90,24 @@ def test_driver_matches_oracle_loop(torch_cuda, tmp_path):
         a, b = np.array(tg[key]), np.array(tr[key])
         assert np.all(np.abs(a - b) <= RTOL * np.abs(b) + 1e-300), key
     st.close()
+
+
+@pytest.mark.parametrize("dim,shape", [(1, (96,)), (2, (24, 20)), (3, (8, 10, 12))])
+def test_step_save_fp32c_tracks_fp64(torch_cuda, dim, shape):
+    """The precision form's save-step diagnostics follow the FP64 form's
+    within the FP32c field tolerance (1e-6 relative) on the same steps."""
+    from phasefield5d_b200.stepper import Stepper
+    prob = _problem(dim, shape)
+    a = Stepper.from_problem(prob)
+    b = Stepper.from_problem(prob, precision="fp32c")
+    for k in range(3):
+        g = a.step_save()
+        f = b.step_save()
+        assert g["step"] == f["step"] == k and not f["halted"]
+        for key in ("mass", "comp_min", "comp_max", "max_change"):
+            assert _close(f[key], g[key], np.abs(g[key]), 1e-5), (key, f[key], g[key])
+        assert _close(f["comp_fe_min"], g["comp_fe_min"], 1.0, 1e-6)
+        assert _close(f["dt"], g["dt"], abs(g["dt"]), 1e-6)
+        assert np.all(np.isfinite(f["total_flux"])) and np.isfinite(f["f_grad"])
+    a.close()
+    b.close()

@@ -83,3 +83,33 @@ def test_fp64_backend_alone_equals_mix(torch_cuda):
         alone = alone_srv.finished[0]
         assert alone.final_state["step"] == mixed[r.rid].final_state["step"] == r.n_steps
         assert np.array_equal(alone.result, mixed[r.rid].result), r.rid
+
+
+def test_halting_and_cancelled_requests_leave_others_intact(torch_cuda):
+    """A request whose field is bad from the start halts at its first
+    out-of-bounds check and retires; another is cancelled while active.  The
+    remaining requests finish with the results they have alone."""
+    import copy
+    from phasefield5d_b200.serving import Server
+    reqs = _requests(steps=60)[:4]              # 1D, 2D, 3D, 1D
+    bad = copy.copy(reqs[1])
+    prob = copy.copy(bad.problem)
+    X = prob.X_init.copy()
+    X[2, 3, 1] = np.nan
+    prob.X_init = X
+    bad.problem = prob
+    reqs[1] = bad
+    srv = Server(step_block=10, reserve_bytes=0)
+    for r, a in zip([copy.copy(r) for r in reqs], [0.0, 0.0, 0.0, 0.0]):
+        r.arrival = a
+        srv.submit(r)
+    for _ in range(3):
+        srv.tick()
+    assert srv.cancel(reqs[2].rid)               # the 3D request, while active
+    srv.run(timeout=300)
+    status = {r.rid: r.status for r in srv.finished}
+    assert status == {0: "done", 1: "halted", 2: "cancelled", 3: "done"}
+    for rid in (0, 3):
+        alone_srv, _ = _serve([copy.copy(reqs[rid])], [0.0])
+        mixed = next(r for r in srv.finished if r.rid == rid)
+        assert np.array_equal(alone_srv.finished[0].result, mixed.result), rid
