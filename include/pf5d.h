@@ -217,7 +217,7 @@ pf5d_status pf5d_stepper_mass(pf5d_stepper *h, double *mean_out, void *stream);
 /* Diagnostics: launch one stage of a step by itself on `stream`
  * (PF5D_STAGE_*), so each kernel can be timed with events.  It changes the
  * stepper's state exactly as that stage does inside a step. */
-#define PF5D_STAGE_RATE 0        /* fused chemical potential + flux divergence */
+#define PF5D_STAGE_RATE 0        /* rate kernel(s) (mu/M + flux divergence) and the dt controller */
 #define PF5D_STAGE_UPDATE 1      /* update, clamp, next misfit, OOB test       */
 #define PF5D_STAGE_FFT_FWD 2     /* cuFFT D2Z of the misfit                    */
 #define PF5D_STAGE_BMUL 3        /* B(k) multiply                              */

@@ -107,6 +107,33 @@ def test_2d_512_adaptive_prefix_vs_oracle(torch_cuda):
     gpu.close()
 
 
+def test_2d_512_full_20k_vs_oracle_fixture(torch_cuda):
+    """All 20,000 adaptive steps of the 2D 512x512 workload against the
+    oracle's run of the same steps (tests/golden/full2d_20k.npz, written by
+    tests/golden/make_fullrun.py): the field at 4096 sample points and the
+    per-component minima / maxima within 1e-12 of max|X|, the per-component
+    sums and the final clock within 1e-12 relative."""
+    import os
+    from phasefield5d_b200 import workload as W
+    from phasefield5d_b200.stepper import Stepper
+    g = np.load(os.path.join(os.path.dirname(__file__), "golden", "full2d_20k.npz"))
+    prob = _problem(W.config_2d_adaptive)
+    assert prob.omega_seed == int(g["omega_seed"]) and bool(g["completed"])
+    gpu = Stepper.from_problem(prob)
+    state = gpu.run(int(g["steps"]))
+    X = gpu.X.cpu().numpy().reshape(-1, 4)
+    gpu.close()
+    scale = float(np.max(np.abs(g["maxs"])))
+    assert state["step"] == int(g["steps"]) and not state["halted"]
+    err = np.max(np.abs(X[g["idx"]] - g["X"]))
+    assert err <= FIELD_RTOL * scale, f"sampled field err {err:.2e}"
+    assert np.all(np.abs(X.min(axis=0) - g["mins"]) <= FIELD_RTOL * scale)
+    assert np.all(np.abs(X.max(axis=0) - g["maxs"]) <= FIELD_RTOL * scale)
+    assert np.all(np.abs(X.sum(axis=0) - g["sums"]) <= FIELD_RTOL * np.abs(g["sums"]))
+    assert state["time"] == pytest.approx(float(g["time"]), rel=1e-12)
+    assert state["dt"] == pytest.approx(float(g["dt"]), rel=1e-10)
+
+
 def test_2d_512_full_run_conserves_mass(torch_cuda):
     """All 20,000 adaptive steps on the GPU: the flux form conserves each
     component's mean (up to rounding), no halt, finite field."""
