@@ -149,7 +149,7 @@ struct BatchSmem {
   static constexpr size_t rate = head + (s2d > s1d ? s2d : s1d);
 };
 
-template <int TX, int TY, int MINB, bool WIN, bool SORT = false>
+template <int TX, int TY, int MINB, bool WIN, bool SORT = false, bool PP = false>
 __global__ void __launch_bounds__(TX * TY, MINB)
     kb_rate(const BSolve *__restrict__ solves, int nsolves, int total_tiles, double *tile_max) {
   constexpr int NT = TX * TY;
@@ -174,7 +174,8 @@ __global__ void __launch_bounds__(TX * TY, MINB)
     unsigned flags = 0;
     float vmax;
     if (B.dim == 2)
-      vmax = tile2d32_body<TX, TY, WIN, SORT>(P, local % B.ntx, local / B.ntx, work, &flags, tid);
+      vmax = tile2d32_body<TX, TY, WIN, SORT, false, PP>(P, local % B.ntx, local / B.ntx, work,
+                                                          &flags, tid);
     else
       vmax = tile1d32_body<NT>(B, P, local, reinterpret_cast<float *>(work), &flags, tid);
     if (flags) atomicOr(&P.st->flags, flags);
@@ -389,7 +390,7 @@ struct BatchVariant {
   int (*occupancy)();
 };
 
-template <int TX, int TY, int MINB, bool WIN, bool SORT = false>
+template <int TX, int TY, int MINB, bool WIN, bool SORT = false, bool PP = false>
 BatchVariant make_bvariant() {
   using SM = BatchSmem<TX, TY, SORT>;
   BatchVariant v;
@@ -399,17 +400,17 @@ BatchVariant make_bvariant() {
   v.win = WIN;
   v.smem = SM::rate;
   v.set_attrs = []() {
-    cudaFuncSetAttribute(kb_rate<TX, TY, MINB, WIN, SORT>,
+    cudaFuncSetAttribute(kb_rate<TX, TY, MINB, WIN, SORT, PP>,
                          cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SM::rate);
   };
   v.launch = [](int grid, cudaStream_t s, const BSolve *solves, int n, int tiles,
                 double *tile_max) {
-    launch_pdl(kb_rate<TX, TY, MINB, WIN, SORT>, dim3(grid), dim3(TX, TY), SM::rate, s, solves, n,
+    launch_pdl(kb_rate<TX, TY, MINB, WIN, SORT, PP>, dim3(grid), dim3(TX, TY), SM::rate, s, solves, n,
                tiles, tile_max);
   };
   v.occupancy = []() {
     int nb = 0;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, kb_rate<TX, TY, MINB, WIN, SORT>, TX * TY,
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, kb_rate<TX, TY, MINB, WIN, SORT, PP>, TX * TY,
                                                   SM::rate);
     return nb;
   };
@@ -422,7 +423,8 @@ const std::vector<BatchVariant> &batch_variants() {
       make_bvariant<32, 8, 2, false>(), make_bvariant<32, 8, 3, false>(),
       make_bvariant<32, 4, 4, true>(), make_bvariant<64, 4, 2, true>(),
       make_bvariant<32, 8, 2, false, true>(), make_bvariant<32, 8, 3, false, true>(),
-      make_bvariant<32, 16, 2, false, true>()};
+      make_bvariant<32, 16, 2, false, true>(), make_bvariant<32, 8, 3, false, false, true>(),
+      make_bvariant<32, 16, 2, false, false, true>(), make_bvariant<32, 8, 3, false, true, true>()};
   return v;
 }
 

@@ -171,26 +171,34 @@ __device__ __forceinline__ void chem32(const Rate32 &P, const float d[S], const 
 __device__ __forceinline__ void face_flux32(const Rate32 &P, const float Dc[S], const float Mc[NM],
                                             const float Dn[S], const float Mn[NM],
                                             const float g[S], float J[S]) {
+  // Every operation explicitly rounded: a face evaluated from either side
+  // (or in any kernel) gives the same bits, so the flux form conserves mass
+  // exactly even when the two cells of a face each evaluate it.
   float dm[S], xm[S], mm[NM], dk[S];
 #pragma unroll
   for (int a = 0; a < S; ++a) {
-    dm[a] = 0.5f * (Dc[a] + Dn[a]);
-    xm[a] = P.x0f[a] + dm[a];
+    dm[a] = __fmul_rn(0.5f, __fadd_rn(Dc[a], Dn[a]));
+    xm[a] = __fadd_rn(P.x0f[a], dm[a]);
   }
 #pragma unroll
-  for (int a = 0; a < NM; ++a) mm[a] = 0.5f * (Mc[a] + Mn[a]);
-  const double x_fe = P.c_fe - (((double)dm[0] + (double)dm[1]) + (double)dm[2] + (double)dm[3]);
-  const float w_fe = (float)x_fe * mm[0];
+  for (int a = 0; a < NM; ++a) mm[a] = __fmul_rn(0.5f, __fadd_rn(Mc[a], Mn[a]));
+  const double x_fe = __dsub_rn(P.c_fe, __dadd_rn(__dadd_rn(__dadd_rn((double)dm[0], (double)dm[1]),
+                                                           (double)dm[2]), (double)dm[3]));
+  const float w_fe = __fmul_rn((float)x_fe, mm[0]);
   float dot = 0.f;
 #pragma unroll
   for (int b = 0; b < S; ++b) dot = fmaf(xm[b], g[b], dot);
 #pragma unroll
-  for (int k = 0; k < S; ++k) dk[k] = g[k] - dot;
+  for (int k = 0; k < S; ++k) dk[k] = __fsub_rn(g[k], dot);
   float swk = 0.f;
 #pragma unroll
-  for (int k = 0; k < S; ++k) swk = fmaf(xm[k] * mm[1 + k], dk[k], swk);
+  for (int k = 0; k < S; ++k) swk = fmaf(__fmul_rn(xm[k], mm[1 + k]), dk[k], swk);
 #pragma unroll
-  for (int a = 0; a < S; ++a) J[a] = w_fe * xm[a] * dot + xm[a] * mm[1 + a] * dk[a] - xm[a] * swk;
+  for (int a = 0; a < S; ++a) {
+    const float t1 = __fmul_rn(__fmul_rn(w_fe, xm[a]), dot);
+    const float t2 = __fmul_rn(__fmul_rn(xm[a], mm[1 + a]), dk[a]);
+    J[a] = __fsub_rn(__fadd_rn(t1, t2), __fmul_rn(xm[a], swk));
+  }
 }
 
 // Fold this thread's max |dX/dt| into the block and store the block's max
@@ -243,7 +251,7 @@ __device__ __forceinline__ void face32_between(const Rate32 &P, const float *XL,
   for (int c = 0; c < S; ++c) {
     Dc[c] = XL[c * PX + pl];
     Dn[c] = XH[c * PX + ph];
-    g[c] = (MH[c * PM + qh] - ML[c * PM + ql]) * P.inv_dx;
+    g[c] = __fmul_rn(__fsub_rn(MH[c * PM + qh], ML[c * PM + ql]), P.inv_dx);
   }
 #pragma unroll
   for (int c = 0; c < NM; ++c) {
@@ -495,7 +503,7 @@ struct Tile2dSmem32 {
 
 // Evaluates tile (bx, by) of solve P and writes its dX/dt; returns this
 // thread's max |dX/dt|.  Ends with all threads past a barrier.
-template <int TX, int TY, bool WIN, bool SORT = false, bool SPLIT = false>
+template <int TX, int TY, bool WIN, bool SORT = false, bool SPLIT = false, bool PERPOINT = false>
 __device__ __forceinline__ float tile2d32_body(const Rate32 &P, int bx, int by, float4 *sm4,
                                                unsigned *flags, int tid) {
   using G = PlaneGeom<TX, TY>;
@@ -527,16 +535,34 @@ __device__ __forceinline__ float tile2d32_body(const Rate32 &P, int bx, int by, 
     mu_plane32<TX, TY, 2, WIN, SORT>(P, nullptr, Xs, nullptr, Ms, 0, wx, wy, false, win, wred,
                                      win_lo, flags, tid, ss);
   __syncthreads();
+  float vmax = 0.f;
+  if constexpr (PERPOINT) {
+    // each point evaluates its four faces (each face is evaluated by both of
+    // its cells, with identical operands and operation order)
+    if (x0 + tx < P.nx && y0 + ty < P.ny) {
+      const int pX = (ty + 2) * G::HX + (tx + 2), pM = (ty + 1) * G::MX + (tx + 1);
+      float jyp[S], jym[S], jxp[S], jxm[S], out[S];
+      face32_between<G::PX, G::PM>(P, Xs, Ms, pX, pM, Xs, Ms, pX + G::HX, pM + G::MX, jyp);
+      face32_between<G::PX, G::PM>(P, Xs, Ms, pX - G::HX, pM - G::MX, Xs, Ms, pX, pM, jym);
+      face32_between<G::PX, G::PM>(P, Xs, Ms, pX, pM, Xs, Ms, pX + 1, pM + 1, jxp);
+      face32_between<G::PX, G::PM>(P, Xs, Ms, pX - 1, pM - 1, Xs, Ms, pX, pM, jxm);
+#pragma unroll
+      for (int c = 0; c < S; ++c)
+        out[c] = __fmul_rn(__fadd_rn(__fsub_rn(jyp[c], jym[c]), __fsub_rn(jxp[c], jxm[c])),
+                           P.inv_dx);
+      store_rate(P.dX, (int64_t)(y0 + ty) * P.nx + (x0 + tx), out, vmax);
+    }
+    return vmax;                     // (shared memory still being read: callers sync first)
+  }
   plane_faces32<TX, TY>(P, Xs, Ms, Fx, Fy, tid);
   __syncthreads();
-  float vmax = 0.f;
   if (x0 + tx < P.nx && y0 + ty < P.ny) {
     float out[S];
 #pragma unroll
     for (int c = 0; c < S; ++c) {
-      const float a = (Fy[c * G::NFY + (ty + 1) * TX + tx] - Fy[c * G::NFY + ty * TX + tx]) +
-                      (Fx[c * G::NFX + ty * (TX + 1) + tx + 1] - Fx[c * G::NFX + ty * (TX + 1) + tx]);
-      out[c] = a * P.inv_dx;
+      const float ay = __fsub_rn(Fy[c * G::NFY + (ty + 1) * TX + tx], Fy[c * G::NFY + ty * TX + tx]);
+      const float ax = __fsub_rn(Fx[c * G::NFX + ty * (TX + 1) + tx + 1], Fx[c * G::NFX + ty * (TX + 1) + tx]);
+      out[c] = __fmul_rn(__fadd_rn(ay, ax), P.inv_dx);
     }
     store_rate(P.dX, (int64_t)(y0 + ty) * P.nx + (x0 + tx), out, vmax);
   }

@@ -40,15 +40,16 @@ namespace pf5d {
 // Rate kernels (same tiling as the FP64 kernels)
 // ------------------------------------------------------------------------
 
-template <int TX, int TY, int MINB, bool WIN, bool SORT = false, bool SPLIT = false>
+template <int TX, int TY, int MINB, bool WIN, bool SORT = false, bool SPLIT = false,
+          bool PERPOINT = false>
 __global__ void __launch_bounds__(TX * TY, MINB) k32_rate_tile2d(Rate32 P) {
   pdl_wait();
   if (P.st->halt) return;
   extern __shared__ float4 sm4[];
   const int tid = threadIdx.y * TX + threadIdx.x;
   unsigned flags = 0;
-  const float vmax =
-      tile2d32_body<TX, TY, WIN, SORT, SPLIT>(P, blockIdx.x, blockIdx.y, sm4, &flags, tid);
+  const float vmax = tile2d32_body<TX, TY, WIN, SORT, SPLIT, PERPOINT>(P, blockIdx.x, blockIdx.y,
+                                                                      sm4, &flags, tid);
   if (flags) atomicOr(&P.st->flags, flags);
   finish_rate32(P, vmax, Tile2dSmem32<TX, TY, SORT>::red(sm4));
 }
@@ -146,10 +147,10 @@ __global__ void __launch_bounds__(TX * TY, MINB) k32_rate_march3d(Rate32 P, int 
       float out[S];
 #pragma unroll
       for (int c = 0; c < S; ++c) {
-        const float a = (Jz[c] - Jm[c]) +
-                        (Fy[c * G::NFY + (ty + 1) * TX + tx] - Fy[c * G::NFY + ty * TX + tx]) +
-                        (Fx[c * G::NFX + ty * (TX + 1) + tx + 1] - Fx[c * G::NFX + ty * (TX + 1) + tx]);
-        out[c] = a * P.inv_dx;
+        const float ay = __fsub_rn(Fy[c * G::NFY + (ty + 1) * TX + tx], Fy[c * G::NFY + ty * TX + tx]);
+        const float ax = __fsub_rn(Fx[c * G::NFX + ty * (TX + 1) + tx + 1],
+                                   Fx[c * G::NFX + ty * (TX + 1) + tx]);
+        out[c] = __fmul_rn(__fadd_rn(__fadd_rn(__fsub_rn(Jz[c], Jm[c]), ay), ax), P.inv_dx);
       }
       store_rate(P.dX, (int64_t)z * plane + (int64_t)(y0 + ty) * P.nx + (x0 + tx), out, vmax);
     }
@@ -488,7 +489,7 @@ __device__ __forceinline__ void copy_plane_async32(const Rate32 &P, int64_t zoff
 // a plane tile marching along axis 0, mu/M read from P.mm.  The copies of
 // plane z+2 are in flight while plane z is evaluated (three-slot rings for
 // X and mu/M).  Same face routine and divergence order as k32_rate_march3d.
-template <int TX, int TY, int MINB>
+template <int TX, int TY, int MINB, bool PERPOINT = false>
 __global__ void __launch_bounds__(TX * TY, MINB) k32_flux_march3d(Rate32 P, int zc) {
   using G = PlaneGeom<TX, TY>;
   pdl_wait();
@@ -538,16 +539,33 @@ __global__ void __launch_bounds__(TX * TY, MINB) k32_flux_march3d(Rate32 P, int 
     float Jz[S];
     face32_between<G::PX, G::PM>(P, xplane(z), mplane(z), pX, pM, xplane(z + 1), mplane(z + 1),
                                  pX, pM, Jz);
-    plane_faces32<TX, TY>(P, xplane(z), mplane(z), Fx, Fy, tid);
-    __syncthreads();
+    float jyp[S], jym[S], jxp[S], jxm[S];
+    if constexpr (PERPOINT) {
+      // each point evaluates its four in-plane faces (each face by both of
+      // its cells, identical operands and order): no face buffers, no barrier
+      const float *Xp = xplane(z), *Mp = mplane(z);
+      face32_between<G::PX, G::PM>(P, Xp, Mp, pX, pM, Xp, Mp, pX + G::HX, pM + G::MX, jyp);
+      face32_between<G::PX, G::PM>(P, Xp, Mp, pX - G::HX, pM - G::MX, Xp, Mp, pX, pM, jym);
+      face32_between<G::PX, G::PM>(P, Xp, Mp, pX, pM, Xp, Mp, pX + 1, pM + 1, jxp);
+      face32_between<G::PX, G::PM>(P, Xp, Mp, pX - 1, pM - 1, Xp, Mp, pX, pM, jxm);
+    } else {
+      plane_faces32<TX, TY>(P, xplane(z), mplane(z), Fx, Fy, tid);
+      __syncthreads();
+#pragma unroll
+      for (int c = 0; c < S; ++c) {
+        jyp[c] = Fy[c * G::NFY + (ty + 1) * TX + tx];
+        jym[c] = Fy[c * G::NFY + ty * TX + tx];
+        jxp[c] = Fx[c * G::NFX + ty * (TX + 1) + tx + 1];
+        jxm[c] = Fx[c * G::NFX + ty * (TX + 1) + tx];
+      }
+    }
     if (in_tile) {
       float out[S];
 #pragma unroll
       for (int c = 0; c < S; ++c) {
-        const float a = (Jz[c] - Jm[c]) +
-                        (Fy[c * G::NFY + (ty + 1) * TX + tx] - Fy[c * G::NFY + ty * TX + tx]) +
-                        (Fx[c * G::NFX + ty * (TX + 1) + tx + 1] - Fx[c * G::NFX + ty * (TX + 1) + tx]);
-        out[c] = a * P.inv_dx;
+        const float a = __fadd_rn(__fadd_rn(__fsub_rn(Jz[c], Jm[c]), __fsub_rn(jyp[c], jym[c])),
+                                  __fsub_rn(jxp[c], jxm[c]));
+        out[c] = __fmul_rn(a, P.inv_dx);
       }
       store_rate(P.dX, (int64_t)z * plane + (int64_t)(y0 + ty) * P.nx + (x0 + tx), out, vmax);
     }
@@ -625,7 +643,7 @@ struct Variant32 {
   void (*launch3d)(dim3, dim3, size_t, cudaStream_t, const Rate32 &, int);
 };
 
-template <int TX, int TY, int MINB, bool WIN = true, bool SORT = false>
+template <int TX, int TY, int MINB, bool WIN = true, bool SORT = false, bool PP = false>
 Variant32 make_variant32() {
   Variant32 v;
   v.tx = TX;
@@ -636,13 +654,13 @@ Variant32 make_variant32() {
   v.smem3d = march3d32_smem<TX, TY, SORT>();
   v.set_attrs = []() {
     const auto a = cudaFuncAttributeMaxDynamicSharedMemorySize;
-    cudaFuncSetAttribute(k32_rate_tile2d<TX, TY, MINB, WIN, SORT>, a,
+    cudaFuncSetAttribute(k32_rate_tile2d<TX, TY, MINB, WIN, SORT, false, PP>, a,
                          (int)tile2d32_smem<TX, TY, SORT>());
     cudaFuncSetAttribute(k32_rate_march3d<TX, TY, MINB, WIN, SORT>, a,
                          (int)march3d32_smem<TX, TY, SORT>());
   };
   v.launch2d = [](dim3 g, dim3 b, size_t sm, cudaStream_t s, const Rate32 &P) {
-    launch_pdl(k32_rate_tile2d<TX, TY, MINB, WIN, SORT>, g, b, sm, s, P);
+    launch_pdl(k32_rate_tile2d<TX, TY, MINB, WIN, SORT, false, PP>, g, b, sm, s, P);
   };
   v.launch3d = [](dim3 g, dim3 b, size_t sm, cudaStream_t s, const Rate32 &P, int zc) {
     launch_pdl(k32_rate_march3d<TX, TY, MINB, WIN, SORT>, g, b, sm, s, P, zc);
@@ -652,7 +670,7 @@ Variant32 make_variant32() {
 
 // Split variant: k32_chem over all points, then the tile / marching kernel
 // reading mu/M back.
-template <int TX, int TY, int MINB, int KMINB>
+template <int TX, int TY, int MINB, int KMINB, bool PP = false>
 Variant32 make_split_variant32() {
   Variant32 v;
   v.tx = TX;
@@ -665,7 +683,7 @@ Variant32 make_split_variant32() {
     const auto a = cudaFuncAttributeMaxDynamicSharedMemorySize;
     cudaFuncSetAttribute(k32_rate_tile2d<TX, TY, MINB, false, false, true>, a,
                          (int)tile2d32_smem<TX, TY>());
-    cudaFuncSetAttribute(k32_flux_march3d<TX, TY, MINB>, a, (int)flux_march3d32_smem<TX, TY>());
+    cudaFuncSetAttribute(k32_flux_march3d<TX, TY, MINB, PP>, a, (int)flux_march3d32_smem<TX, TY>());
   };
   v.launch2d = [](dim3 g, dim3 b, size_t sm, cudaStream_t s, const Rate32 &P) {
     launch_chem32<2, KMINB>(s, P);
@@ -673,7 +691,7 @@ Variant32 make_split_variant32() {
   };
   v.launch3d = [](dim3 g, dim3 b, size_t sm, cudaStream_t s, const Rate32 &P, int zc) {
     launch_chem32<3, KMINB>(s, P);
-    launch_pdl(k32_flux_march3d<TX, TY, MINB>, g, b, sm, s, P, zc);
+    launch_pdl(k32_flux_march3d<TX, TY, MINB, PP>, g, b, sm, s, P, zc);
   };
   return v;
 }
@@ -686,7 +704,10 @@ const std::vector<Variant32> &variants32() {
       make_variant32<32, 8, 2, true, true>(), make_variant32<32, 8, 3, false, true>(),
       make_variant32<32, 16, 2, false, true>(), make_variant32<32, 8, 2, false, true>(),
       make_split_variant32<32, 8, 3, 3>(), make_split_variant32<32, 16, 2, 3>(),
-      make_split_variant32<32, 8, 4, 4>(), make_split_variant32<32, 16, 2, 4>()};
+      make_split_variant32<32, 8, 4, 4>(), make_split_variant32<32, 16, 2, 4>(),
+      make_variant32<32, 8, 3, false, true, true>(), make_variant32<32, 16, 2, false, true, true>(),
+      make_variant32<32, 8, 3, false, false, true>(), make_variant32<32, 16, 2, false, false, true>(),
+      make_split_variant32<32, 8, 4, 4, true>(), make_split_variant32<32, 16, 2, 4, true>()};
   return v;
 }
 
