@@ -497,7 +497,7 @@ __device__ __forceinline__ void load_plane(const double *__restrict__ X, int64_t
 // NTH >= the mu/M position count every position takes one pass).  SORT:
 // mu/M positions evaluated in table-cell order.
 template <int TX, int TY, int MINB, bool VEC, bool WIN, bool SPLIT = false, int NTH = TX * TY,
-          bool SORT = false>
+          bool SORT = false, bool PERPOINT = false>
 __global__ void __launch_bounds__(NTH, MINB) k_rate_tile2d(RateParams P) {
   using G = PlaneGeom<TX, TY, NTH>;
   static_assert(NTH >= TX * TY && NTH % 32 == 0, "one thread per tile point at least");
@@ -539,16 +539,39 @@ __global__ void __launch_bounds__(NTH, MINB) k_rate_tile2d(RateParams P) {
                                                reinterpret_cast<double2 *>(Fx), win_lo, &flags,
                                                tid, ss);
   __syncthreads();
-  plane_faces<TX, TY, NTH>(Xs, Ms, Fx, Fy, P.inv_dx, tid);
-  __syncthreads();
+  double jyp[S], jym[S], jxp[S], jxm[S];
+  const bool mine = tid < TX * TY && x0 + tx < P.nx && y0 + ty < P.ny;
+  if constexpr (PERPOINT) {
+    // each point evaluates its four faces from the shared planes (each face
+    // by both of its cells, with identical operands and operation order)
+    if (mine) {
+      const int pX = (ty + 2) * G::HX + (tx + 2), pM = (ty + 1) * G::MX + (tx + 1);
+      face_between<G::PX, G::PM>(Xs, Ms, pX, pM, Xs, Ms, pX + G::HX, pM + G::MX, P.inv_dx, jyp);
+      face_between<G::PX, G::PM>(Xs, Ms, pX - G::HX, pM - G::MX, Xs, Ms, pX, pM, P.inv_dx, jym);
+      face_between<G::PX, G::PM>(Xs, Ms, pX, pM, Xs, Ms, pX + 1, pM + 1, P.inv_dx, jxp);
+      face_between<G::PX, G::PM>(Xs, Ms, pX - 1, pM - 1, Xs, Ms, pX, pM, P.inv_dx, jxm);
+    }
+  } else {
+    plane_faces<TX, TY, NTH>(Xs, Ms, Fx, Fy, P.inv_dx, tid);
+    __syncthreads();
+    if (mine) {
+#pragma unroll
+      for (int c = 0; c < S; ++c) {
+        jyp[c] = Fy[c * G::NFY + (ty + 1) * TX + tx];
+        jym[c] = Fy[c * G::NFY + ty * TX + tx];
+        jxp[c] = Fx[c * G::NFX + ty * (TX + 1) + tx + 1];
+        jxm[c] = Fx[c * G::NFX + ty * (TX + 1) + tx];
+      }
+    }
+  }
   double vmax = 0.0;
-  if (tid < TX * TY && x0 + tx < P.nx && y0 + ty < P.ny) {
+  if (mine) {
     double out[S];
 #pragma unroll
     for (int c = 0; c < S; ++c) {
-      double a = Fy[c * G::NFY + (ty + 1) * TX + tx] - Fy[c * G::NFY + ty * TX + tx];
-      a = a + Fx[c * G::NFX + ty * (TX + 1) + tx + 1];
-      a = a - Fx[c * G::NFX + ty * (TX + 1) + tx];
+      double a = jyp[c] - jym[c];
+      a = a + jxp[c];
+      a = a - jxm[c];
       out[c] = a * P.inv_dx;
       const double v = fabs(out[c]);
       if (v > vmax) vmax = v;
@@ -998,7 +1021,8 @@ struct RateVariant {
 
 // NTH shapes the 2D kernel only (the 3D marching kernel has one thread per
 // tile point); SORT applies to both.
-template <int TX, int TY, int MINB, bool WIN = true, int NTH = TX * TY, bool SORT = false>
+template <int TX, int TY, int MINB, bool WIN = true, int NTH = TX * TY, bool SORT = false,
+          bool PP = false>
 RateVariant make_variant() {
   RateVariant v;
   v.tx = TX;
@@ -1013,16 +1037,16 @@ RateVariant make_variant() {
     const int s2 = (int)tile2d_smem<TX, TY, NTH, SORT>(), s3 = (int)march3d_smem<TX, TY, SORT>();
     const auto a = cudaFuncAttributeMaxDynamicSharedMemorySize;
     if (vec) {
-      cudaFuncSetAttribute(k_rate_tile2d<TX, TY, MINB, true, WIN, false, NTH, SORT>, a, s2);
+      cudaFuncSetAttribute(k_rate_tile2d<TX, TY, MINB, true, WIN, false, NTH, SORT, PP>, a, s2);
       cudaFuncSetAttribute(k_rate_march3d<TX, TY, MINB, true, WIN, false, SORT>, a, s3);
     } else {
-      cudaFuncSetAttribute(k_rate_tile2d<TX, TY, MINB, false, WIN, false, NTH, SORT>, a, s2);
+      cudaFuncSetAttribute(k_rate_tile2d<TX, TY, MINB, false, WIN, false, NTH, SORT, PP>, a, s2);
       cudaFuncSetAttribute(k_rate_march3d<TX, TY, MINB, false, WIN, false, SORT>, a, s3);
     }
   };
   v.launch2d = [](bool vec, dim3 g, dim3 b, size_t sm, cudaStream_t s, const RateParams &P) {
-    if (vec) launch_pdl(k_rate_tile2d<TX, TY, MINB, true, WIN, false, NTH, SORT>, g, b, sm, s, P);
-    else launch_pdl(k_rate_tile2d<TX, TY, MINB, false, WIN, false, NTH, SORT>, g, b, sm, s, P);
+    if (vec) launch_pdl(k_rate_tile2d<TX, TY, MINB, true, WIN, false, NTH, SORT, PP>, g, b, sm, s, P);
+    else launch_pdl(k_rate_tile2d<TX, TY, MINB, false, WIN, false, NTH, SORT, PP>, g, b, sm, s, P);
   };
   v.launch3d = [](bool vec, dim3 g, dim3 b, size_t sm, cudaStream_t s, const RateParams &P,
                   int zc) {
@@ -1080,7 +1104,9 @@ const std::vector<RateVariant> &rate_variants() {
       make_split_variant<32, 8, 3, 4>(), make_split_variant<32, 4, 4, 4>(),
       make_variant<32, 8, 2, true, 352, true>(), make_variant<32, 8, 2, false, 352, true>(),
       make_variant<32, 8, 2, true, 352, false>(), make_variant<32, 4, 4, true, 224, true>(),
-      make_variant<32, 4, 4, false, 224, true>(), make_variant<32, 16, 1, false, 608, true>()};
+      make_variant<32, 4, 4, false, 224, true>(), make_variant<32, 16, 1, false, 608, true>(),
+      make_variant<32, 8, 2, false, 352, true, true>(), make_variant<32, 8, 2, true, 352, false, true>(),
+      make_variant<32, 8, 3, false, 256, false, true>(), make_variant<64, 4, 2, true, 256, false, true>()};
   return v;
 }
 
