@@ -636,7 +636,8 @@ struct March64Geom {
   static constexpr int NFMAX = G::NFX > G::NFY ? G::NFX : G::NFY;
 };
 
-template <int TX, int TY, int MINB, bool VEC, bool WIN, bool SPLIT = false, bool SORT = false>
+template <int TX, int TY, int MINB, bool VEC, bool WIN, bool SPLIT = false, bool SORT = false,
+          bool PERPOINT = false>
 __global__ void __launch_bounds__(TX * TY, MINB) k_rate_march3d(RateParams P, int zc) {
   using G = PlaneGeom<TX, TY>;
   pdl_wait();
@@ -730,6 +731,33 @@ __global__ void __launch_bounds__(TX * TY, MINB) k_rate_march3d(RateParams P, in
       const double jz = a[c];
       a[c] = jz - Jm[c];
       Jm[c] = jz;
+    }
+    if constexpr (PERPOINT) {
+      // each point evaluates its four in-plane faces (each face by both of
+      // its cells, identical operands and order): no face buffer, no barriers
+      if (in_tile) {
+        const double *Xp = xplane(z), *Mp = mplane(z);
+        double jyp[S], jym[S], jxp[S], jxm[S], out[S];
+        face_between<G::PX, G::PM>(Xp, Mp, pX, pM, Xp, Mp, pX + G::HX, pM + G::MX, P.inv_dx, jyp);
+        face_between<G::PX, G::PM>(Xp, Mp, pX - G::HX, pM - G::MX, Xp, Mp, pX, pM, P.inv_dx, jym);
+        face_between<G::PX, G::PM>(Xp, Mp, pX, pM, Xp, Mp, pX + 1, pM + 1, P.inv_dx, jxp);
+        face_between<G::PX, G::PM>(Xp, Mp, pX - 1, pM - 1, Xp, Mp, pX, pM, P.inv_dx, jxm);
+#pragma unroll
+        for (int c = 0; c < S; ++c) {
+          double v = a[c] + jyp[c];
+          v = v - jym[c];
+          v = v + jxp[c];
+          v = v - jxm[c];
+          out[c] = v * P.inv_dx;
+          const double m = fabs(out[c]);
+          if (m > vmax) vmax = m;
+        }
+        const int64_t g = (int64_t)z * plane + (int64_t)(y0 + ty) * P.nx + (x0 + tx);
+        double2 *o = reinterpret_cast<double2 *>(P.dX + 4 * g);
+        o[0] = make_double2(out[0], out[1]);
+        o[1] = make_double2(out[2], out[3]);
+      }
+      continue;
     }
     plane_faces_axis<TX, TY, 1>(xplane(z), mplane(z), F, P.inv_dx, tid);
     __syncthreads();
@@ -1038,10 +1066,10 @@ RateVariant make_variant() {
     const auto a = cudaFuncAttributeMaxDynamicSharedMemorySize;
     if (vec) {
       cudaFuncSetAttribute(k_rate_tile2d<TX, TY, MINB, true, WIN, false, NTH, SORT, PP>, a, s2);
-      cudaFuncSetAttribute(k_rate_march3d<TX, TY, MINB, true, WIN, false, SORT>, a, s3);
+      cudaFuncSetAttribute(k_rate_march3d<TX, TY, MINB, true, WIN, false, SORT, PP>, a, s3);
     } else {
       cudaFuncSetAttribute(k_rate_tile2d<TX, TY, MINB, false, WIN, false, NTH, SORT, PP>, a, s2);
-      cudaFuncSetAttribute(k_rate_march3d<TX, TY, MINB, false, WIN, false, SORT>, a, s3);
+      cudaFuncSetAttribute(k_rate_march3d<TX, TY, MINB, false, WIN, false, SORT, PP>, a, s3);
     }
   };
   v.launch2d = [](bool vec, dim3 g, dim3 b, size_t sm, cudaStream_t s, const RateParams &P) {
@@ -1050,8 +1078,8 @@ RateVariant make_variant() {
   };
   v.launch3d = [](bool vec, dim3 g, dim3 b, size_t sm, cudaStream_t s, const RateParams &P,
                   int zc) {
-    if (vec) launch_pdl(k_rate_march3d<TX, TY, MINB, true, WIN, false, SORT>, g, b, sm, s, P, zc);
-    else launch_pdl(k_rate_march3d<TX, TY, MINB, false, WIN, false, SORT>, g, b, sm, s, P, zc);
+    if (vec) launch_pdl(k_rate_march3d<TX, TY, MINB, true, WIN, false, SORT, PP>, g, b, sm, s, P, zc);
+    else launch_pdl(k_rate_march3d<TX, TY, MINB, false, WIN, false, SORT, PP>, g, b, sm, s, P, zc);
   };
   return v;
 }
@@ -1064,7 +1092,7 @@ void launch_chem(bool vec, cudaStream_t s, const RateParams &P) {
   else launch_pdl(k_chem64<DIM, false, KMINB>, g, b, 0, s, P);
 }
 
-template <int TX, int TY, int MINB, int KMINB>
+template <int TX, int TY, int MINB, int KMINB, bool PP = false>
 RateVariant make_split_variant() {
   RateVariant v;
   v.tx = TX;
@@ -1079,7 +1107,7 @@ RateVariant make_split_variant() {
     const auto a = cudaFuncAttributeMaxDynamicSharedMemorySize;
     cudaFuncSetAttribute(k_rate_tile2d<TX, TY, MINB, true, false, true>, a,
                          (int)tile2d_smem<TX, TY>());
-    cudaFuncSetAttribute(k_rate_march3d<TX, TY, MINB, true, false, true>, a,
+    cudaFuncSetAttribute(k_rate_march3d<TX, TY, MINB, true, false, true, false, PP>, a,
                          (int)march3d_smem<TX, TY>());
   };
   v.launch2d = [](bool vec, dim3 g, dim3 b, size_t sm, cudaStream_t s, const RateParams &P) {
@@ -1089,7 +1117,7 @@ RateVariant make_split_variant() {
   v.launch3d = [](bool vec, dim3 g, dim3 b, size_t sm, cudaStream_t s, const RateParams &P,
                   int zc) {
     launch_chem<3, KMINB>(vec, s, P);
-    launch_pdl(k_rate_march3d<TX, TY, MINB, true, false, true>, g, b, sm, s, P, zc);
+    launch_pdl(k_rate_march3d<TX, TY, MINB, true, false, true, false, PP>, g, b, sm, s, P, zc);
   };
   return v;
 }
@@ -1106,7 +1134,8 @@ const std::vector<RateVariant> &rate_variants() {
       make_variant<32, 8, 2, true, 352, false>(), make_variant<32, 4, 4, true, 224, true>(),
       make_variant<32, 4, 4, false, 224, true>(), make_variant<32, 16, 1, false, 608, true>(),
       make_variant<32, 8, 2, false, 352, true, true>(), make_variant<32, 8, 2, true, 352, false, true>(),
-      make_variant<32, 8, 3, false, 256, false, true>(), make_variant<64, 4, 2, true, 256, false, true>()};
+      make_variant<32, 8, 3, false, 256, false, true>(), make_variant<64, 4, 2, true, 256, false, true>(),
+      make_split_variant<32, 8, 3, 3, true>(), make_split_variant<32, 4, 4, 3, true>()};
   return v;
 }
 
