@@ -7,12 +7,22 @@ the whole field.  The composition field, rates and FFT buffers of this
 workload fit in L2, so L2 is flushed (a 256 MiB write) between timed steps
 and each step is timed alone with CUDA events on the launching stream.
 
-Prints one JSON line.  ``--impl reference`` times the reference algorithm's
-CPU implementation (the oracle restatement of the Numba kernels + scipy FFT,
-all host threads) on the same workload and prints the same line with
-"impl": "reference".  Under torchrun every rank runs an independent replica
-(the path has no cross-solve exchange); value = all ranks' grid-point steps
-/ the slowest rank's time.
+Prints one JSON line.  Beside the headline it carries the rate stage's
+roofline (algorithmic bytes over CUDA-event time, against the measured HBM
+copy peak, with the DRAM traffic of the committed ncu capture), the per-stage
+times, an end-to-end figure through the C ABI with the field copied in from
+and out to pinned host memory every step, a CPU baseline (the oracle on a
+bounded sample of the same workload), the SM clocks sampled during the timed
+region, and -- at N=1, unless ``--forms none`` -- the other forms:
+``forms.fp32c_same_workload`` (precision form + its accuracy report),
+``forms.batch64`` (the 64-solve batched form against 64 plain FP64 steppers)
+and ``forms.serving`` (p50/p99 time to solution at several Poisson rates).
+
+``--impl reference`` times the reference algorithm's CPU implementation (the
+oracle restatement of the Numba kernels + scipy FFT, all host threads) on the
+same workload and prints the same line with "impl": "reference".  Under
+torchrun every rank runs an independent replica (the path has no cross-solve
+exchange); value = all ranks' grid-point steps / the slowest rank's time.
 """
 from __future__ import annotations
 

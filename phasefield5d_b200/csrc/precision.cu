@@ -59,7 +59,7 @@ constexpr size_t tile2d32_smem() {
   return Tile2dSmem32<TX, TY, SORT>::bytes;
 }
 
-template <int TX, int TY, int MINB, bool WIN, bool SORT = false, bool SPLIT = false>
+template <int TX, int TY, int MINB, bool WIN, bool SORT = false>
 __global__ void __launch_bounds__(TX * TY, MINB) k32_rate_march3d(Rate32 P, int zc) {
   using G = PlaneGeom<TX, TY>;
   pdl_wait();
@@ -94,34 +94,23 @@ __global__ void __launch_bounds__(TX * TY, MINB) k32_rate_march3d(Rate32 P, int 
     load_plane32<TX, TY>(P.D, (int64_t)wrap_any(z, P.nz) * plane, wx, wy, P.nx, xplane(z), tid);
   };
   auto compute_mu = [&](int z, bool interior_only) {
-    if constexpr (SPLIT)
-      load_mu_plane32<TX, TY>(P, (int64_t)wrap_any(z, P.nz) * plane, wx, wy, interior_only,
-                              mplane(z), tid);
-    else
-      mu_plane32<TX, TY, 3, WIN, SORT>(P, xplane(z - 1), xplane(z), xplane(z + 1), mplane(z),
-                                       (int64_t)wrap_any(z, P.nz) * plane, wx, wy, interior_only,
-                                       win, wred, win_lo, &flags, tid, ss);
+    mu_plane32<TX, TY, 3, WIN, SORT>(P, xplane(z - 1), xplane(z), xplane(z + 1), mplane(z),
+                                     (int64_t)wrap_any(z, P.nz) * plane, wx, wy, interior_only,
+                                     win, wred, win_lo, &flags, tid, ss);
   };
   const int pX = (ty + 2) * G::HX + (tx + 2);
   const int pM = (ty + 1) * G::MX + (tx + 1);
   const bool in_tile = (x0 + tx < P.nx) && (y0 + ty < P.ny);
   __syncthreads();
-  if constexpr (SPLIT) {          // faces need X and mu/M of planes z and z+1 only
-    load_x(zb - 1);
-    load_x(zb);
-    compute_mu(zb - 1, true);
-    compute_mu(zb, false);
-  } else {
-    load_x(zb - 2);
-    load_x(zb - 1);
-    load_x(zb);
-    __syncthreads();
-    compute_mu(zb - 1, true);
-    __syncthreads();
-    load_x(zb + 1);
-    __syncthreads();
-    compute_mu(zb, false);
-  }
+  load_x(zb - 2);
+  load_x(zb - 1);
+  load_x(zb);
+  __syncthreads();
+  compute_mu(zb - 1, true);
+  __syncthreads();
+  load_x(zb + 1);
+  __syncthreads();
+  compute_mu(zb, false);
   __syncthreads();
   float Jm[S];
   face32_between<G::PX, G::PM>(P, xplane(zb - 1), mplane(zb - 1), pX, pM, xplane(zb), mplane(zb),
@@ -129,14 +118,9 @@ __global__ void __launch_bounds__(TX * TY, MINB) k32_rate_march3d(Rate32 P, int 
   float vmax = 0.f;
   for (int z = zb; z < ze; ++z) {
     __syncthreads();
-    if constexpr (SPLIT) {
-      load_x(z + 1);
-      compute_mu(z + 1, false);
-    } else {
-      load_x(z + 2);
-      __syncthreads();
-      compute_mu(z + 1, false);
-    }
+    load_x(z + 2);
+    __syncthreads();
+    compute_mu(z + 1, false);
     __syncthreads();
     float Jz[S];
     face32_between<G::PX, G::PM>(P, xplane(z), mplane(z), pX, pM, xplane(z + 1), mplane(z + 1),

@@ -2,16 +2,21 @@
 
 Requests (a ``workload.Problem`` plus a step count) arrive over time.  The
 server admits them while batch slots and free HBM allow, keeps their fields
-and the temperature tables resident on the device, and advances all admitted
-solves together in step blocks:
+and the temperature tables resident on the device, and advances them in
+step blocks on device units that run independently -- each unit takes its
+next block as soon as its own last one is done, so a small request is never
+held by a large one's block:
 
-* 1D and 2D solves share one batched stepper (``batch.BatchStepper``);
+* 1D and 2D solves share one batched stepper (``batch.BatchStepper``), one
+  unit;
   whenever membership changes (a request admitted, finished, halted or
   cancelled) the batch is rebuilt and every continuing solve resumes its
   exact FP32 state (hi/lo pair, dt, time, step), so a request's trajectory
   does not depend on when others come and go;
 * 3D solves each get their own FP32-compensated ``Stepper`` on their own
-  stream, so their work overlaps the batch on the device.
+  stream (one unit each), so their work overlaps the batch on the device;
+* the device tables of each temperature are built once and shared by the
+  batch and the 3D steppers.
 
 ``GpuBackend(precision="fp64")`` is the plain-FP64 comparison: every request
 gets its own bit-faithful FP64 ``Stepper`` on its own stream (the FP64 form
@@ -320,16 +325,6 @@ class GpuBackend:
                                                table_cache=self.tables)
             self.fresh = True
 
-    def advance(self, blocks):
-        if self.batch is not None and self.batch_ids:
-            n = blocks[self.batch_ids[0]]
-            if n > 0:
-                self.batch.advance(n)
-        for rid, st in self.steppers.items():
-            if blocks.get(rid, 0) > 0:
-                st.advance(blocks[rid])
-        self.torch.cuda.synchronize()
-
     # -- asynchronous protocol: every unit runs its own blocks -------------
     def busy(self):
         """Request ids whose unit has a block not yet reported by poll."""
@@ -379,7 +374,17 @@ class GpuBackend:
                 return out
             time.sleep(0.0002)
 
-    # -- synchronous protocol ----------------------------------------------
+    # -- synchronous protocol (every block waits for all units) -------------
+    def advance(self, blocks):
+        if self.batch is not None and self.batch_ids:
+            n = blocks[self.batch_ids[0]]
+            if n > 0:
+                self.batch.advance(n)
+        for rid, st in self.steppers.items():
+            if blocks.get(rid, 0) > 0:
+                st.advance(blocks[rid])
+        self.torch.cuda.synchronize()
+
     def states(self):
         out = {}
         if self.batch is not None:
