@@ -151,14 +151,15 @@ struct BatchSmem {
 
 template <int TX, int TY, int MINB, bool WIN, bool SORT = false, bool PP = false>
 __global__ void __launch_bounds__(TX * TY, MINB)
-    kb_rate(const BSolve *__restrict__ solves, int nsolves, int total_tiles, double *tile_max) {
+    kb_rate(const BSolve *__restrict__ solves, int nsolves, int tile_begin, int tile_end,
+            double *tile_max) {
   constexpr int NT = TX * TY;
   extern __shared__ float4 sm4[];
   Rate32 *Rs = reinterpret_cast<Rate32 *>(sm4);
   float4 *work = sm4 + BatchSmem<TX, TY, SORT>::head / 16;
   const int tid = threadIdx.y * TX + threadIdx.x;
   pdl_wait();
-  for (int t = blockIdx.x; t < total_tiles; t += gridDim.x) {
+  for (int t = tile_begin + blockIdx.x; t < tile_end; t += gridDim.x) {
     const int si = find_solve_tile(solves, nsolves, t);
     const BSolve &B = solves[si];
     __syncthreads();                               // previous tile done with shared memory
@@ -186,11 +187,11 @@ __global__ void __launch_bounds__(TX * TY, MINB)
 }
 
 __global__ void __launch_bounds__(kUpdThreads)
-    kb_update(const BSolve *__restrict__ solves, int nsolves, int total_chunks) {
+    kb_update(const BSolve *__restrict__ solves, int nsolves, int chunk_begin, int chunk_end) {
   __shared__ double red[kUpdThreads / 32];
   const int tid = threadIdx.x;
   pdl_wait();
-  for (int cidx = blockIdx.x; cidx < total_chunks; cidx += gridDim.x) {
+  for (int cidx = chunk_begin + blockIdx.x; cidx < chunk_end; cidx += gridDim.x) {
     const BSolve &B = solves[find_solve_chunk(solves, nsolves, cidx)];
     StepState32 *st = B.R.st;
     if (st->halt) continue;
@@ -385,8 +386,8 @@ struct BatchVariant {
   bool win;
   size_t smem;
   void (*set_attrs)();
-  void (*launch)(int grid, cudaStream_t s, const BSolve *solves, int n, int tiles,
-                 double *tile_max);
+  void (*launch)(int grid, cudaStream_t s, const BSolve *solves, int n, int tile_begin,
+                 int tile_end, double *tile_max);
   int (*occupancy)();
 };
 
@@ -403,10 +404,10 @@ BatchVariant make_bvariant() {
     cudaFuncSetAttribute(kb_rate<TX, TY, MINB, WIN, SORT, PP>,
                          cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SM::rate);
   };
-  v.launch = [](int grid, cudaStream_t s, const BSolve *solves, int n, int tiles,
-                double *tile_max) {
+  v.launch = [](int grid, cudaStream_t s, const BSolve *solves, int n, int tile_begin,
+                int tile_end, double *tile_max) {
     launch_pdl(kb_rate<TX, TY, MINB, WIN, SORT, PP>, dim3(grid), dim3(TX, TY), SM::rate, s, solves, n,
-               tiles, tile_max);
+               tile_begin, tile_end, tile_max);
   };
   v.occupancy = []() {
     int nb = 0;
@@ -431,6 +432,22 @@ const std::vector<BatchVariant> &batch_variants() {
 // Parallel FFT branches of a batch step graph (one stream per branch).
 constexpr int kFftBranches = 16;
 
+// The solves are split into lanes whose step chains (FFT branches -> rate
+// -> dt -> update) are separate branches of the step graph, the second
+// lane one FFT phase behind the first: one lane's cuFFT chains (small
+// grids, mostly latency) then run while the other lane's rate kernel fills
+// the SMs.  Each shape group's solves stay in one lane (one batched plan).
+constexpr int kLanes = 2;
+
+struct Lane {
+  int s0 = 0, ns = 0;             // positions [s0, s0 + ns) of the lane order
+  int tile0 = 0, ntiles = 0;      // the lane's tiles (current variant)
+  int chunk0 = 0, nchunks = 0;    // the lane's update chunks
+  std::vector<int> order;         // the lane's shape groups, largest first
+  int aux0 = 0, naux = 0;         // its FFT branch streams aux[aux0, aux0 + naux)
+  cudaEvent_t fork = nullptr;
+};
+
 struct ShapeGroup {
   int ny, nx, count;
   int64_t s_off, k_off, nk;
@@ -453,16 +470,23 @@ struct pf5d_batch {
   StepState32 *st = nullptr;
   std::vector<ShapeGroup> groups;
   int total_tiles = 0, total_chunks = 0;
-  int variant = 0, rate_grid = 1, upd_grid = 1;
+  int variant = 0, upd_grid = 1;
+  int lane_grid = 1;                // persistent rate blocks of one lane
   cudaStream_t cap = nullptr;
   double *tile_max = nullptr;       // per-tile max |dX/dt| of the last rate launch
   // Shape groups' FFT chains run as parallel branches of the step graph:
-  // forked from the capture stream onto `aux`, joined back before the rate
-  // kernel.  `order` lists the groups largest first, dealt round-robin.
+  // forked from the lane's stream onto its `aux` streams (high priority, so
+  // their blocks get SM slots as the other lane's rate blocks retire),
+  // joined back before the lane's rate kernel.
   std::vector<cudaStream_t> aux;
   std::vector<cudaEvent_t> join;
-  cudaEvent_t fork = nullptr;
-  std::vector<int> order;
+  // Step kernels read the descriptors in lane order (tiles and chunks are
+  // numbered in that order); d_solves keeps the caller's order.
+  BSolve *d_lane = nullptr;
+  std::vector<int> lane_order;      // caller's index at each lane-order position
+  std::vector<Lane> lanes;
+  cudaStream_t lane_stream = nullptr;
+  cudaEvent_t lane_ev[2] = {nullptr, nullptr};
   std::map<int64_t, cudaGraphExec_t> graphs;
   int64_t total_points = 0;
 };
@@ -486,39 +510,53 @@ pf5d_status configure_batch(pf5d_batch *h, int variant) {
   const BatchVariant &v = vars[variant];
   v.set_attrs();
   PF5D_LAUNCHED();
-  // Tile grid of every solve for this variant.
+  // Tile grid of every solve for this variant, numbered in lane order.
   const int nt = v.tx * v.ty;
   int tiles = 0;
-  for (auto &b : h->solves) {
-    if (b.dim == 2) {
-      b.ntx = (b.R.nx + v.tx - 1) / v.tx;
-      b.nty = (b.R.ny + v.ty - 1) / v.ty;
-    } else {
-      b.ntx = (b.R.nx + nt - 1) / nt;
-      b.nty = 1;
+  for (auto &ln : h->lanes) {
+    ln.tile0 = tiles;
+    for (int k = ln.s0; k < ln.s0 + ln.ns; ++k) {
+      BSolve &b = h->solves[h->lane_order[k]];
+      if (b.dim == 2) {
+        b.ntx = (b.R.nx + v.tx - 1) / v.tx;
+        b.nty = (b.R.ny + v.ty - 1) / v.ty;
+      } else {
+        b.ntx = (b.R.nx + nt - 1) / nt;
+        b.nty = 1;
+      }
+      b.tile0 = tiles;
+      b.ntiles = b.ntx * b.nty;
+      tiles += b.ntiles;
     }
-    b.tile0 = tiles;
-    b.ntiles = b.ntx * b.nty;
-    tiles += b.ntiles;
+    ln.ntiles = tiles - ln.tile0;
   }
   h->total_tiles = tiles;
+  std::vector<BSolve> lane(h->lane_order.size());
+  for (size_t k = 0; k < lane.size(); ++k) lane[k] = h->solves[h->lane_order[k]];
   PF5D_CUDA(cudaMemcpy(h->d_solves, h->solves.data(), h->solves.size() * sizeof(BSolve),
                        cudaMemcpyHostToDevice));
+  PF5D_CUDA(cudaMemcpy(h->d_lane, lane.data(), lane.size() * sizeof(BSolve),
+                       cudaMemcpyHostToDevice));
+  // each lane's rate kernel holds at most its share of the resident block
+  // slots, so the other lane's FFT kernels find free slots
   const int per_sm = std::max(1, v.occupancy());
-  h->rate_grid = std::min(tiles, sm_count() * per_sm);
+  h->lane_grid = std::max(1, sm_count() * per_sm / (int)std::max<size_t>(h->lanes.size(), 1));
   h->variant = variant;
   return PF5D_OK;
 }
 
-pf5d_status enqueue_batch_step(pf5d_batch *h, cudaStream_t s) {
-  const int na = std::min<int>((int)h->groups.size(), (int)h->aux.size());
+// One step of lane L on stream s.  `offset` (optional) is recorded on s
+// once the lane's FFT branches have joined.
+pf5d_status enqueue_lane_step(pf5d_batch *h, int L, cudaStream_t s, cudaEvent_t offset) {
+  const Lane &ln = h->lanes[L];
+  const int na = std::min<int>((int)ln.order.size(), ln.naux);
   if (na > 0) {
-    PF5D_CUDA(cudaEventRecord(h->fork, s));
-    for (int a = 0; a < na; ++a) PF5D_CUDA(cudaStreamWaitEvent(h->aux[a], h->fork, 0));
+    PF5D_CUDA(cudaEventRecord(ln.fork, s));
+    for (int a = 0; a < na; ++a) PF5D_CUDA(cudaStreamWaitEvent(h->aux[ln.aux0 + a], ln.fork, 0));
   }
-  for (int j = 0; j < (int)h->order.size(); ++j) {
-    ShapeGroup &g = h->groups[h->order[j]];
-    cudaStream_t gs = h->aux[j % na];
+  for (int j = 0; j < (int)ln.order.size(); ++j) {
+    ShapeGroup &g = h->groups[ln.order[j]];
+    cudaStream_t gs = h->aux[ln.aux0 + j % na];
     if (cufftSetStream(g.fwd, gs) != CUFFT_SUCCESS ||
         cufftExecR2C(g.fwd, h->s + g.s_off, h->k + g.k_off) != CUFFT_SUCCESS) {
       set_error("batch cuFFT R2C failed");
@@ -534,17 +572,18 @@ pf5d_status enqueue_batch_step(pf5d_batch *h, cudaStream_t s) {
     }
   }
   for (int a = 0; a < na; ++a) {
-    PF5D_CUDA(cudaEventRecord(h->join[a], h->aux[a]));
-    PF5D_CUDA(cudaStreamWaitEvent(s, h->join[a], 0));
+    PF5D_CUDA(cudaEventRecord(h->join[ln.aux0 + a], h->aux[ln.aux0 + a]));
+    PF5D_CUDA(cudaStreamWaitEvent(s, h->join[ln.aux0 + a], 0));
   }
-  batch_variants()[h->variant].launch(h->rate_grid, s, h->d_solves, (int)h->solves.size(),
-                                      h->total_tiles, h->tile_max);
+  if (offset) PF5D_CUDA(cudaEventRecord(offset, s));
+  const BSolve *ls = h->d_lane + ln.s0;
+  batch_variants()[h->variant].launch(std::max(1, std::min(ln.ntiles, h->lane_grid)), s, ls, ln.ns,
+                                      ln.tile0, ln.tile0 + ln.ntiles, h->tile_max);
   PF5D_LAUNCHED();
-  PF5D_CUDA(launch_pdl(kb_dt, dim3((unsigned)((h->solves.size() + 7) / 8)), dim3(256), 0, s,
-                       (const BSolve *)h->d_solves, (int)h->solves.size(),
+  PF5D_CUDA(launch_pdl(kb_dt, dim3((unsigned)((ln.ns + 7) / 8)), dim3(256), 0, s, ls, ln.ns,
                        (const double *)h->tile_max));
-  PF5D_CUDA(launch_pdl(kb_update, dim3(h->upd_grid), dim3(kUpdThreads), 0, s,
-                       (const BSolve *)h->d_solves, (int)h->solves.size(), h->total_chunks));
+  PF5D_CUDA(launch_pdl(kb_update, dim3((unsigned)std::max(1, std::min(ln.nchunks, h->upd_grid))),
+                       dim3(kUpdThreads), 0, s, ls, ln.ns, ln.chunk0, ln.chunk0 + ln.nchunks));
   PF5D_LAUNCHED();
   return PF5D_OK;
 }
@@ -561,17 +600,36 @@ pf5d_status batch_graph(pf5d_batch *h, int64_t n, cudaGraphExec_t *out) {
     return PF5D_OK;
   }
   cudaGraph_t g = nullptr;
+  const bool two = h->lanes.size() > 1;
   PF5D_CUDA(cudaStreamBeginCapture(h->cap, cudaStreamCaptureModeThreadLocal));
   pf5d_status st = PF5D_OK;
-  for (int64_t i = 0; i < n && st == PF5D_OK; ++i) st = enqueue_batch_step(h, h->cap);
-  cudaError_t e = cudaStreamEndCapture(h->cap, &g);
-  if (st != PF5D_OK) {
-    if (g) cudaGraphDestroy(g);
-    return st;
+  cudaError_t e = cudaSuccess;
+  if (two) {
+    // the second lane joins the capture, then starts after the first lane's
+    // first FFT phase
+    e = cudaEventRecord(h->lane_ev[0], h->cap);
+    if (e == cudaSuccess) e = cudaStreamWaitEvent(h->lane_stream, h->lane_ev[0], 0);
   }
-  PF5D_REQUIRE(e == cudaSuccess, PF5D_ERR_CUDA, "graph capture: %s", cudaGetErrorString(e));
+  for (int64_t i = 0; i < n && st == PF5D_OK && e == cudaSuccess; ++i) {
+    st = enqueue_lane_step(h, 0, h->cap, two && i == 0 ? h->lane_ev[1] : nullptr);
+    if (st == PF5D_OK && two) {
+      if (i == 0) e = cudaStreamWaitEvent(h->lane_stream, h->lane_ev[1], 0);
+      if (e == cudaSuccess) st = enqueue_lane_step(h, 1, h->lane_stream, nullptr);
+    }
+  }
+  if (two && st == PF5D_OK && e == cudaSuccess) {
+    e = cudaEventRecord(h->lane_ev[0], h->lane_stream);
+    if (e == cudaSuccess) e = cudaStreamWaitEvent(h->cap, h->lane_ev[0], 0);
+  }
+  const cudaError_t e_end = cudaStreamEndCapture(h->cap, &g);
+  if (e == cudaSuccess) e = e_end;
+  if (st != PF5D_OK || e != cudaSuccess) {
+    if (g) cudaGraphDestroy(g);
+    if (st != PF5D_OK) return st;
+    PF5D_REQUIRE(false, PF5D_ERR_CUDA, "graph capture: %s", cudaGetErrorString(e));
+  }
   cudaGraphExec_t exec = nullptr;
-  e = cudaGraphInstantiate(&exec, g, 0);
+  e = cudaGraphInstantiateWithFlags(&exec, g, cudaGraphInstantiateFlagUseNodePriority);
   cudaGraphDestroy(g);
   PF5D_REQUIRE(e == cudaSuccess, PF5D_ERR_CUDA, "graph instantiate: %s", cudaGetErrorString(e));
   h->graphs[n] = exec;
@@ -622,6 +680,7 @@ pf5d_status pf5d_batch_create(const pf5d_batch_solve *solves, int32_t nsolves,
   h->total_points = npts_total;
   // s layout: 2D elastic solves contiguous per shape group first, then the rest.
   std::vector<int64_t> s_off(nsolves, -1);
+  std::vector<std::vector<int>> members;     // solves of each shape group
   int64_t s_total = 0, k_total = 0;
   for (auto &kv : by_shape) {
     ShapeGroup g;
@@ -637,6 +696,7 @@ pf5d_status pf5d_batch_create(const pf5d_batch_solve *solves, int32_t nsolves,
     }
     k_total += g.nk * g.count;
     h->groups.push_back(g);
+    members.push_back(kv.second);
   }
   for (int i = 0; i < nsolves; ++i)
     if (s_off[i] < 0) {
@@ -651,6 +711,7 @@ pf5d_status pf5d_batch_create(const pf5d_batch_solve *solves, int32_t nsolves,
       cudaMalloc(&h->spart, std::max<int64_t>(nchunks_total, 1) * sizeof(double)) != cudaSuccess ||
       cudaMalloc(&h->st, nsolves * sizeof(StepState32)) != cudaSuccess ||
       cudaMalloc(&h->d_solves, nsolves * sizeof(BSolve)) != cudaSuccess ||
+      cudaMalloc(&h->d_lane, nsolves * sizeof(BSolve)) != cudaSuccess ||
       cudaStreamCreateWithFlags(&h->cap, cudaStreamNonBlocking) != cudaSuccess) {
     set_error("device allocation failed");
     return fail(PF5D_ERR_CUDA);
@@ -684,31 +745,75 @@ pf5d_status pf5d_batch_create(const pf5d_batch_solve *solves, int32_t nsolves,
       return fail(PF5D_ERR_CUDA);
     }
   }
-  // --- FFT branches: groups largest first over up to kFftBranches streams ----
-  for (int j = 0; j < (int)h->groups.size(); ++j) h->order.push_back(j);
-  std::stable_sort(h->order.begin(), h->order.end(), [&](int a, int b) {
+  // --- lanes: shape groups largest first to the lighter lane, then the
+  //     solves without an FFT; FFT branch streams split between the lanes --
+  std::vector<int> gorder;
+  for (int j = 0; j < (int)h->groups.size(); ++j) gorder.push_back(j);
+  std::stable_sort(gorder.begin(), gorder.end(), [&](int a, int b) {
     const auto &ga = h->groups[a], &gb = h->groups[b];
     return (int64_t)ga.ny * ga.nx * ga.count > (int64_t)gb.ny * gb.nx * gb.count;
   });
-  const int nbranch = std::min<int>((int)h->groups.size(), kFftBranches);
-  if (nbranch > 0 &&
-      cudaEventCreateWithFlags(&h->fork, cudaEventDisableTiming) != cudaSuccess) {
-    set_error("event creation failed");
+  const int nl = nsolves >= 2 ? kLanes : 1;
+  std::vector<int> lane_of(nsolves, -1);
+  std::vector<int64_t> lane_pts(nl, 0);
+  std::vector<std::vector<int>> lane_groups(nl);
+  auto lighter = [&]() {
+    return (int)(std::min_element(lane_pts.begin(), lane_pts.end()) - lane_pts.begin());
+  };
+  for (int j : gorder) {
+    const int L = lighter();
+    lane_groups[L].push_back(j);
+    lane_pts[L] += (int64_t)h->groups[j].ny * h->groups[j].nx * h->groups[j].count;
+    for (int i : members[j]) lane_of[i] = L;
+  }
+  for (int i = 0; i < nsolves; ++i)
+    if (lane_of[i] < 0) {
+      const int L = lighter();
+      lane_of[i] = L;
+      lane_pts[L] += solves[i].dim == 1 ? solves[i].shape[0] : solves[i].shape[0] * solves[i].shape[1];
+    }
+  int least_pri = 0, greatest_pri = 0;
+  if (cudaDeviceGetStreamPriorityRange(&least_pri, &greatest_pri) != cudaSuccess) {
+    set_error("stream priority query failed");
     return fail(PF5D_ERR_CUDA);
   }
-  for (int a = 0; a < nbranch; ++a) {
-    cudaStream_t as = nullptr;
-    cudaEvent_t ev = nullptr;
-    if (cudaStreamCreateWithFlags(&as, cudaStreamNonBlocking) != cudaSuccess) {
-      set_error("stream creation failed");
-      return fail(PF5D_ERR_CUDA);
-    }
-    h->aux.push_back(as);
-    if (cudaEventCreateWithFlags(&ev, cudaEventDisableTiming) != cudaSuccess) {
+  const int per_lane = std::max(1, kFftBranches / nl);
+  for (int L = 0; L < nl; ++L) {
+    Lane ln;
+    ln.s0 = (int)h->lane_order.size();
+    for (int i = 0; i < nsolves; ++i)
+      if (lane_of[i] == L) h->lane_order.push_back(i);
+    ln.ns = (int)h->lane_order.size() - ln.s0;
+    if (ln.ns == 0) continue;
+    ln.order = lane_groups[L];
+    ln.aux0 = (int)h->aux.size();
+    ln.naux = std::min<int>((int)ln.order.size(), per_lane);
+    if (ln.naux > 0 && cudaEventCreateWithFlags(&ln.fork, cudaEventDisableTiming) != cudaSuccess) {
       set_error("event creation failed");
       return fail(PF5D_ERR_CUDA);
     }
-    h->join.push_back(ev);
+    for (int a = 0; a < ln.naux; ++a) {
+      cudaStream_t as = nullptr;
+      cudaEvent_t ev = nullptr;
+      if (cudaStreamCreateWithPriority(&as, cudaStreamNonBlocking, greatest_pri) != cudaSuccess) {
+        set_error("stream creation failed");
+        return fail(PF5D_ERR_CUDA);
+      }
+      h->aux.push_back(as);
+      if (cudaEventCreateWithFlags(&ev, cudaEventDisableTiming) != cudaSuccess) {
+        set_error("event creation failed");
+        return fail(PF5D_ERR_CUDA);
+      }
+      h->join.push_back(ev);
+    }
+    h->lanes.push_back(ln);
+  }
+  if (h->lanes.size() > 1 &&
+      (cudaStreamCreateWithFlags(&h->lane_stream, cudaStreamNonBlocking) != cudaSuccess ||
+       cudaEventCreateWithFlags(&h->lane_ev[0], cudaEventDisableTiming) != cudaSuccess ||
+       cudaEventCreateWithFlags(&h->lane_ev[1], cudaEventDisableTiming) != cudaSuccess)) {
+    set_error("stream creation failed");
+    return fail(PF5D_ERR_CUDA);
   }
   // --- per-solve descriptors -------------------------------------------------
   int64_t chunk = 0;
@@ -728,7 +833,6 @@ pf5d_status pf5d_batch_create(const pf5d_batch_solve *solves, int32_t nsolves,
     b.lo = h->lo + h->pt_off[i];
     b.s = h->s + s_off[i];
     b.spart = h->spart + chunk;
-    b.chunk0 = (int)chunk;
     b.nchunks = (int)((b.npts + kChunk - 1) / kChunk);
     chunk += b.nchunks;
     b.emode = !q.elastic ? 0 : (q.dim == 1 ? 1 : 2);
@@ -782,6 +886,18 @@ pf5d_status pf5d_batch_create(const pf5d_batch_solve *solves, int32_t nsolves,
     h->solves.push_back(b);
   }
   h->total_chunks = (int)chunk;
+  // update chunks numbered in lane order (b.spart keeps the solve's own
+  // partial-sum region)
+  int run = 0;
+  for (auto &ln : h->lanes) {
+    ln.chunk0 = run;
+    for (int k = ln.s0; k < ln.s0 + ln.ns; ++k) {
+      BSolve &b = h->solves[h->lane_order[k]];
+      b.chunk0 = run;
+      run += b.nchunks;
+    }
+    ln.nchunks = run - ln.chunk0;
+  }
   h->upd_grid = std::min<int>(h->total_chunks, sm_count() * 8);
   cudaStream_t s = as_stream(stream);
   if (cudaMemcpy(h->st, init.data(), nsolves * sizeof(StepState32), cudaMemcpyHostToDevice) !=
@@ -893,11 +1009,12 @@ pf5d_status pf5d_batch_autotune(pf5d_batch *h, int32_t *variant, float *best_ms,
   float best_t = 1e30f;
   for (int v = 0; v < (int)batch_variants().size(); ++v) {
     if (configure_batch(h, v) != PF5D_OK) continue;
-    batch_variants()[v].launch(h->rate_grid, s, h->d_solves, (int)n, h->total_tiles, h->tile_max);
+    const int grid = std::max(h->total_tiles, 1);
+    batch_variants()[v].launch(grid, s, h->d_lane, (int)n, 0, h->total_tiles, h->tile_max);
     if (cudaGetLastError() != cudaSuccess) continue;
     PF5D_CUDA(cudaEventRecord(e0, s));
     for (int r = 0; r < 3; ++r)
-      batch_variants()[v].launch(h->rate_grid, s, h->d_solves, (int)n, h->total_tiles, h->tile_max);
+      batch_variants()[v].launch(grid, s, h->d_lane, (int)n, 0, h->total_tiles, h->tile_max);
     PF5D_CUDA(cudaEventRecord(e1, s));
     PF5D_CUDA(cudaEventSynchronize(e1));
     float ms = 0.f;
@@ -935,11 +1052,16 @@ pf5d_status pf5d_batch_destroy(pf5d_batch *h) {
   cudaFree(h->spart);
   cudaFree(h->st);
   cudaFree(h->d_solves);
+  cudaFree(h->d_lane);
   cudaFree(h->tile_max);
   if (h->cap) cudaStreamDestroy(h->cap);
   for (auto as : h->aux) cudaStreamDestroy(as);
   for (auto ev : h->join) cudaEventDestroy(ev);
-  if (h->fork) cudaEventDestroy(h->fork);
+  for (auto &ln : h->lanes)
+    if (ln.fork) cudaEventDestroy(ln.fork);
+  if (h->lane_stream) cudaStreamDestroy(h->lane_stream);
+  for (auto ev : h->lane_ev)
+    if (ev) cudaEventDestroy(ev);
   delete h;
   return PF5D_OK;
 }
