@@ -574,7 +574,9 @@ def run_ours(args, rank, world, local_rank):
                           "achieved_gbs": per_step * value / world / 1e9,
                           "frac": per_step * value / world / 1e9 / peak},
         "stage_ms": stage_ms,
-        "rate_variant": {"index": st.variant, "tuned_ms": st.tuned_ms},
+        "rate_variant": {"index": st.variant, "tuned_ms": st.tuned_ms,
+                         "tuned_ms_is": "ms per step of the fastest whole-step graph (FP64 2D/3D)"
+                                        if not fp32c and prob.dim > 1 else "ms per rate stage"},
         "resident_l2_warm": {"value": world * P / (resident_ms * 1e-3),
                              "ms_per_step": resident_ms,
                              "note": "200 back-to-back steps from 50-step graphs, no flush"},

@@ -224,8 +224,11 @@ pf5d_status pf5d_stepper_mass(pf5d_stepper *h, double *mean_out, void *stream);
 #define PF5D_STAGE_FFT_INV 4     /* cuFFT Z2D                                  */
 pf5d_status pf5d_stepper_launch_stage(pf5d_stepper *h, int32_t stage, void *stream);
 /* Autotuner: time every rate-kernel variant (plane tile shape x resident
- * blocks per SM) on this solve and keep the fastest; the step state is
- * preserved.  *variant / *best_ms (either may be NULL) report the choice. */
+ * blocks per SM, ...) on this solve; the plain FP64 form then times the
+ * fastest few as captured graphs of whole steps and keeps the fastest.  The
+ * field and step state are preserved.  *variant / *best_ms (either may be
+ * NULL) report the choice and its time: ms per step (plain FP64 2D/3D) or
+ * ms per rate stage (other forms). */
 pf5d_status pf5d_stepper_autotune(pf5d_stepper *h, int32_t *variant, float *best_ms,
                                   void *stream);
 /* Select a rate-kernel variant explicitly (index from a previous autotune). */

@@ -1214,9 +1214,17 @@ pf5d_status launch_rate(pf5d_stepper *h, cudaStream_t s) {
   return PF5D_OK;
 }
 
-// Time every rate-kernel variant on this solve (events on `s`, a few reps
-// each) and keep the fastest.  The step state is saved and restored, so
-// tuning leaves the solve where it was; any captured graphs are dropped.
+pf5d_status graph_for(pf5d_stepper *h, int64_t nsteps, cudaGraphExec_t *out);
+
+constexpr int kTuneFinalists = 6;    // variants timed as whole steps
+constexpr int kTuneSteps = 10;       // steps per timed graph
+
+// Time every rate-kernel variant's rate stage on this solve (events on `s`,
+// a few reps each); then time the fastest few as captured graphs of whole
+// steps (what a run executes: the FFT chain, update and launch chaining
+// change the order), each from the same saved state, and keep the fastest.
+// The field, s and the step state are restored, so tuning leaves the solve
+// where it was; any captured graphs are dropped.
 pf5d_status autotune_rate(pf5d_stepper *h, cudaStream_t s, float *best_ms) {
   if (h->d.dim == 1) {
     if (best_ms) *best_ms = 0.f;
@@ -1228,9 +1236,8 @@ pf5d_status autotune_rate(pf5d_stepper *h, cudaStream_t s, float *best_ms) {
   cudaEvent_t e0, e1;
   PF5D_CUDA(cudaEventCreate(&e0));
   PF5D_CUDA(cudaEventCreate(&e1));
-  int best = h->variant;
-  float best_t = 1e30f;
   const int reps = 5;
+  std::vector<std::pair<float, int>> rate_t;
   for (int v = 0; v < (int)rate_variants().size(); ++v) {
     pf5d_status st = configure_rate(h, v);
     if (st != PF5D_OK) continue;
@@ -1245,19 +1252,57 @@ pf5d_status autotune_rate(pf5d_stepper *h, cudaStream_t s, float *best_ms) {
     PF5D_CUDA(cudaEventSynchronize(e1));
     float ms = 0.f;
     PF5D_CUDA(cudaEventElapsedTime(&ms, e0, e1));
-    if (st == PF5D_OK && ms / reps < best_t) {
-      best_t = ms / reps;
+    if (st == PF5D_OK) rate_t.push_back({ms / reps, v});
+  }
+  PF5D_REQUIRE(!rate_t.empty(), PF5D_ERR_CUDA, "no rate variant ran");
+  std::sort(rate_t.begin(), rate_t.end());
+  // whole steps of the finalists, each from the saved field / s / state
+  const size_t nx = (size_t)h->npts * 4, ns = h->d.elastic ? (size_t)h->npts : 0;
+  double *keep = nullptr;
+  PF5D_CUDA(cudaMalloc(&keep, (nx + ns) * sizeof(double)));
+  auto restore = [&]() {
+    cudaMemcpyAsync(h->X, keep, nx * sizeof(double), cudaMemcpyDeviceToDevice, s);
+    if (ns) cudaMemcpyAsync(h->s, keep + nx, ns * sizeof(double), cudaMemcpyDeviceToDevice, s);
+    cudaMemcpyAsync(h->st, &saved, sizeof(saved), cudaMemcpyHostToDevice, s);
+    return cudaGetLastError();
+  };
+  cudaError_t e = cudaMemcpyAsync(keep, h->X, nx * sizeof(double), cudaMemcpyDeviceToDevice, s);
+  if (e == cudaSuccess && ns)
+    e = cudaMemcpyAsync(keep + nx, h->s, ns * sizeof(double), cudaMemcpyDeviceToDevice, s);
+  int best = rate_t[0].second;
+  float best_t = 1e30f;
+  const int nfin = std::min<int>((int)rate_t.size(), kTuneFinalists);
+  for (int i = 0; i < nfin && e == cudaSuccess; ++i) {
+    const int v = rate_t[i].second;
+    for (auto &kv : h->graphs) cudaGraphExecDestroy(kv.second);
+    h->graphs.clear();
+    cudaGraphExec_t g = nullptr;
+    if (configure_rate(h, v) != PF5D_OK || graph_for(h, kTuneSteps, &g) != PF5D_OK) continue;
+    if ((e = restore()) != cudaSuccess || (e = cudaGraphLaunch(g, s)) != cudaSuccess) break;
+    if ((e = restore()) != cudaSuccess || (e = cudaEventRecord(e0, s)) != cudaSuccess ||
+        (e = cudaGraphLaunch(g, s)) != cudaSuccess || (e = cudaEventRecord(e1, s)) != cudaSuccess ||
+        (e = cudaEventSynchronize(e1)) != cudaSuccess)
+      break;
+    StepState after;
+    float ms = 0.f;
+    if ((e = cudaMemcpy(&after, h->st, sizeof(after), cudaMemcpyDeviceToHost)) != cudaSuccess ||
+        (e = cudaEventElapsedTime(&ms, e0, e1)) != cudaSuccess)
+      break;
+    if (!after.halt && ms / kTuneSteps < best_t) {
+      best_t = ms / kTuneSteps;
       best = v;
     }
   }
+  if (e == cudaSuccess) e = restore();
+  if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+  cudaFree(keep);
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
-  pf5d_status st = configure_rate(h, best);
-  if (st != PF5D_OK) return st;
+  PF5D_REQUIRE(e == cudaSuccess, PF5D_ERR_CUDA, "autotune: %s", cudaGetErrorString(e));
   for (auto &kv : h->graphs) cudaGraphExecDestroy(kv.second);
   h->graphs.clear();
-  PF5D_CUDA(cudaMemcpyAsync(h->st, &saved, sizeof(saved), cudaMemcpyHostToDevice, s));
-  PF5D_CUDA(cudaStreamSynchronize(s));
+  pf5d_status st = configure_rate(h, best);
+  if (st != PF5D_OK) return st;
   if (best_ms) *best_ms = best_t;
   return PF5D_OK;
 }
