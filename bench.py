@@ -84,6 +84,9 @@ def parse():
     ap.add_argument("--serve-requests", type=int, default=12)
     ap.add_argument("--serve-rates", default="1,10,50", help="Poisson arrival rates, req/s")
     ap.add_argument("--serve-steps", type=int, default=2000)
+    ap.add_argument("--ncu-range", action="store_true",
+                    help="after warm-up, run one extra step (untimed) between cudaProfilerStart/"
+                         "Stop, for ncu --profile-from-start off")
     return ap.parse_args()
 
 
@@ -105,8 +108,9 @@ def measured_peak():
 
 
 def committed_traffic(kernel, workload, precision):
-    """DRAM bytes per launch of ``kernel`` on this workload from the committed
-    ncu capture (profiles/traffic.json), or None when none was taken."""
+    """DRAM bytes of one step's ``kernel`` stage (all its launches) on this
+    workload from the committed ncu capture (profiles/traffic.json), or None
+    when none was taken."""
     try:
         with open(os.path.join(HERE, "profiles", "traffic.json")) as f:
             ent = json.load(f)[kernel][f"{workload}_{precision}"]
@@ -302,6 +306,17 @@ def form_fp32c(prob, args, flush, torch):
     return out
 
 
+def profiled_step(torch, step, flush):
+    """One untimed step between cudaProfilerStart / Stop (L2 flushed before),
+    so that ncu --profile-from-start off captures exactly one step's kernels."""
+    flush.zero_()
+    torch.cuda.synchronize()
+    torch.cuda.cudart().cudaProfilerStart()
+    step()
+    torch.cuda.synchronize()
+    torch.cuda.cudart().cudaProfilerStop()
+
+
 def form_batch(args, flush, torch):
     """The 64-solve batched FP32-compensated form (uneven 1D 2048-8192 and
     2D 128^2-384^2 grids, four temperature tables) against the plain FP64
@@ -320,6 +335,8 @@ def form_batch(args, flush, torch):
     b = BatchStepper(probs, stream=stream)
     for _ in range(n_warm):
         b.advance(block)
+    if args.ncu_range:
+        profiled_step(torch, lambda: b.advance(1), flush)
     ev = []
     for _ in range(n_blocks):
         flush.zero_()
@@ -453,6 +470,8 @@ def run_ours(args, rank, world, local_rank):
     for _ in range(args.warmup):
         flush.zero_()
         st.advance(1)
+    if args.ncu_range:
+        profiled_step(torch, lambda: st.advance(1), flush)
     barrier()
     clocks = ClockSampler(local_rank).start()
     ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
