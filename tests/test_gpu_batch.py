@@ -63,6 +63,28 @@ def test_batch_tracks_fp64(small_probs):
     b.close()
 
 
+def test_workload_sized_solves_track_fp64(torch_cuda):
+    """2D solves at the batched workload's sizes (squares 128^2 to 368^2,
+    prime factors 3, 23 in the FFT lengths) beside a small non-square one:
+    each tracks its plain-FP64 run within the precision tolerance."""
+    from phasefield5d_b200 import workload as W
+    from phasefield5d_b200.batch import BatchStepper
+    cfgs = W.batched_configs(4, seed=9, steps=200)
+    for c, sh in zip(cfgs, [(128, 128), (144, 144), (48, 40), (368, 368)]):
+        c.shape = sh
+        c.system_dim = 2
+    probs, _ = W.build_batched_problems(cfgs)
+    n = 200
+    b = BatchStepper(probs)
+    b.advance(n)
+    for i, p in enumerate(probs):
+        Xb = b.field(i).cpu().numpy()
+        X64 = _fp64(p, n)
+        err = np.max(np.abs(Xb - X64)) / np.max(np.abs(X64))
+        assert err <= FIELD_RTOL_FP32C, (i, p.shape, err)
+    b.close()
+
+
 def test_alone_vs_mix(small_probs):
     from phasefield5d_b200.batch import BatchStepper
     n = 120
