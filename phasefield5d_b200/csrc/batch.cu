@@ -788,7 +788,9 @@ pf5d_status pf5d_batch_create(const pf5d_batch_solve *solves, int32_t nsolves,
     ln.order = lane_groups[L];
     ln.aux0 = (int)h->aux.size();
     ln.naux = std::min<int>((int)ln.order.size(), per_lane);
-    if (ln.naux > 0 && cudaEventCreateWithFlags(&ln.fork, cudaEventDisableTiming) != cudaSuccess) {
+    h->lanes.push_back(ln);             // registered first: teardown frees what follows
+    if (ln.naux > 0 &&
+        cudaEventCreateWithFlags(&h->lanes.back().fork, cudaEventDisableTiming) != cudaSuccess) {
       set_error("event creation failed");
       return fail(PF5D_ERR_CUDA);
     }
@@ -806,7 +808,6 @@ pf5d_status pf5d_batch_create(const pf5d_batch_solve *solves, int32_t nsolves,
       }
       h->join.push_back(ev);
     }
-    h->lanes.push_back(ln);
   }
   if (h->lanes.size() > 1 &&
       (cudaStreamCreateWithFlags(&h->lane_stream, cudaStreamNonBlocking) != cudaSuccess ||
