@@ -1,15 +1,20 @@
 // batch.cu -- many independent solves advanced together (the batched form).
 //
 // Solves of different dimension (1D / 2D), size, composition, temperature
-// table and kappa share every launch of a step:
+// table and kappa are split into two lanes (balanced by points); the solves
+// of a lane share every launch of its step:
 //   * one cuFFT R2C/C2R pair per group of 2D solves with the same shape
 //     (batched plans; B(k) depends only on the direction of k, so a shape
-//     group shares one B(k)/N), plus one B(k) multiply over all groups;
-//   * one persistent rate launch: blocks loop over the tiles of all solves
-//     (32x8-style plane tiles for 2D, runs of TX*TY points for 1D); per
-//     tile the solve's max|dX/dt| is folded into that solve's accumulator
-//     and the tile completing a solve runs its FP64 dt controller;
+//     group shares one B(k)/N) and its B(k) multiply, the groups' chains on
+//     parallel graph branches;
+//   * one persistent rate launch: blocks loop over the lane's tiles
+//     (32x8-style plane tiles for 2D, runs of TX*TY points for 1D) and
+//     store each tile's max|dX/dt| in its own slot;
+//   * kb_dt: one warp per solve reduces its slots and runs its FP64 dt
+//     controller;
 //   * one persistent compensated-update launch over fixed 1024-point chunks.
+// The two lanes' chains are separate branches of the step graph, the second
+// one FFT phase behind, so one lane's FFTs run beside the other's rate kernel.
 // In 1D, B(k) is the same constant B_n for every k != 0 and zero at k = 0,
 // so the elastic term is exactly B_n * (s - mean(s)): 1D solves need no FFT.
 // The mean (the k = 0 mode) is formed in FP64 from per-chunk partial sums

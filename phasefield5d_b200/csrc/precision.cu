@@ -2,8 +2,9 @@
 // form").  Same dataflow and tiling as the FP64 stepper (stepper.cu):
 //   cuFFT R2C of the misfit -> B(k)/N multiply -> cuFFT C2R -> fused rate
 //   kernel (FP32 interpolation, Laplacian, mu, one flux per face,
-//   divergence, max|dX/dt| and the FP64 dt controller in the last block)
-//   -> compensated update + clamp + next misfit + out-of-bounds test,
+//   divergence, a max|dX/dt| slot per block) -> k32_dt (one block: the
+//   FP64 dt controller) -> compensated update + clamp + next misfit +
+//   out-of-bounds test,
 // replayed from CUDA graphs.
 //
 // Numerics:

@@ -14,10 +14,15 @@
 //          mu = (mu_chem - lap*kappa) + s'*l,
 //        - one flux per face (the +axis0 face of the previous plane is kept
 //          in registers and reused as this plane's -axis0 face),
-//        - dX/dt written once; block max |dX/dt| folded into a device
-//          accumulator; the last block to finish evaluates the adaptive dt
-//          rule and advances dt, time and the step counter on the device.
-//   5. k_update_step: X += dX*dt; clamp; s for the next step; every
+//        - dX/dt written once; each block stores its max |dX/dt| in its
+//          own slot (plain store).
+//      Variants (autotuned, all computing the same values): tile shapes,
+//      a split form (k_chem64 writes mu/M once per point, the tile kernel
+//      reads them back), table-cell sort, shared table window, per-point
+//      faces.
+//   5. k_dt_finish (one block): max over the slots, the adaptive dt rule,
+//      dt / time / step advanced on the device.
+//   6. k_update_step: X += dX*dt; clamp; s for the next step; every
 //      oob_interval steps the out_of_bounds test, which halts the stepper
 //      (every later kernel returns at entry) on a hard violation.
 //

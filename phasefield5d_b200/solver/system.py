@@ -79,9 +79,10 @@ def apply_adaptive_time(dt_current, xdotmax, ctld, t_cfl, *,
                         max_change_factor=2.0):
     """Host copy of the adaptive-Δt rule (phasefield5d/solver/system.py:90-112).
 
-    The device step evaluates the same rule in FP64 inside the flux kernel's
-    last block (``pf5d_adaptive_dt`` in csrc/pf5d_device.cuh); this host copy
-    serves callers that drive the loop from Python with a host ``xdotmax``.
+    The device step evaluates the same rule in FP64 in a one-block kernel
+    after each rate launch (``adaptive_dt`` in csrc/pf5d_device.cuh); this
+    host copy serves callers that drive the loop from Python with a host
+    ``xdotmax``.
     """
     if xdotmax is None or xdotmax <= 0.0:
         dt_raw = dt_current
