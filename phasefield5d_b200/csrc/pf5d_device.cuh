@@ -263,12 +263,6 @@ __host__ __device__ inline double adaptive_dt(double dt, double xdotmax, double 
   return m;
 }
 
-// atomicMax for non-negative doubles (their bit patterns order like the values).
-__device__ __forceinline__ void atomic_max_nonneg(double *addr, double v) {
-  atomicMax(reinterpret_cast<unsigned long long *>(addr),
-            static_cast<unsigned long long>(__double_as_longlong(v)));
-}
-
 // Block-wide max of non-negative values (NaN already filtered by the caller).
 template <int NT>
 __device__ __forceinline__ double block_max(double v, double *red) {

@@ -5,7 +5,6 @@
 // shared table window, and the compensated-update helpers.
 #pragma once
 
-#include <climits>
 
 #include <cufft.h>
 

@@ -11,31 +11,10 @@
 // before, so the result never depends on the box.
 #pragma once
 
-#include <climits>
 
 #include "pf5d_device.cuh"
 
 namespace pf5d {
-
-// Block-wide minimum of 4 ints (INT_MAX = no candidate).  `red` holds
-// 4 * (NT/32) ints; returns the minimum in out[4] (shared) after a barrier.
-template <int NT>
-__device__ __forceinline__ void block_min4(int v[S], int *red, int *out, int tid) {
-#pragma unroll
-  for (int a = 0; a < S; ++a)
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) v[a] = min(v[a], __shfl_xor_sync(0xffffffffu, v[a], o));
-  if ((tid & 31) == 0)
-#pragma unroll
-    for (int a = 0; a < S; ++a) red[(tid >> 5) * S + a] = v[a];
-  __syncthreads();
-  if (tid < S) {
-    int m = INT_MAX;
-    for (int w = 0; w < NT / 32; ++w) m = min(m, red[w * S + tid]);
-    out[tid] = m;
-  }
-  __syncthreads();
-}
 
 // Copy the W^4 node box starting at node `lo` (shared) from the global
 // table into `win`: node (a,b,c,d) of the box at ((a*W+b)*W+c)*W+d, each
