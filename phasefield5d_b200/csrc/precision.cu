@@ -692,7 +692,8 @@ const std::vector<Variant32> &variants32() {
       make_split_variant32<32, 8, 4, 4>(), make_split_variant32<32, 16, 2, 4>(),
       make_variant32<32, 8, 3, false, true, true>(), make_variant32<32, 16, 2, false, true, true>(),
       make_variant32<32, 8, 3, false, false, true>(), make_variant32<32, 16, 2, false, false, true>(),
-      make_split_variant32<32, 8, 4, 4, true>(), make_split_variant32<32, 16, 2, 4, true>()};
+      make_split_variant32<32, 8, 4, 4, true>(), make_split_variant32<32, 16, 2, 4, true>(),
+      make_split_variant32<32, 16, 2, 5, true>(), make_split_variant32<32, 16, 2, 6, true>()};
   return v;
 }
 
