@@ -269,26 +269,11 @@ def compute_initial_kinetics(initial_composition, resolution, kappa_value, kappa
     return 1.0 / rate, kmax
 
 
-# ---------------------------------------------------------------------------
-# Simplex snapping helper used by sweeps (phasefield5d/solver/system.py:64-73)
-# ---------------------------------------------------------------------------
-
-def snap_to_grid_floor(comp, step=0.01):
-    comp = np.asarray(comp, dtype=float).copy()
-    scale = 1.0 / step
-    np.clip(comp, 0.0, 1.0, out=comp)
-    sums = comp.sum(axis=-1, keepdims=True)
-    rows = sums[:, 0] > 1.0
-    if np.any(rows):
-        comp[rows] /= sums[rows]
-    return np.floor(comp * scale + 1e-9).astype(int) / scale
-
-
 __all__ = [
     "round_to_first_nonzero", "round_down_to_first_nonzero", "apply_fluctuations",
     "get_time_increment", "cahn_hilliard_cfl_dt", "apply_adaptive_time",
     "get_system_dimensions", "build_fourier_grid_1d_along_direction",
     "build_fourier_grid_2d_in_plane", "build_fourier_grid_3d", "build_fourier_grid_for",
     "calculate_wavenumber_cutoff", "max_growth_rate_scan", "dyadic_mobility_matrix",
-    "compute_initial_kinetics", "snap_to_grid_floor",
+    "compute_initial_kinetics",
 ]

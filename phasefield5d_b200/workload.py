@@ -156,6 +156,93 @@ class SolveConfig:
     ic_seed: int = 2
     shape: tuple | None = None     # override mw*ppw cells per axis (batched solves)
     n_k: int = 10_000
+    # the reference driver's loop and save-schedule options
+    # (driver.run_simulation); they do not change the device step
+    elements: tuple = tuple(ELEMENTS)
+    atomic_radius_tag: str = "senkov"
+    time_linear_end_multiplier: float = 100.0
+    early_stage_frames: int = 100
+    late_burst_duration_ctld: int = 100
+    late_burst_frames: int = 700
+    late_tail_frames: int = 300
+
+    @classmethod
+    def from_simulation_config(cls, sim, **overrides):
+        """The solve described by the reference's ``SimulationConfig``
+        (phasefield5d/solver/config.py:30-71, e.g. from its
+        ``parse_args_to_config``), taken as it is.
+
+        Mapped: elements (must be Fe, Mn, Ni, Co, Cu -- the system the
+        synthetic tables and molar volumes describe), temperature ("873K" or
+        a number, K), resolution, system_dim, initial_composition,
+        fluctuation, mw, ppw, kappa_value, kappa_i, include_cubic_anisotropy,
+        direction, total_timesteps, steps_per_ctld,
+        time_linear_end_multiplier, lower_limit, upper_limit, safety and the
+        save schedule (early_stage_frames, late_burst_duration_ctld,
+        late_burst_frames, late_tail_frames); the reference loop is always
+        adaptive.  Accepted without effect on the device step: threads,
+        fft_workers (host thread counts), log_name, atomic_radius_tag (the
+        synthetic workload draws its Vegard misfits from ``misfit_seed``),
+        same_initial_configurations (the initial field is always seeded from
+        ``ic_seed``).  Rejected with ValueError: a different element set, a
+        ``data_path`` (tables on disk are read by the caller and passed to
+        ``Stepper`` as a dense grid), a ``load_path`` resume, an
+        unparseable temperature or a dimension other than 1, 2 or 3.
+        ``overrides`` set any SolveConfig field afterwards (seeds, shape,
+        elastic constants)."""
+        elements = tuple(str(e).strip() for e in sim.elements)
+        if tuple(e.lower() for e in elements) != tuple(e.lower() for e in ELEMENTS):
+            raise ValueError(f"elements {list(elements)}: the synthetic CALPHAD tables and molar "
+                             f"volumes describe {','.join(ELEMENTS)} only")
+        if str(getattr(sim, "data_path", "") or ""):
+            raise ValueError("data_path: CALPHAD tables on disk are read by the caller and "
+                             "passed to Stepper as a dense grid; this config builds the "
+                             "synthetic table")
+        if str(getattr(sim, "load_path", "") or ""):
+            raise ValueError("load_path: resuming from a saved state is done by loading the "
+                             "state and passing its field to Stepper")
+        temp = str(sim.temperature).strip()
+        try:
+            temperature = float(temp[:-1] if temp[-1:] in ("K", "k") else temp)
+        except ValueError:
+            raise ValueError(f"temperature {sim.temperature!r} is not a number of kelvin") from None
+        dim = int(sim.system_dim)
+        if dim not in (1, 2, 3):
+            raise ValueError(f"Unsupported system_dim={dim}. Choose 1, 2, or 3.")
+        cfg = cls(
+            system_dim=dim,
+            initial_composition=tuple(float(v) for v in np.asarray(sim.initial_composition,
+                                                                    dtype=float).reshape(-1)),
+            fluctuation=float(sim.fluctuation), mw=int(sim.mw), ppw=int(sim.ppw),
+            kappa_value=float(sim.kappa_value),
+            kappa_i=tuple(float(v) for v in np.asarray(sim.kappa_i, dtype=float).reshape(-1)),
+            resolution=float(sim.resolution), temperature=temperature,
+            include_cubic_anisotropy=bool(sim.include_cubic_anisotropy),
+            direction=tuple(int(v) for v in np.asarray(sim.direction).reshape(-1)),
+            steps_per_ctld=int(sim.steps_per_ctld), total_timesteps=int(sim.total_timesteps),
+            lower_limit=float(sim.lower_limit), upper_limit=float(sim.upper_limit),
+            safety=float(sim.safety), adaptive=True, elements=elements,
+            atomic_radius_tag=str(sim.atomic_radius_tag),
+            time_linear_end_multiplier=float(sim.time_linear_end_multiplier),
+            early_stage_frames=int(sim.early_stage_frames),
+            late_burst_duration_ctld=int(sim.late_burst_duration_ctld),
+            late_burst_frames=int(sim.late_burst_frames),
+            late_tail_frames=int(sim.late_tail_frames))
+        for k, v in overrides.items():
+            if not hasattr(cfg, k):
+                raise ValueError(f"SolveConfig has no field {k!r}")
+            setattr(cfg, k, v)
+        if len(cfg.initial_composition) != 4 or len(cfg.kappa_i) != 4:
+            raise ValueError("initial_composition and kappa_i need 4 values")
+        return cfg
+
+    def save_schedule(self):
+        """Keyword arguments of ``driver.run_simulation`` for this solve's
+        save schedule (examples/simulate.py:285-294)."""
+        return dict(early_stage_frames=self.early_stage_frames,
+                    late_burst_duration_ctld=self.late_burst_duration_ctld,
+                    late_burst_frames=self.late_burst_frames,
+                    late_tail_frames=self.late_tail_frames, adaptive=self.adaptive)
 
 
 @dataclass

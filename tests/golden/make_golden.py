@@ -2,7 +2,7 @@
 
 Run in a container where the reference source tree is available:
 
-    python tests/golden/make_golden.py [--ref /path/to/phasefield5d]
+    python tests/golden/make_golden.py --ref /path/to/phasefield5d
 
 It imports the reference read-only (with the import-only matplotlib stand-in
 in ``_mplstub``), feeds its hot-path functions seeded inputs, and writes:
@@ -19,7 +19,9 @@ in ``_mplstub``), feeds its hot-path functions seeded inputs, and writes:
                           rank-1 factor, B(k) samples) for the named workloads;
 * ``fullres.json``     -- SHA-256 digests of reference outputs at the full
                           41^4-table resolution (1D 1280 and 2D 512² steps),
-                          guarded by a digest of the regenerated table.
+                          guarded by a digest of the regenerated table;
+* ``sim_configs.json`` -- SimulationConfig objects parsed by the reference's
+                          own parse_args_to_config from seeded command lines.
 
 Tables come from ``phasefield5d_b200.workload.make_table`` (the synthetic
 regular-solution table), so the same inputs can be rebuilt by the tests.
@@ -371,12 +373,64 @@ def gen_save(ref, out_path):
         json.dump(dict(schedule=cases, npz=npz, trace_csv=csv_text, trace_info=info), f, indent=1)
 
 
+# Command lines of examples/simulate.py whose parsed SimulationConfig the
+# adapter test replays: the defaults, the named workloads' settings, and
+# options the adapter must reject.
+CONFIG_ARGVS = [
+    [],
+    ["--system_dim", "2", "--resolution", "0.025", "--initial_composition", "0.1,0.2,0.3,0.2",
+     "--mw", "32", "--ppw", "16", "--kappa_value", "7.6e-15", "--total_timesteps", "20000"],
+    ["--system_dim", "3", "--resolution", "0.02", "--mw", "16", "--kappa_i", "1,0.5,2,1",
+     "--direction", "1,1,0", "--temperature", "973K", "--no_include_cubic_anisotropy",
+     "--lower_limit", "2e-5", "--upper_limit", "5e-4", "--safety", "0.05",
+     "--early_stage_frames", "50", "--late_burst_duration_ctld", "40",
+     "--late_burst_frames", "300", "--late_tail_frames", "200", "--threads", "8",
+     "--fft_workers", "-1", "--time_linear_end_multiplier", "50"],
+    ["--elements", "Fe,Cr,Ni,Co,Mn"],
+    ["--data_path", "data/FeMnNiCoCu_fcc"],
+    ["--load_path", "run/data/state_000100.npz"],
+]
+
+
+def gen_configs(ref, out_path):
+    """SimulationConfig objects built by the reference's own
+    parse_args_to_config (phasefield5d/solver/config.py:146-184), stored as
+    field dicts (arrays as nested lists)."""
+    import dataclasses
+    import importlib.util
+    spec = importlib.util.spec_from_file_location(
+        "pf5d_ref_config", os.path.join(ref, "phasefield5d", "solver", "config.py"))
+    C = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(C)
+    cases = []
+    for argv in CONFIG_ARGVS:
+        cfg = C.parse_args_to_config(argv)
+        fields = {}
+        for f in dataclasses.fields(cfg):
+            v = getattr(cfg, f.name)
+            fields[f.name] = v.tolist() if isinstance(v, np.ndarray) else v
+        arrays = [f.name for f in dataclasses.fields(cfg)
+                  if isinstance(getattr(cfg, f.name), np.ndarray)]
+        cases.append(dict(argv=argv, fields=fields, arrays=arrays))
+    with open(out_path, "w") as f:
+        json.dump(dict(field_order=[f.name for f in dataclasses.fields(C.SimulationConfig)],
+                       cases=cases), f, indent=1)
+
+
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("--ref", default="/root/reference")
+    ap.add_argument("--ref", default=os.environ.get("PHASEFIELD5D_REF"),
+                    help="path of the phasefield5d source tree (default: $PHASEFIELD5D_REF)")
     ap.add_argument("--only-save", action="store_true",
                     help="regenerate only the save-step host logic fixture")
+    ap.add_argument("--only-configs", action="store_true",
+                    help="regenerate only the parsed SimulationConfig fixture")
     args = ap.parse_args()
+    if not args.ref:
+        ap.error("give the reference source tree with --ref or $PHASEFIELD5D_REF")
+    gen_configs(args.ref, os.path.join(HERE, "sim_configs.json"))
+    if args.only_configs:
+        return
     R = import_reference(args.ref)
     gen_save(args.ref, os.path.join(HERE, "save_io.json"))
     if args.only_save:
