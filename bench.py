@@ -15,8 +15,11 @@ and out to pinned host memory every step, a CPU baseline (the oracle on a
 bounded sample of the same workload), the SM clocks sampled during the timed
 region, and -- at N=1, unless ``--forms none`` -- the other forms:
 ``forms.fp32c_same_workload`` (precision form + its accuracy report),
-``forms.batch64`` (the 64-solve batched form against 64 plain FP64 steppers)
-and ``forms.serving`` (p50/p99 time to solution at several Poisson rates).
+``forms.batch64`` (the 64-solve batched form against 64 plain FP64 steppers),
+``forms.serving`` (p50/p99 time to solution at several Poisson rates),
+``forms.3d256`` (the 3D 256^3 workload, 51^4 table, in both forms with their
+rooflines and the 5,000-step accuracy report) and ``forms.1d1280`` (the 1D
+1280 fixed-dt workload in both forms).
 
 ``--impl reference`` times the reference algorithm's CPU implementation (the
 oracle restatement of the Numba kernels + scipy FFT, all host threads) on the
@@ -75,10 +78,15 @@ def parse():
                     help="plain FP64 (bit-faithful) or FP32-compensated form")
     ap.add_argument("--accuracy-steps", type=int, default=2000,
                     help="steps of the FP32c-vs-FP64 accuracy report")
-    ap.add_argument("--cpu-steps", type=int, default=3, help="steps in the CPU-baseline sample")
+    ap.add_argument("--cpu-steps", type=int, default=None,
+                    help="steps in the CPU-baseline sample (default: --steps, the reference "
+                         "arm's sample; at most as many as fit in about 20 s)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--forms", default="fp32c,batch,serve",
-                    help="extra measurements at N=1 (comma list of fp32c, batch, serve; 'none')")
+    ap.add_argument("--forms", default="fp32c,batch,serve,3d,1d",
+                    help="extra measurements at N=1 (comma list of fp32c, batch, serve, 3d, 1d; "
+                         "'none')")
+    ap.add_argument("--accuracy-steps-3d", type=int, default=5000,
+                    help="steps of the 3D 256^3 FP32c-vs-FP64 accuracy report")
     ap.add_argument("--batch-steps", type=int, default=1000,
                     help="timed steps of the 64-solve batched form (and its FP64 comparison)")
     ap.add_argument("--serve-requests", type=int, default=12)
@@ -206,29 +214,44 @@ def cpu_threads():
     return O.num_threads()
 
 
-def time_oracle(prob, steps, warmup):
-    """Reference algorithm on the host cores: (grid-point steps/s, seconds)."""
+def time_oracle(prob, steps, warmup, budget_s=None):
+    """Reference algorithm on the host cores: (grid-point steps/s, seconds,
+    steps timed).  With ``budget_s`` the sample stops early once that much
+    time has passed (at least one step is timed)."""
     from oracle.oracle import OracleStepper
     st = OracleStepper.from_problem(prob, fft_workers=-1)
     for _ in range(warmup):
         st.step()
     t0 = time.perf_counter()
-    for _ in range(steps):
+    done = 0
+    while done < steps:
         st.step()
+        done += 1
+        if budget_s is not None and time.perf_counter() - t0 > budget_s:
+            break
     dt = time.perf_counter() - t0
-    return prob.n_points * steps / dt, dt
+    return prob.n_points * done / dt, dt, done
+
+
+def cpu_baseline(prob, args, workload_name, budget_s=20.0):
+    """The oracle on the host cores, on a bounded sample of the workload."""
+    steps = args.cpu_steps if args.cpu_steps is not None else args.steps
+    val, secs, done = time_oracle(prob, steps, 1, budget_s=budget_s)
+    return {"value": val, "unit": "grid-point steps/s", "cores": cpu_threads(), "kind": "port",
+            "sample": f"{done} steps ({secs:.1f} s) of the full {workload_name} after 1 warm-up "
+                      f"(oracle C restatement + scipy FFT, all host threads)"}
 
 
 def run_reference(args, rank):
     if rank != 0:
         return
     prob = build_problem(args.workload)
-    value, secs = time_oracle(prob, args.steps, args.warmup)
-    sample = f"{args.steps} steps of the full {WORKLOADS[args.workload][0]} after {args.warmup} warm-up"
+    value, secs, done = time_oracle(prob, args.steps, args.warmup)
+    sample = f"{done} steps of the full {WORKLOADS[args.workload][0]} after {args.warmup} warm-up"
     line = {
         "impl": "reference", "metric": "grid-point steps/s", "value": value,
         "unit": "grid-point steps/s", "n_gpus": args.gpus, "steps": args.steps,
-        "warmup": args.warmup, "ms_per_step": 1e3 * secs / args.steps, "higher_is_better": True,
+        "warmup": args.warmup, "ms_per_step": 1e3 * secs / done, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
         "config": {"workload": WORKLOADS[args.workload][0], "shape": list(prob.shape),
                    "parallelism": "cpu-threads"},
@@ -277,45 +300,65 @@ def _stepper_timing(prob, precision, args, flush, torch):
         rate.append((a, b))
     torch.cuda.synchronize()
     rate_ms = sum(a.elapsed_time(b) for a, b in rate) / len(rate)
-    variant = st.variant
+    variant, kernels = st.variant, st.rate_kernels
     st.close()
-    return step_ms, rate_ms, variant
+    return step_ms, rate_ms, variant, kernels
+
+
+def form_workload(prob, workload, precision, args, flush, torch, accuracy_steps=0):
+    """One workload in one form: device-resident steps timed alone with L2
+    flushed between them, and the rate stage launched alone (its roofline:
+    algorithmic bytes over CUDA-event time against the measured HBM peak,
+    beside the DRAM traffic of the committed ncu capture).  With
+    ``accuracy_steps`` (FP32c only) the accuracy report against the plain
+    FP64 form over that many steps."""
+    from phasefield5d_b200.precision import compare_forms
+    peak, peak_kind = measured_peak()
+    P = prob.n_points
+    fp32c = precision == "fp32c"
+    step_ms, rate_ms, variant, kernels = _stepper_timing(prob, precision, args, flush, torch)
+    per_rate = RATE_BYTES_FP32C if fp32c else RATE_BYTES_FP64
+    per_step = STEP_BYTES_FP32C if fp32c else STEP_BYTES_FP64
+    if prob.lvec is None:
+        per_rate -= 4 if fp32c else 8
+        per_step -= 24 if fp32c else 48
+    rate_bytes = per_rate * P
+    value = P / (step_ms * 1e-3)
+    achieved = rate_bytes / (rate_ms * 1e-3) / 1e9
+    out = {"value": value, "unit": "grid-point steps/s", "ms_per_step": step_ms,
+           "shape": list(prob.shape), "precision": precision,
+           "l2": "flushed (256 MiB write) between timed steps", "rate_variant": variant,
+           "roofline": {"bound": "hbm", "kernel": kernels, "ms_per_launch": rate_ms,
+                        "achieved": achieved, "peak": peak, "peak_kind": peak_kind,
+                        "unit": "GB/s", "frac": achieved / peak,
+                        "algorithmic_bytes_per_launch": rate_bytes,
+                        "traffic": committed_traffic("rate", workload, precision)},
+           "step_roofline": {"bytes_per_grid_point_step": per_step,
+                             "achieved_gbs": per_step * value / 1e9,
+                             "frac": per_step * value / 1e9 / peak}}
+    if fp32c and accuracy_steps > 0:
+        out["accuracy_vs_fp64"] = compare_forms(prob, accuracy_steps)
+    return out
 
 
 def form_fp32c(prob, args, flush, torch):
     """FP32-compensated form on the headline workload, with its accuracy
     report against the plain FP64 form (max/RMS error, mass drift)."""
-    from phasefield5d_b200.precision import compare_forms
-    peak, peak_kind = measured_peak()
-    P = prob.n_points
-    step_ms, rate_ms, variant = _stepper_timing(prob, "fp32c", args, flush, torch)
-    rate_bytes = RATE_BYTES_FP32C * P
-    value = P / (step_ms * 1e-3)
-    out = {"value": value, "unit": "grid-point steps/s", "ms_per_step": step_ms,
-           "l2": "flushed (256 MiB write) between timed steps", "rate_variant": variant,
-           "rate_kernel": {"ms_per_launch": rate_ms,
-                           "achieved_gbs": rate_bytes / (rate_ms * 1e-3) / 1e9,
-                           "algorithmic_bytes_per_launch": rate_bytes,
-                           "frac": rate_bytes / (rate_ms * 1e-3) / 1e9 / peak,
-                           "peak_kind": peak_kind},
-           "step_roofline": {"bytes_per_grid_point_step": STEP_BYTES_FP32C,
-                             "achieved_gbs": STEP_BYTES_FP32C * value / 1e9,
-                             "frac": STEP_BYTES_FP32C * value / 1e9 / peak}}
-    if args.accuracy_steps > 0:
-        out["accuracy_vs_fp64"] = compare_forms(prob, args.accuracy_steps)
+    return form_workload(prob, args.workload, "fp32c", args, flush, torch,
+                         accuracy_steps=args.accuracy_steps)
+
+
+def form_named(workload, args, flush, torch, accuracy_steps):
+    """A named workload other than the headline's (``3d``: 3D 256^3 with the
+    51^4 table, the one whose field exceeds L2; ``1d``: 1D 1280 at fixed dt)
+    in the plain FP64 and FP32c forms, with FP32c's accuracy report."""
+    prob = build_problem(workload)
+    out = {"workload": WORKLOADS[workload][0]}
+    for prec in ("fp64", "fp32c"):
+        out[prec] = form_workload(prob, workload, prec, args, flush, torch,
+                                  accuracy_steps=accuracy_steps if prec == "fp32c" else 0)
+    out["speedup_fp32c_vs_fp64"] = out["fp32c"]["value"] / out["fp64"]["value"]
     return out
-
-
-def rate_kernel_label(dim, fp32c):
-    """Name of the rate stage's kernel family for the roofline entry."""
-    p = "k32_" if fp32c else "k_"
-    if dim == 1:
-        return p + "rate_1d"
-    fused = p + ("rate_tile2d" if dim == 2 else "rate_march3d")
-    flux = p + ("rate_tile2d" if dim == 2 else ("flux_march3d" if fp32c else "rate_march3d"))
-    chem = "k32_chem" if fp32c else "k_chem64"
-    return (f"{fused} (fused mu/M + flux divergence) or {chem} + {flux} (split), "
-            "the autotuned variant; plus the one-block dt kernel")
 
 
 def profiled_step(torch, step, flush):
@@ -498,6 +541,7 @@ def run_ours(args, rank, world, local_rank):
     step_ms = [e0.elapsed_time(e1) for e0, e1 in ev]
     total_ms = sum(step_ms)
     launches_per_step = st.launches_per_step
+    rate_kernels = st.rate_kernels
     state = st.state()
     if state["halted"]:
         raise RuntimeError(f"stepper halted during the benchmark: {state}")
@@ -579,11 +623,7 @@ def run_ours(args, rank, world, local_rank):
     achieved = rate_bytes / (stage_ms["rate"] * 1e-3) / 1e9
     cpu = None
     if not args.no_cpu_baseline and world == 1:        # the CPU baseline: N = 1 only
-        cpu_val, _ = time_oracle(prob, args.cpu_steps, 1)
-        cpu = {"value": cpu_val, "unit": "grid-point steps/s", "cores": cpu_threads(),
-               "kind": "port",
-               "sample": f"{args.cpu_steps} steps of the full {WORKLOADS[args.workload][0]} "
-                         f"after 1 warm-up (oracle C restatement + scipy FFT)"}
+        cpu = cpu_baseline(prob, args, WORKLOADS[args.workload][0])
     line = {
         "metric": "grid-point steps/s", "value": value, "unit": "grid-point steps/s",
         "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
@@ -595,7 +635,7 @@ def run_ours(args, rank, world, local_rank):
                    "table_nodes_per_axis": int(prob.grid.shape[0]), "omega_seed": prob.omega_seed,
                    "l2": "flushed (256 MiB write) between timed steps",
                    "parallelism": f"replicas x{world}" if world > 1 else "single solve"},
-        "roofline": {"bound": "hbm", "kernel": rate_kernel_label(prob.dim, fp32c),
+        "roofline": {"bound": "hbm", "kernel": rate_kernels,
                      "achieved": achieved, "peak": peak, "peak_kind": peak_kind, "unit": "GB/s",
                      "frac": achieved / peak, "traffic": committed_traffic("rate", args.workload, args.precision),
                      "algorithmic_bytes_per_launch": rate_bytes,
@@ -632,6 +672,10 @@ def run_ours(args, rank, world, local_rank):
             extra["batch64"] = form_batch(args, flush, torch)
         if "serve" in forms:
             extra["serving"] = form_serve(args)
+        if "3d" in forms and args.workload != "3d":
+            extra["3d256"] = form_named("3d", args, flush, torch, args.accuracy_steps_3d)
+        if "1d" in forms and args.workload != "1d":
+            extra["1d1280"] = form_named("1d", args, flush, torch, 10_000)
         line["forms"] = extra
     print(json.dumps(line), flush=True)
 

@@ -50,9 +50,15 @@ typedef enum {
 #define PF5D_FLAG_OOB_HARD     0x02u  /* |violation| > tol_hard (1e-3)              */
 #define PF5D_FLAG_OOB_SOFT     0x04u  /* |violation| > tol_soft (1e-5)              */
 #define PF5D_FLAG_NN_FAR       0x08u  /* nearest-row distance > max_nn_dist         */
-#define PF5D_FLAG_NN_TRUNCATED 0x10u  /* nearest-row search window may have missed */
+#define PF5D_FLAG_NN_TRUNCATED 0x10u  /* nearest-row search found no present node   */
 #define PF5D_FLAG_NN_USED      0x20u  /* some point took the nearest-row fallback   */
-#define PF5D_FLAG_HALTED       0x40u  /* step loop stopped at an OOB check          */
+#define PF5D_FLAG_HALTED       0x40u  /* step loop stopped (OOB check or an NN error) */
+#define PF5D_FLAG_NN_NONFINITE 0x80u  /* a fallback point had a NaN/inf component   */
+/* The nearest-row search is exact for every finite point (it widens its
+ * window until the nearest present node is proven).  NN_FAR, NN_TRUNCATED and
+ * NN_NONFINITE are errors where the reference raises (RuntimeError for the
+ * distance, ValueError from cKDTree.query for a non-finite point): the step
+ * loop halts before that step's update, and the Python mirror raises. */
 
 const char *pf5d_last_error(void);
 int32_t pf5d_version(void);
@@ -268,6 +274,11 @@ int32_t pf5d_stepper_variant_count(const pf5d_stepper *h);
  * (rate kernel(s), dt controller, update, and the B(k) multiply when
  * elasticity is on; cuFFT's own kernels not counted); 0 for a null stepper. */
 int32_t pf5d_stepper_launches_per_step(const pf5d_stepper *h);
+/* The kernel instances one rate stage of the current variant launches, as
+ * profilers name them ("k_rate_tile2d<32, 8, 2, 1, 1, 0, 352, 1, 0> +
+ * k_dt_finish"); the text is owned by the stepper and valid until the next
+ * call on it.  No counterpart in the reference (a diagnostic). */
+const char *pf5d_stepper_rate_kernels(pf5d_stepper *h);
 /* Re-derive internal state after the caller modified X (e.g. a restart). */
 pf5d_status pf5d_stepper_reset(pf5d_stepper *h, double dt, double time, void *stream);
 pf5d_status pf5d_stepper_destroy(pf5d_stepper *h);

@@ -29,6 +29,7 @@ FLAG_NN_FAR = 0x08
 FLAG_NN_TRUNCATED = 0x10
 FLAG_NN_USED = 0x20
 FLAG_HALTED = 0x40
+FLAG_NN_NONFINITE = 0x80
 
 STAGE_RATE, STAGE_UPDATE, STAGE_FFT_FWD, STAGE_BMUL, STAGE_FFT_INV = 0, 1, 2, 3, 4
 PRECISION_FP64, PRECISION_FP32C = 0, 1
@@ -114,6 +115,7 @@ _SIGS = {
     "pf5d_stepper_set_variant": (_i32, [_vp, _i32]),
     "pf5d_stepper_variant_count": (_i32, [_vp]),
     "pf5d_stepper_launches_per_step": (_i32, [_vp]),
+    "pf5d_stepper_rate_kernels": (ctypes.c_char_p, [_vp]),
     "pf5d_stepper_step_save": (_i32, [_vp, ctypes.POINTER(SaveDiag), _vp]),
     "pf5d_batch_variant_count": (_i32, []),
     "pf5d_stepper_reset": (_i32, [_vp, _f64, _f64, _vp]),
@@ -174,8 +176,31 @@ def check(status, what=""):
     if status == PF5D_ERR_DIM:
         raise ValueError(msg)
     if status == PF5D_ERR_NN_DISTANCE:
-        raise RuntimeError("Some compositions are outside the CALPHAD domain (KD-tree).")
+        raise RuntimeError(NN_FAR_MSG)
     raise RuntimeError(f"pf5d error {status}: {msg}")
+
+
+NN_NONFINITE_MSG = "'x' must be finite, check for nan or inf values"
+NN_FAR_MSG = "Some compositions are outside the CALPHAD domain (KD-tree)."
+
+
+def nn_flags(flags):
+    """Decode the nearest-row fallback bits of a device status word."""
+    return {"nn_used": bool(flags & FLAG_NN_USED), "nn_far": bool(flags & FLAG_NN_FAR),
+            "nn_nonfinite": bool(flags & FLAG_NN_NONFINITE),
+            "nn_no_row": bool(flags & FLAG_NN_TRUNCATED)}
+
+
+def raise_nn_errors(flags, check_far=True):
+    """Raise where the reference's fallback raises: ValueError for a
+    non-finite composition (cKDTree.query), RuntimeError for a row farther
+    than max_nn_dist (interpolation.py:207-208) or a table without rows."""
+    if flags & FLAG_NN_NONFINITE:
+        raise ValueError(NN_NONFINITE_MSG)
+    if check_far and flags & FLAG_NN_FAR:
+        raise RuntimeError(NN_FAR_MSG)
+    if flags & FLAG_NN_TRUNCATED:
+        raise RuntimeError("nearest-row fallback: the table has no rows")
 
 
 def stream_handle(stream=None):

@@ -131,10 +131,13 @@ class BatchStepper:
         _lib.check(self.L.pf5d_batch_advance(self.h, int(n_steps), self._s()), "advance")
 
     def states(self):
+        """Per-solve step state, with the nearest-row fallback bits decoded
+        as in ``Stepper.state`` (a solve whose fallback failed is halted)."""
         out = (_lib.StepState * len(self.problems))()
         _lib.check(self.L.pf5d_batch_states(self.h, out, self._s()), "states")
         return [dict(dt=s.dt, time=s.time, xdotmax=s.xdotmax, step=int(s.step),
-                     flags=int(s.flags), halted=bool(s.halted)) for s in out]
+                     flags=int(s.flags), halted=bool(s.halted), **_lib.nn_flags(int(s.flags)))
+                for s in out]
 
     def field(self, i):
         p = self.problems[i]

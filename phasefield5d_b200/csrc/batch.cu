@@ -184,7 +184,7 @@ __global__ void __launch_bounds__(TX * TY, MINB)
                                                           &flags, tid);
     else
       vmax = tile1d32_body<NT>(B, P, local, reinterpret_cast<float *>(work), &flags, tid);
-    if (flags) atomicOr(&P.st->flags, flags);
+    raise_rate_flags(P.st, flags);
     double *red = reinterpret_cast<double *>(work);    // free after the body's last barrier
     __syncthreads();
     finish_slot32(vmax, red, tile_max + t);
@@ -855,7 +855,6 @@ pf5d_status pf5d_batch_create(const pf5d_batch_solve *solves, int32_t nsolves,
     T.inv_step = 1.0 / resolution;
     T.inv_step_f = (float)T.inv_step;
     T.threshold = 1.0 - 4.0 * resolution - 1e-9;
-    T.exact_d2 = (1.99 * resolution) * (1.99 * resolution);
     T.max_nn_dist = q.max_nn_dist;
     double sx = 0.0;
     for (int c = 0; c < S; ++c) {

@@ -364,7 +364,6 @@ pf5d_status pf5d_interp4d(const double *comp, int64_t npts, const double *grid, 
   T.stride = node_stride;
   T.inv_step = 1.0 / resolution;
   T.threshold = 1.0 - 4.0 * resolution - 1e-9;
-  T.exact_d2 = (1.99 * resolution) * (1.99 * resolution);
   T.max_nn_dist = max_nn_dist;
   k_interp4d<<<grid_for(npts, 128), 128, 0, as_stream(stream)>>>(comp, npts, T, out, out_stride,
                                                                   mask, flags);

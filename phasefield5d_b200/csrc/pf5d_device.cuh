@@ -36,7 +36,6 @@ struct Table {
   int stride;               // doubles per node
   double inv_step;          // 1.0 / resolution
   double threshold;         // 1.0 - 4.0*resolution - 1e-9
-  double exact_d2;          // (1.99*resolution)^2: window search is exact below this
   double max_nn_dist;       // <= 0: unchecked
 };
 
@@ -112,79 +111,138 @@ __device__ __forceinline__ void interp_linear(const Table &T, const double x[S],
 // (interpolation.py:203-209, cKDTree over the row compositions); returns the
 // node index (the caller reads the row).
 //
-// Rows sit on grid nodes, so the nearest row is the nearest present node.
-// Every node within two cells of x along each axis is inside the
-// [floor(u)-2, floor(u)+2]^4 window searched here; when the best distance is
-// below 1.99 cells the answer is therefore the exact nearest node (as long
-// as floor(u) itself is a present node, true for sum(x) < 1 + res on a full
-// simplex table).  Farther results set PF5D_FLAG_NN_TRUNCATED.  Distances
-// are accumulated as sum_d (x_d - c_d)^2 in axis order; on an exact tie the
-// first node in lexicographic order wins.
+// Rows sit on grid nodes, so the nearest row is the nearest present node
+// (the table's first prop is NaN at absent nodes).  The search is exact for
+// any finite point, on or far off the simplex:
+//   * it scans the window [f_d - r, f_d + r] (clipped to [0, N]) around the
+//     point's clamped cell f_d = clamp(floor(x_d / res), 0, N), r = 2 first;
+//   * every node outside the window lies farther than `gap`, the distance
+//     from x to the nearest excluded coordinate on any axis, so a best
+//     squared distance below gap^2 is the global minimum (the comparison is
+//     made on the same rounded squares the scan computes, so rounding cannot
+//     break it);
+//   * otherwise the window grows (r = 8, 32, ...) until the bound holds or
+//     the window spans the whole table.
+// Per axis the scan walks coordinates upward and stops once a coordinate
+// above x already makes the partial distance exceed the best.  Distances
+// are sum_d (x_d - c_d)^2 in axis order; of exactly equal distances the
+// first node in lexicographic order wins.  A non-finite component returns
+// no node with PF5D_FLAG_NN_NONFINITE (cKDTree.query raises ValueError for
+// it); a table with no present node returns none with NN_TRUNCATED.
 struct NearestNode {
-  int64_t node;        // -1: nothing present in the window
+  int64_t node;        // -1: no node (non-finite point or empty table)
   unsigned flags;      // PF5D_FLAG_NN_*
 };
 
-// The search needs only the node coordinates and a presence probe (the
-// table's first prop is NaN at absent nodes), so it serves FP64 and FP32
-// tables alike: `grid` points at the first prop of node 0, `stride` is in
-// elements of type E.
+// Flags of the fallback that end a step loop where the reference's loop
+// raises: a non-finite composition (ValueError from cKDTree.query), a row
+// farther than max_nn_dist (RuntimeError, interpolation.py:207-208), and a
+// table without rows.
+constexpr unsigned kNNErrorFlags = PF5D_FLAG_NN_FAR | PF5D_FLAG_NN_TRUNCATED | PF5D_FLAG_NN_NONFINITE;
+
+// Record a rate kernel's flags in its step state (flags, halt); the
+// fallback's error flags halt the loop before the step's update.
+template <typename St>
+__device__ __forceinline__ void raise_rate_flags(St *st, unsigned f) {
+  if (!f) return;
+  atomicOr(&st->flags, f);
+  if (f & kNNErrorFlags) atomicExch(&st->halt, 1u);
+}
+
+// The search needs only the node coordinates and a presence probe, so it
+// serves FP64 and FP32 tables alike: `grid` points at the first prop of
+// node 0, `stride` is in elements of type E.
 template <typename E>
 static __device__ __noinline__ NearestNode nearest_node_g(const E *grid, int stride,
                                                           const double *coord, int n_axis,
-                                                          double inv_step, double exact_d2,
-                                                          double max_nn_dist, double x0,
-                                                          double x1, double x2, double x3) {
+                                                          double inv_step, double max_nn_dist,
+                                                          double x0, double x1, double x2,
+                                                          double x3) {
   const double x[S] = {x0, x1, x2, x3};
+  NearestNode r{-1, PF5D_FLAG_NN_USED};
+  if (!(isfinite(x0) && isfinite(x1) && isfinite(x2) && isfinite(x3))) {
+    r.flags |= PF5D_FLAG_NN_NONFINITE;
+    return r;
+  }
   const int N = n_axis - 1;
-  int lo[S], hi[S];
+  const int64_t n = n_axis;
+  int f[S];
 #pragma unroll
   for (int d = 0; d < S; ++d) {
-    double u = x[d] * inv_step;
-    if (!(u > -4.0)) u = -4.0;             // also maps NaN
-    if (!(u < (double)N + 4.0)) u = (double)N + 4.0;
-    const int f = (int)floor(u);
-    lo[d] = max(0, f - 2);
-    hi[d] = min(N, f + 2);
+    const double u = fmin(fmax(x[d] * inv_step, 0.0), (double)N);
+    f[d] = (int)floor(u);
   }
   double best = __longlong_as_double(0x7ff0000000000000LL);   // +inf
   int64_t best_node = -1;
-  const int64_t n = n_axis;
-  for (int k0 = lo[0]; k0 <= hi[0]; ++k0) {
-    const double d0 = x[0] - coord[k0];
-    const double e0 = d0 * d0;
-    for (int k1 = lo[1]; k1 <= hi[1]; ++k1) {
-      const double d1 = x[1] - coord[k1];
-      const double e1 = e0 + d1 * d1;
-      for (int k2 = lo[2]; k2 <= hi[2]; ++k2) {
-        const double d2 = x[2] - coord[k2];
-        const double e2 = e1 + d2 * d2;
-        for (int k3 = lo[3]; k3 <= hi[3]; ++k3) {
-          const double d3 = x[3] - coord[k3];
-          const double e3 = e2 + d3 * d3;
-          if (e3 < best) {
+  for (int rad = 2;; rad *= 4) {
+    int lo[S], hi[S];
+    double gap = __longlong_as_double(0x7ff0000000000000LL);
+    bool whole = true;
+#pragma unroll
+    for (int d = 0; d < S; ++d) {
+      lo[d] = max(0, f[d] - rad);
+      hi[d] = min(N, f[d] + rad);
+      if (lo[d] > 0) {
+        gap = fmin(gap, fmax(x[d] - coord[lo[d] - 1], 0.0));
+        whole = false;
+      }
+      if (hi[d] < N) {
+        gap = fmin(gap, fmax(coord[hi[d] + 1] - x[d], 0.0));
+        whole = false;
+      }
+    }
+    for (int k0 = lo[0]; k0 <= hi[0]; ++k0) {
+      const double d0 = x[0] - coord[k0];
+      const double e0 = d0 * d0;
+      if (e0 > best) {
+        if (d0 < 0.0) break;          // coordinates only move away from here on
+        continue;
+      }
+      for (int k1 = lo[1]; k1 <= hi[1]; ++k1) {
+        const double d1 = x[1] - coord[k1];
+        const double e1 = e0 + d1 * d1;
+        if (e1 > best) {
+          if (d1 < 0.0) break;
+          continue;
+        }
+        for (int k2 = lo[2]; k2 <= hi[2]; ++k2) {
+          const double d2 = x[2] - coord[k2];
+          const double e2 = e1 + d2 * d2;
+          if (e2 > best) {
+            if (d2 < 0.0) break;
+            continue;
+          }
+          for (int k3 = lo[3]; k3 <= hi[3]; ++k3) {
+            const double d3 = x[3] - coord[k3];
+            const double e3 = e2 + d3 * d3;
+            if (e3 > best) {
+              if (d3 < 0.0) break;
+              continue;
+            }
             const int64_t node = ((k0 * n + k1) * n + k2) * n + k3;
-            const E probe = __ldg(grid + node * stride);
-            if (probe == probe) {            // present (not NaN)
-              best = e3;
-              best_node = node;
+            if (e3 < best || node < best_node) {
+              const E probe = __ldg(grid + node * stride);
+              if (probe == probe) {          // present (not NaN)
+                best = e3;
+                best_node = node;
+              }
             }
           }
         }
       }
     }
+    if (whole || (best_node >= 0 && best < gap * gap)) break;
   }
-  NearestNode r{best_node, PF5D_FLAG_NN_USED};
-  if (best_node < 0 || !(best < exact_d2)) r.flags |= PF5D_FLAG_NN_TRUNCATED;
-  if (best_node >= 0 && max_nn_dist > 0.0 && sqrt(best) > max_nn_dist)
-    r.flags |= PF5D_FLAG_NN_FAR;
+  r.node = best_node;
+  if (best_node < 0) r.flags |= PF5D_FLAG_NN_TRUNCATED;
+  else if (max_nn_dist > 0.0 && sqrt(best) > max_nn_dist) r.flags |= PF5D_FLAG_NN_FAR;
   return r;
 }
 
 __device__ __forceinline__ NearestNode nearest_node(const Table &T, double x0, double x1,
                                                     double x2, double x3) {
-  return nearest_node_g<double>(T.grid, T.stride, T.coord, T.n, T.inv_step, T.exact_d2,
-                                T.max_nn_dist, x0, x1, x2, x3);
+  return nearest_node_g<double>(T.grid, T.stride, T.coord, T.n, T.inv_step, T.max_nn_dist, x0,
+                                x1, x2, x3);
 }
 
 // Interpolation with fallback for one point; returns true on the linear branch.

@@ -30,7 +30,7 @@ struct Table32 {
   const double *coord;
   int n;
   int stride;
-  double inv_step, threshold, exact_d2, max_nn_dist;
+  double inv_step, threshold, max_nn_dist;
   float inv_step_f;
   int ib[S];          // floor(X0_d / res)
   float fb[S];        // X0_d / res - floor(X0_d / res)
@@ -140,7 +140,7 @@ __device__ __forceinline__ void interp32(const Rate32 &P, const float d[S], cons
     return;
   }
   const NearestNode r = nearest_node_g<float>(T.grid, T.stride, T.coord, T.n, T.inv_step,
-                                              T.exact_d2, T.max_nn_dist, T.x0[0] + (double)d[0],
+                                              T.max_nn_dist, T.x0[0] + (double)d[0],
                                               T.x0[1] + (double)d[1], T.x0[2] + (double)d[2],
                                               T.x0[3] + (double)d[3]);
   *flags |= r.flags;

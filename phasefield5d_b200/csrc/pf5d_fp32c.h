@@ -25,6 +25,8 @@ pf5d_status s32_mass(Stepper32 *h, double *mean_out, void *stream);
 pf5d_status s32_autotune(Stepper32 *h, int32_t *variant, float *best_ms, void *stream);
 pf5d_status s32_set_variant(Stepper32 *h, int32_t variant);
 int32_t s32_variant_count();
+// Kernel instances of the current variant's rate stage (text owned by h).
+const char *s32_rate_kernels(Stepper32 *h);
 // Save steps: one step up to its rate evaluation plus FP64 copies of the
 // field before the update (X), dX/dt and mu/M (SoA, 9 rows); then the update.
 pf5d_status s32_step_save_inputs(Stepper32 *h, double *X_out, double *dX_out, double *mm_out,

@@ -5,6 +5,7 @@
 #include <cstdarg>
 #include <cstdint>
 #include <cstdio>
+#include <initializer_list>
 #include <string>
 
 #include <cuda_runtime.h>
@@ -16,6 +17,20 @@ namespace pf5d {
 void set_error(const char *fmt, ...);
 
 inline cudaStream_t as_stream(void *s) { return reinterpret_cast<cudaStream_t>(s); }
+
+// A kernel instance as profilers print it, "name<a, b, ...>" (bools as 0/1),
+// so reports can name the exact kernels a variant launches.
+inline std::string kname(const char *name, std::initializer_list<long long> targs) {
+  std::string s = name;
+  s += "<";
+  bool first = true;
+  for (long long v : targs) {
+    if (!first) s += ", ";
+    s += std::to_string(v);
+    first = false;
+  }
+  return s + ">";
+}
 
 // Number of SMs on the current device (cached per device).
 int sm_count();

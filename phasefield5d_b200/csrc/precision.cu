@@ -51,7 +51,7 @@ __global__ void __launch_bounds__(TX * TY, MINB) k32_rate_tile2d(Rate32 P) {
   unsigned flags = 0;
   const float vmax = tile2d32_body<TX, TY, WIN, SORT, SPLIT, PERPOINT>(P, blockIdx.x, blockIdx.y,
                                                                       sm4, &flags, tid);
-  if (flags) atomicOr(&P.st->flags, flags);
+  raise_rate_flags(P.st, flags);
   finish_rate32(P, vmax, Tile2dSmem32<TX, TY, SORT>::red(sm4));
 }
 
@@ -142,7 +142,7 @@ __global__ void __launch_bounds__(TX * TY, MINB) k32_rate_march3d(Rate32 P, int 
 #pragma unroll
     for (int c = 0; c < S; ++c) Jm[c] = Jz[c];
   }
-  if (flags) atomicOr(&P.st->flags, flags);
+  raise_rate_flags(P.st, flags);
   finish_rate32(P, vmax, red);
 }
 
@@ -218,7 +218,7 @@ __global__ void __launch_bounds__(TX) k32_rate_1d(Rate32 P) {
     for (int c = 0; c < S; ++c) out[c] = (Fx[c][tx + 1] - Fx[c][tx]) * P.inv_dx;
     store_rate(P.dX, x0 + tx, out, vmax);
   }
-  if (flags) atomicOr(&P.st->flags, flags);
+  raise_rate_flags(P.st, flags);
   finish_rate32(P, vmax, red);
 }
 
@@ -445,7 +445,7 @@ __global__ void __launch_bounds__(256, MINB) k32_chem(Rate32 P) {
 #pragma unroll
     for (int c = 0; c < NM; ++c) P.mm[(S + c) * P.npts + gq] = M[c];
   }
-  if (flags) atomicOr(&P.st->flags, flags);
+  raise_rate_flags(P.st, flags);
 }
 
 // Copies (cp.async) of one plane's composition hi and mu/M at the tile and
@@ -626,6 +626,7 @@ struct Variant32 {
   void (*set_attrs)();
   void (*launch2d)(dim3, dim3, size_t, cudaStream_t, const Rate32 &);
   void (*launch3d)(dim3, dim3, size_t, cudaStream_t, const Rate32 &, int);
+  std::string (*kernels)(int dim);     // the kernel instances of a 2D/3D rate stage
 };
 
 template <int TX, int TY, int MINB, bool WIN = true, bool SORT = false, bool PP = false>
@@ -649,6 +650,10 @@ Variant32 make_variant32() {
   };
   v.launch3d = [](dim3 g, dim3 b, size_t sm, cudaStream_t s, const Rate32 &P, int zc) {
     launch_pdl(k32_rate_march3d<TX, TY, MINB, WIN, SORT>, g, b, sm, s, P, zc);
+  };
+  v.kernels = [](int dim) {
+    if (dim == 2) return kname("k32_rate_tile2d", {TX, TY, MINB, WIN, SORT, 0, PP});
+    return kname("k32_rate_march3d", {TX, TY, MINB, WIN, SORT});
   };
   return v;
 }
@@ -677,6 +682,11 @@ Variant32 make_split_variant32() {
   v.launch3d = [](dim3 g, dim3 b, size_t sm, cudaStream_t s, const Rate32 &P, int zc) {
     launch_chem32<3, KMINB>(s, P);
     launch_pdl(k32_flux_march3d<TX, TY, MINB, PP>, g, b, sm, s, P, zc);
+  };
+  v.kernels = [](int dim) {
+    const std::string chem = kname("k32_chem", {dim, KMINB}) + " + ";
+    if (dim == 2) return chem + kname("k32_rate_tile2d", {TX, TY, MINB, 0, 0, 1, 0});
+    return chem + kname("k32_flux_march3d", {TX, TY, MINB, PP});
   };
   return v;
 }
@@ -718,6 +728,7 @@ struct Stepper32 {
   size_t smem = 0;
   int zc = 1;
   int variant = 0;
+  std::string kernels;           // text returned by s32_rate_kernels
 };
 
 #define PF5D_CUFFT32(call)                                                         \
@@ -907,7 +918,6 @@ pf5d_status s32_create(const pf5d_stepper_desc *desc, const double *X_init, void
   T.inv_step = 1.0 / desc->resolution;
   T.inv_step_f = (float)T.inv_step;
   T.threshold = 1.0 - 4.0 * desc->resolution - 1e-9;
-  T.exact_d2 = (1.99 * desc->resolution) * (1.99 * desc->resolution);
   T.max_nn_dist = desc->max_nn_dist;
   double sx = 0.0;
   for (int c = 0; c < S; ++c) {
@@ -1071,6 +1081,13 @@ pf5d_status s32_mass(Stepper32 *h, double *mean_out, void *stream) {
 }
 
 int32_t s32_variant_count() { return (int32_t)variants32().size(); }
+
+const char *s32_rate_kernels(Stepper32 *h) {
+  if (h->d.dim == 1) h->kernels = kname("k32_rate_1d", {kTX1_32});
+  else h->kernels = variants32()[h->variant].kernels(h->d.dim);
+  h->kernels += " + k32_dt";
+  return h->kernels.c_str();
+}
 
 int32_t s32_launches_per_step(const Stepper32 *h) {
   const bool split = h->d.dim >= 2 && variants32()[h->variant].split;

@@ -382,7 +382,7 @@ __global__ void __launch_bounds__(256, MINB) k_chem64(RateParams P) {
 #pragma unroll
     for (int c = 0; c < NM; ++c) P.mm[(S + c) * P.npts + gq] = v[S + c];
   }
-  if (flags) atomicOr(&P.st->flags, flags);
+  raise_rate_flags(P.st, flags);
 }
 
 // Fold this thread's max |dX/dt| into the block and store the block's max
@@ -586,7 +586,7 @@ __global__ void __launch_bounds__(NTH, MINB) k_rate_tile2d(RateParams P) {
     o[0] = make_double2(out[0], out[1]);
     o[1] = make_double2(out[2], out[3]);
   }
-  if (flags) atomicOr(&P.st->flags, flags);
+  raise_rate_flags(P.st, flags);
   finish_rate(P, vmax, red);
 }
 
@@ -790,7 +790,7 @@ __global__ void __launch_bounds__(TX * TY, MINB) k_rate_march3d(RateParams P, in
       o[1] = make_double2(out[2], out[3]);
     }
   }
-  if (flags) atomicOr(&P.st->flags, flags);
+  raise_rate_flags(P.st, flags);
   finish_rate(P, vmax, red);
 }
 
@@ -878,7 +878,7 @@ __global__ void __launch_bounds__(TX) k_rate_1d(RateParams P) {
     o[0] = make_double2(out[0], out[1]);
     o[1] = make_double2(out[2], out[3]);
   }
-  if (flags) atomicOr(&P.st->flags, flags);
+  raise_rate_flags(P.st, flags);
   finish_rate(P, vmax, red);
 }
 
@@ -1029,6 +1029,7 @@ struct pf5d_stepper {
   double *diag_ws = nullptr;     // save-step partial rows + mean
   double *partial = nullptr;     // rate kernel block maxima
   double *save_x = nullptr;      // FP32C save steps: FP64 field, dX/dt, mu/M
+  std::string kernels;           // text returned by pf5d_stepper_rate_kernels
 };
 
 namespace {
@@ -1050,6 +1051,7 @@ struct RateVariant {
   void (*launch2d)(bool vec, dim3 g, dim3 b, size_t sm, cudaStream_t s, const RateParams &P);
   void (*launch3d)(bool vec, dim3 g, dim3 b, size_t sm, cudaStream_t s, const RateParams &P,
                    int zc);
+  std::string (*kernels)(bool vec, int dim);   // the kernel instances of a 2D/3D rate stage
 };
 
 // NTH shapes the 2D kernel only (the 3D marching kernel has one thread per
@@ -1085,6 +1087,10 @@ RateVariant make_variant() {
                   int zc) {
     if (vec) launch_pdl(k_rate_march3d<TX, TY, MINB, true, WIN, false, SORT, PP>, g, b, sm, s, P, zc);
     else launch_pdl(k_rate_march3d<TX, TY, MINB, false, WIN, false, SORT, PP>, g, b, sm, s, P, zc);
+  };
+  v.kernels = [](bool vec, int dim) {
+    if (dim == 2) return kname("k_rate_tile2d", {TX, TY, MINB, vec, WIN, 0, NTH, SORT, PP});
+    return kname("k_rate_march3d", {TX, TY, MINB, vec, WIN, 0, SORT, PP});
   };
   return v;
 }
@@ -1123,6 +1129,11 @@ RateVariant make_split_variant() {
                   int zc) {
     launch_chem<3, KMINB>(vec, s, P);
     launch_pdl(k_rate_march3d<TX, TY, MINB, true, false, true, false, PP>, g, b, sm, s, P, zc);
+  };
+  v.kernels = [](bool vec, int dim) {
+    const std::string chem = kname("k_chem64", {dim, vec, KMINB}) + " + ";
+    if (dim == 2) return chem + kname("k_rate_tile2d", {TX, TY, MINB, 1, 0, 1, TX * TY, 0, 0});
+    return chem + kname("k_rate_march3d", {TX, TY, MINB, 1, 0, 1, 0, PP});
   };
   return v;
 }
@@ -1439,7 +1450,6 @@ pf5d_status pf5d_stepper_create(const pf5d_stepper_desc *desc, double *X, void *
   P.T.stride = desc->node_stride;
   P.T.inv_step = 1.0 / desc->resolution;
   P.T.threshold = 1.0 - 4.0 * desc->resolution - 1e-9;
-  P.T.exact_d2 = (1.99 * desc->resolution) * (1.99 * desc->resolution);
   P.T.max_nn_dist = desc->max_nn_dist;
   for (int c = 0; c < 4; ++c) {
     P.kappa.v[c] = desc->kappa[c];
@@ -1713,6 +1723,15 @@ int32_t pf5d_stepper_launches_per_step(const pf5d_stepper *h) {
   if (h->s32) return s32_launches_per_step(h->s32);
   const bool split = h->d.dim >= 2 && rate_variants()[h->variant].split;
   return (split ? 2 : 1) + 2 + (h->d.elastic ? 1 : 0);   // rate (+chem), dt, update, bmul
+}
+
+const char *pf5d_stepper_rate_kernels(pf5d_stepper *h) {
+  if (!h) return "";
+  if (h->s32) return s32_rate_kernels(h->s32);
+  if (h->d.dim == 1) h->kernels = kname("k_rate_1d", {kTX1, h->vec});
+  else h->kernels = rate_variants()[h->variant].kernels(h->vec, h->d.dim);
+  h->kernels += " + k_dt_finish";
+  return h->kernels.c_str();
 }
 
 int32_t pf5d_stepper_variant_count(const pf5d_stepper *h) {

@@ -23,9 +23,12 @@ def interpolator_nb(composition_array, data_grid, resolution, tree, calphad_valu
     """phasefield5d/solver/interpolation.py:154-211 on the device.
 
     Accepts numpy arrays (copied to the device, results copied back into
-    ``out`` / ``mask_buffer``) or CUDA tensors (used in place).  Raises
-    ``RuntimeError`` when ``max_nn_dist`` is set and a fallback row is
-    farther than it, as the reference does.
+    ``out`` / ``mask_buffer``) or CUDA tensors (used in place).  The
+    fallback row is the exact nearest table row for any finite point, on or
+    off the simplex.  Raises where the reference raises: ``RuntimeError``
+    when ``max_nn_dist`` is set and a fallback row is farther than it, and
+    ``ValueError`` for a non-finite composition that takes the fallback
+    (``cKDTree.query`` rejects it).
     """
     t = D.torch()
     L = D.lib()
@@ -48,8 +51,7 @@ def interpolator_nb(composition_array, data_grid, resolution, tree, calphad_valu
                                float(max_nn_dist) if max_nn_dist is not None else -1.0,
                                _lib.ptr(res), n_props, _lib.ptr(mask), _lib.ptr(flags),
                                _lib.stream_handle()), "interpolator_nb")
-    if max_nn_dist is not None and int(flags.item()) & _lib.FLAG_NN_FAR:
-        raise RuntimeError("Some compositions are outside the CALPHAD domain (KD-tree).")
+    _lib.raise_nn_errors(int(flags.item()), check_far=max_nn_dist is not None)
     if mask_buffer is not None:
         if D.is_cuda_tensor(mask_buffer):
             mask_buffer.copy_(mask.view(mask_buffer.shape).to(mask_buffer.dtype))

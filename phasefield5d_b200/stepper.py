@@ -139,17 +139,30 @@ class Stepper:
         self.steps_enqueued += int(n_steps)
 
     def state(self):
-        """Synchronise and return {dt, time, xdotmax, step, flags, halted}."""
+        """Synchronise and return {dt, time, xdotmax, step, flags, halted}
+        plus the decoded nearest-row fallback bits: ``nn_used`` (some point
+        took the fallback), ``nn_far`` (a row farther than max_nn_dist),
+        ``nn_nonfinite`` (a non-finite composition reached the fallback) and
+        ``nn_no_row``.  The last three halt the loop before that step's
+        update, where the reference's loop raises."""
         st = _lib.StepState()
         _lib.check(self.L.pf5d_stepper_state(self.h, ctypes.byref(st), self._s()), "state")
-        return dict(dt=st.dt, time=st.time, xdotmax=st.xdotmax, step=int(st.step),
-                    flags=int(st.flags), halted=bool(st.halted))
+        out = dict(dt=st.dt, time=st.time, xdotmax=st.xdotmax, step=int(st.step),
+                   flags=int(st.flags), halted=bool(st.halted))
+        out.update(_lib.nn_flags(int(st.flags)))
+        return out
 
     def run(self, n_steps):
         """Advance ``n_steps`` and return the state; ``halted`` is True when an
-        out-of-bounds check stopped the loop (simulate.py:231-239)."""
+        out-of-bounds check stopped the loop (simulate.py:231-239).  A
+        nearest-row error raises as the reference's loop does: ValueError for
+        a non-finite composition, RuntimeError for a row beyond max_nn_dist;
+        the field is left as it was before the failing step."""
         self.advance(n_steps)
-        return self.state()
+        st = self.state()
+        if st["halted"]:
+            _lib.raise_nn_errors(st["flags"])
+        return st
 
     def rate(self):
         """dX/dt of the last step as a (*shape, 4) CUDA tensor (a view)."""
@@ -184,6 +197,12 @@ class Stepper:
     def launches_per_step(self):
         """Kernels of this library one step launches (cuFFT's not counted)."""
         return int(self.L.pf5d_stepper_launches_per_step(self.h))
+
+    @property
+    def rate_kernels(self):
+        """The kernel instances one rate stage of the current variant launches
+        (profiler names), e.g. for a roofline report."""
+        return (self.L.pf5d_stepper_rate_kernels(self.h) or b"").decode()
 
     @property
     def n_variants(self):

@@ -70,6 +70,88 @@ def test_nearest_row_matches_kdtree_property(torch_cuda, small_table):
     assert np.array_equal(out[bad], small_table["vals"][nn])
 
 
+def _off_simplex_points(seed):
+    """Points a window-limited search could miss: row sums in [1.05, 1.5],
+    components far outside [0, 1], and a few hand-picked extremes."""
+    rng = np.random.default_rng(seed)
+    s = rng.uniform(1.05, 1.5, size=(3000, 1))
+    beyond = rng.dirichlet(np.ones(4), size=3000) * s
+    far = rng.uniform(-0.6, 1.6, size=(3000, 4))
+    picked = np.array([[1.2, 0.0, 0.0, 0.0], [0.0, 0.0, 0.0, 2.0], [5.0, 5.0, 5.0, 5.0],
+                       [-3.0, 0.1, 0.1, 0.1], [0.6, 0.6, 0.0, 0.0], [1.0, 1.0, 1.0, 1.0],
+                       [-1.0, -1.0, -1.0, -1.0], [0.3, 0.3, 0.3, 0.3], [40.0, -7.0, 0.2, 0.9]])
+    return np.concatenate([beyond, far, picked])
+
+
+def test_nearest_row_exact_off_simplex(torch_cuda, small_table):
+    """Every point outside the linear region -- including points well past the
+    simplex face and far outside [0, 1] -- gets exactly the row the
+    reference's cKDTree returns, and the whole output (linear branch
+    included) equals the oracle's bit for bit."""
+    from oracle import oracle as O
+    from phasefield5d_b200.solver.interpolation import interpolator_nb
+    x = _off_simplex_points(17)
+    t = small_table
+    out = np.empty((x.shape[0], 9))
+    mask = np.empty(x.shape[0], dtype=np.bool_)
+    interpolator_nb(x, t["grid"], t["resolution"], t["tree"], t["vals"], out=out,
+                    mask_buffer=mask)
+    bad = ~mask
+    assert bad.sum() > 4000
+    _, nn = t["tree"].query(x[bad])
+    assert np.array_equal(out[bad], t["vals"][nn])
+    ref = O.interpolator_nb(x, t["grid"], t["resolution"], t["tree"], t["vals"])
+    assert np.array_equal(out, ref, equal_nan=True)
+
+
+def test_nearest_row_exact_on_fine_table(torch_cuda):
+    """The same property on the 0.025-spacing (41^4) workload table, whose
+    windows are narrower in composition units."""
+    from phasefield5d_b200 import workload as W
+    from phasefield5d_b200.solver.interpolation import interpolator_nb
+    from phasefield5d_b200.solver.table import build_4d_grid, build_calphad_kdtree
+    data = W.make_table(0.025, 873.0, 4).data
+    _, grid = build_4d_grid(data, 0.025)
+    tree, vals = build_calphad_kdtree(data)
+    x = _off_simplex_points(23)
+    out = np.empty((x.shape[0], 9))
+    mask = np.empty(x.shape[0], dtype=np.bool_)
+    interpolator_nb(x, grid, 0.025, tree, vals, out=out, mask_buffer=mask)
+    bad = ~mask
+    _, nn = tree.query(x[bad])
+    assert np.array_equal(out[bad], vals[nn])
+
+
+def test_nearest_row_nonfinite_raises(torch_cuda, small_table):
+    """A NaN composition reaches the fallback (NaN <= threshold is false);
+    the reference's cKDTree.query raises ValueError for it, and so does the
+    device path."""
+    from oracle import oracle as O
+    from phasefield5d_b200.solver.interpolation import interpolator_nb
+    t = small_table
+    x = np.array([[0.1, 0.2, 0.1, 0.1], [np.nan, 0.2, 0.1, 0.1]])
+    with pytest.raises(ValueError):
+        O.interpolator_nb(x, t["grid"], t["resolution"], t["tree"], t["vals"])
+    with pytest.raises(ValueError):
+        interpolator_nb(x, t["grid"], t["resolution"], t["tree"], t["vals"])
+
+
+def test_nearest_row_far_off_simplex_distance_error(torch_cuda, small_table):
+    """x = (1.2, 0, 0, 0) is 0.2 from its nearest row (1, 0, 0, 0): with
+    max_nn_dist = 0.1 both the reference and the device raise."""
+    from oracle import oracle as O
+    from phasefield5d_b200.solver.interpolation import interpolator_nb
+    t = small_table
+    x = np.array([[1.2, 0.0, 0.0, 0.0]])
+    with pytest.raises(RuntimeError):
+        O.interpolator_nb(x, t["grid"], t["resolution"], t["tree"], t["vals"], max_nn_dist=0.1)
+    with pytest.raises(RuntimeError):
+        interpolator_nb(x, t["grid"], t["resolution"], t["tree"], t["vals"], max_nn_dist=0.1)
+    out = interpolator_nb(x, t["grid"], t["resolution"], t["tree"], t["vals"], max_nn_dist=0.25)
+    _, nn = t["tree"].query(x)
+    assert np.array_equal(out, t["vals"][nn])
+
+
 @pytest.mark.parametrize("dim", [1, 2, 3])
 def test_laplacian_bitwise(torch_cuda, kernels_golden, dim):
     from phasefield5d_b200.solver.operators import calculate_laplacian

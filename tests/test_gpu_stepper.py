@@ -239,6 +239,65 @@ def test_out_of_bounds_halts(torch_cuda, inject):
     gpu.close()
 
 
+@pytest.mark.parametrize("dim,shape", [(1, (64,)), (2, (40, 36)), (3, (12, 20, 24))])
+def test_nonfinite_midrun_raises_like_reference(torch_cuda, dim, shape):
+    """Host-made failure between steps: a NaN written into the field after 5
+    steps reaches the nearest-row fallback at the next step (NaN fails the
+    linear-region test), where the reference's cKDTree.query raises
+    ValueError.  The stepper halts before that step's update and ``run``
+    raises ValueError; the field and the step count stay as they were."""
+    from oracle.oracle import OracleStepper
+    from phasefield5d_b200 import workload as W
+    from phasefield5d_b200.stepper import Stepper
+    cfg = W.SolveConfig(system_dim=dim, initial_composition=(0.1, 0.2, 0.2, 0.25),
+                        resolution=0.05, kappa_value=5e-16, mw=4, ppw=16, shape=shape,
+                        adaptive=True, n_k=2000)
+    prob = W.build_problem(cfg)
+    gpu = Stepper.from_problem(prob)
+    gpu.run(5)
+    bad = (0,) * (dim - 1) + (3,)
+    gpu.X[bad + (1,)] = float("nan")
+    before = gpu.X.cpu().numpy()
+    with pytest.raises(ValueError):
+        gpu.run(10)
+    st = gpu.state()
+    assert st["halted"] and st["nn_nonfinite"] and st["step"] == 5
+    after = gpu.X.cpu().numpy()
+    assert np.array_equal(after, before, equal_nan=True)
+    ref = OracleStepper.from_problem(prob)
+    ref.run(5)
+    ref.X[bad + (1,)] = np.nan
+    with pytest.raises(ValueError):
+        ref.step()
+    gpu.close()
+
+
+@pytest.mark.parametrize("precision", ["fp64", "fp32c"])
+def test_near_face_point_takes_row_inside_step(torch_cuda, precision):
+    """A point near the simplex face (row sum 0.99, past the 0.8 linear
+    threshold of the 0.05 table) takes the nearest table row inside the
+    fused step, in both forms, with the fallback reported and no error
+    flag; the FP64 form still tracks the oracle."""
+    from oracle.oracle import OracleStepper
+    from phasefield5d_b200 import workload as W
+    from phasefield5d_b200.stepper import Stepper
+    cfg = W.SolveConfig(system_dim=2, initial_composition=(0.1, 0.2, 0.2, 0.25), resolution=0.05,
+                        kappa_value=5e-16, mw=4, ppw=16, shape=(24, 20), adaptive=True, n_k=2000)
+    prob = W.build_problem(cfg)
+    X = prob.X_init.copy()
+    X[3, 4] = [0.28, 0.25, 0.24, 0.22]
+    prob.X_init = X
+    gpu = Stepper.from_problem(prob, precision=precision)
+    st = gpu.run(3)
+    assert st["nn_used"] and not (st["nn_far"] or st["nn_nonfinite"] or st["nn_no_row"])
+    if precision == "fp64":
+        ref = OracleStepper.from_problem(prob)
+        ref.run(3)
+        r_field, _ = _rel(gpu.X.cpu().numpy(), ref.X, prob.X0)
+        assert r_field <= FIELD_RTOL
+    gpu.close()
+
+
 def test_rate_variants_bitwise_identical(torch_cuda):
     """Every autotuner variant (tile shape x occupancy) computes each point
     the same way, so trajectories are bit-identical across variants."""

@@ -65,3 +65,54 @@ def test_noalloc_empty_and_limit(cuda):
     with pytest.raises(RuntimeError, match="at most"):
         _lib.check(L.pf5d_abs_max_noalloc(_lib.ptr(one), too_many, _lib.ptr(res),
                                           _lib.stream_handle()))
+
+
+def test_noalloc_full_blocks_and_largest_size(cuda):
+    """n an exact multiple of the 2048-element block (the last block full) and
+    the largest n the scratch covers (32768 blocks: 512 MiB of doubles)."""
+    torch = cuda[0]
+    gen = torch.Generator(device="cuda").manual_seed(7)
+    for n in (2048, 2048 * 37, 32768 * 2048):
+        a = torch.randn(n, dtype=torch.float64, device="cuda", generator=gen)
+        a[n - 1] = -1e3                          # the maximum sits in the last, full block
+        ref, got = _both(cuda, a)
+        assert got == ref == 1e3
+        del a
+        torch.cuda.empty_cache()
+
+
+_FRESH = r"""
+import sys
+sys.path.insert(0, {repo!r})
+import torch
+from phasefield5d_b200 import _lib
+L = _lib.load()
+a = torch.randn(1_000_003, dtype=torch.float64, device="cuda")
+res = torch.zeros(1, dtype=torch.float64, device="cuda")
+torch.cuda.synchronize()
+free = [torch.cuda.mem_get_info()[0]]
+for _ in range(2):
+    _lib.check(L.pf5d_abs_max_noalloc(_lib.ptr(a), a.numel(), _lib.ptr(res),
+                                      _lib.stream_handle()))
+    torch.cuda.synchronize()
+    free.append(torch.cuda.mem_get_info()[0])
+print(*free, res.item(), a.abs().max().item())
+"""
+
+
+def test_noalloc_first_call_leaves_device_memory_untouched(cuda):
+    """In a fresh process with modules loaded eagerly (so the static scratch
+    already exists when the context is created), the first and second calls
+    leave the device's free memory exactly as it was, and the result is
+    right."""
+    import os
+    import subprocess
+    import sys
+    repo = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    env = dict(os.environ, CUDA_MODULE_LOADING="EAGER")
+    out = subprocess.run([sys.executable, "-c", _FRESH.format(repo=repo)], env=env,
+                         capture_output=True, text=True, timeout=300)
+    assert out.returncode == 0, out.stderr[-2000:]
+    f0, f1, f2, got, want = out.stdout.split()[-5:]
+    assert int(f0) == int(f1) == int(f2), (f0, f1, f2)
+    assert float(got) == float(want)
