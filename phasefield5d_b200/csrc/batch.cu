@@ -78,8 +78,8 @@ __device__ __forceinline__ float tile1d32_body(const BSolve &B, const Rate32 &P,
                                                float *smf, unsigned *flags, int tid) {
   constexpr int HX = NT + 4, MX = NT + 2;
   float *Xs = smf;                 // [S][HX]
-  float *Ms = Xs + S * HX;         // [NP][MX]
-  float *Fx = Ms + NP * MX;        // [S][NT+1]
+  float *Ms = Xs + S * HX;         // [NPM][MX]
+  float *Fx = Ms + NPM * MX;       // [S][NT+1]
   const int x0 = tile * NT;
   const int n = P.nx;
   for (int pos = tid; pos < HX; pos += NT) {
@@ -108,28 +108,15 @@ __device__ __forceinline__ float tile1d32_body(const BSolve &B, const Rate32 &P,
     float spv = 0.f;
     if (B.emode == 1)
       spv = (float)((double)B.bn * ((double)__ldg(B.s + wrap_any(x0 + pos - 1, n)) - mean));
-    float mu[S], M[NM];
-    chem32(P, d, lap, spv, nullptr, nullptr, mu, M, flags);
+    float v[NPM];
+    chem32(P, d, lap, spv, nullptr, nullptr, v, flags);
 #pragma unroll
-    for (int c = 0; c < S; ++c) Ms[c * MX + pos] = mu[c];
-#pragma unroll
-    for (int c = 0; c < NM; ++c) Ms[(S + c) * MX + pos] = M[c];
+    for (int r = 0; r < NPM; ++r) Ms[r * MX + pos] = v[r];
   }
   __syncthreads();
   for (int f = tid; f < NT + 1; f += NT) {
-    float Dc[S], Dn[S], Mc[NM], Mn[NM], g[S], J[S];
-#pragma unroll
-    for (int c = 0; c < S; ++c) {
-      Dc[c] = Xs[c * HX + f + 1];
-      Dn[c] = Xs[c * HX + f + 2];
-      g[c] = (Ms[c * MX + f + 1] - Ms[c * MX + f]) * P.inv_dx;
-    }
-#pragma unroll
-    for (int c = 0; c < NM; ++c) {
-      Mc[c] = Ms[(S + c) * MX + f];
-      Mn[c] = Ms[(S + c) * MX + f + 1];
-    }
-    face_flux32(P, Dc, Mc, Dn, Mn, g, J);
+    float J[S];
+    face32_between<HX, MX>(P, Xs, Ms, f + 1, f, Xs, Ms, f + 2, f + 1, J);
 #pragma unroll
     for (int c = 0; c < S; ++c) Fx[c * (NT + 1) + f] = J[c];
   }
@@ -138,7 +125,8 @@ __device__ __forceinline__ float tile1d32_body(const BSolve &B, const Rate32 &P,
   if (x0 + tid < n) {
     float out[S];
 #pragma unroll
-    for (int c = 0; c < S; ++c) out[c] = (Fx[c * (NT + 1) + tid + 1] - Fx[c * (NT + 1) + tid]) * P.inv_dx;
+    for (int c = 0; c < S; ++c)
+      out[c] = (Fx[c * (NT + 1) + tid + 1] - Fx[c * (NT + 1) + tid]) * P.flux_scale;
     store_rate(P.dX, x0 + tid, out, vmax);
   }
   return vmax;
@@ -147,7 +135,7 @@ __device__ __forceinline__ float tile1d32_body(const BSolve &B, const Rate32 &P,
 template <int TX, int TY, bool SORT = false>
 struct BatchSmem {
   static constexpr int NT = TX * TY;
-  static constexpr size_t s1d = (S * (NT + 4) + NP * (NT + 2) + S * (NT + 1)) * sizeof(float);
+  static constexpr size_t s1d = (S * (NT + 4) + NPM * (NT + 2) + S * (NT + 1)) * sizeof(float);
   static constexpr size_t s2d = Tile2dSmem32<TX, TY, SORT>::bytes;
   // Rate32 copy, rounded up to whole float4 plus one spare float4, then the tile work area.
   static constexpr size_t head = 16 * ((sizeof(Rate32) + 15) / 16 + 1);
@@ -873,7 +861,7 @@ pf5d_status pf5d_batch_create(const pf5d_batch_solve *solves, int32_t nsolves,
     T.sum_x0 = sx;
     b.sum_x0 = sx;
     P.c_fe = 1.0 - sx;
-    P.inv_dx = (float)(1.0 / q.dx);
+    P.flux_scale = (float)(0.5 / (q.dx * q.dx));
     P.inv_dx2 = (float)(1.0 / (q.dx * q.dx));
     P.ctld = q.ctld;
     P.t_cfl = q.t_cfl;

@@ -24,6 +24,9 @@ struct StepState32 {
 };
 
 constexpr int kStride32 = 12;   // floats per FP32 table node (9 props + 3 pad = 48 bytes)
+// Rows of a mu/M array in shared memory: mu_1..4, M_Fe, M_1..4 and the
+// point's FP64-formed closure X_Fe = (1 - sum X0) - sum D, rounded to FP32.
+constexpr int NPM = NP + 1;
 
 struct Table32 {
   const float *grid;
@@ -46,12 +49,15 @@ struct Rate32 {
   Table32 T;
   float kappa[S], lvec[S], x0f[S];
   double c_fe;         // 1 - sum X0
-  float inv_dx, inv_dx2;
+  float flux_scale;    // 0.5 / dx^2: divergence scale of the unscaled face fluxes
+  float inv_dx2;
   double ctld, t_cfl, lower, upper, factor;
   int adaptive;
   StepState32 *st;
   double *partial;     // block maxima of |dX/dt| of the last rate launch
-  float *mm;           // split rate: mu_1..4, M_Fe, M_1..4 per point, SoA [NP][npts]
+  // split rate buffers, one entry per point: mu_1..4; M_1..4; (M_Fe, X_Fe)
+  float4 *mm_mu, *mm_m;
+  float2 *mm_f;
   int64_t npts;
 };
 
@@ -71,11 +77,18 @@ __device__ __forceinline__ float lap32(const float nb[N], float c, float inv_dx2
   return __fmul_rn(__fsub_rn(sum, __fmul_rn((float)N, c)), inv_dx2);
 }
 
+// FP64 sum of the deviation d = X - X0 (left to right): the linear-region
+// test and the closure X_Fe = (1 - sum X0) - sum d both use it.
+__device__ __forceinline__ double dsum32(const float d[S]) {
+  return (((double)d[0] + (double)d[1]) + (double)d[2]) + (double)d[3];
+}
+
 // Table cell and fractional coordinates of X = X0 + d (interpolation.py:103-121
-// clamping).  Returns false when the point is outside the linear region
-// (sum X > 1 - 4 res - 1e-9, tested in FP64) and takes the nearest-row path.
-__device__ __forceinline__ bool cell32(const Table32 &T, const float d[S], int ii[S], float tt[S]) {
-  const double sd = (((double)d[0] + (double)d[1]) + (double)d[2]) + (double)d[3];
+// clamping); sd = dsum32(d).  Returns false when the point is outside the
+// linear region (sum X > 1 - 4 res - 1e-9, tested in FP64) and takes the
+// nearest-row path.
+__device__ __forceinline__ bool cell32(const Table32 &T, const float d[S], double sd, int ii[S],
+                                       float tt[S]) {
   if (!(T.sum_x0 + sd <= T.threshold)) return false;
 #pragma unroll
   for (int a = 0; a < S; ++a) {
@@ -96,36 +109,77 @@ __device__ __forceinline__ bool cell32(const Table32 &T, const float d[S], int i
   return true;
 }
 
+// Corner weights of the quadrilinear interpolation as two pair products:
+// corner c = b0 b1 b2 b3 (binary) has weight wa[b0 b1] * wb[b2 b3], where
+// wa = {q0 q1, q0 t1, t0 q1, t0 t1}, wb likewise for axes 2, 3 (q = 1 - t).
+struct Weights32 {
+  float wa[4], wb[4];
+};
+
+__device__ __forceinline__ Weights32 weights32(const float tt[S]) {
+  const float q0 = 1.f - tt[0], q1 = 1.f - tt[1], q2 = 1.f - tt[2], q3 = 1.f - tt[3];
+  Weights32 w;
+  w.wa[0] = q0 * q1;
+  w.wa[1] = q0 * tt[1];
+  w.wa[2] = tt[0] * q1;
+  w.wa[3] = tt[0] * tt[1];
+  w.wb[0] = q2 * q3;
+  w.wb[1] = q2 * tt[3];
+  w.wb[2] = tt[2] * q3;
+  w.wb[3] = tt[2] * tt[3];
+  return w;
+}
+
+// One corner's contribution: out[p] = w v[p] for the first corner, else
+// fma(w, v[p], out[p]) -- corners in order c = 0..15 in every kernel.
+__device__ __forceinline__ void corner_acc32(int c, float w, const float4 &a, const float4 &b,
+                                             const float4 &e, float out[NP]) {
+  const float v[NP] = {a.x, a.y, a.z, a.w, b.x, b.y, b.z, b.w, e.x};
+#pragma unroll
+  for (int p = 0; p < NP; ++p) out[p] = (c == 0) ? w * v[p] : fmaf(w, v[p], out[p]);
+}
+
 // Quadrilinear interpolation of the 9 props from 16 corner nodes laid out
 // with node strides (s0, s1, s2, s3) in float4 units from `base` (global
 // table or shared window; 3 float4 per node).
 __device__ __forceinline__ void interp_nodes32(const float4 *base, int s0, int s1, int s2, int s3,
                                                const float tt[S], float out[NP]) {
-  const float q0 = 1.f - tt[0], q1 = 1.f - tt[1], q2 = 1.f - tt[2], q3 = 1.f - tt[3];
+  const Weights32 W = weights32(tt);
 #pragma unroll
   for (int c = 0; c < 16; ++c) {
     const int b0 = (c >> 3) & 1, b1 = (c >> 2) & 1, b2 = (c >> 1) & 1, b3 = c & 1;
-    const float w = (b0 ? tt[0] : q0) * (b1 ? tt[1] : q1) * (b2 ? tt[2] : q2) * (b3 ? tt[3] : q3);
+    const float w = W.wa[c >> 2] * W.wb[c & 3];
     const float4 *node = base + b0 * s0 + b1 * s1 + b2 * s2 + b3 * s3;
-    const float4 a = node[0], b = node[1], e = node[2];
-    const float v[NP] = {a.x, a.y, a.z, a.w, b.x, b.y, b.z, b.w, e.x};
-#pragma unroll
-    for (int p = 0; p < NP; ++p) out[p] = (c == 0) ? w * v[p] : fmaf(w, v[p], out[p]);
+    corner_acc32(c, w, node[0], node[1], node[2], out);
   }
+}
+
+// Nearest table row (the fallback outside the linear region) of X0 + d.
+__device__ __forceinline__ void nearest_row32(const Table32 &T, const float d[S], float out[NP],
+                                              unsigned *flags) {
+  const NearestNode r = nearest_node_g<float>(T.grid, T.stride, T.coord, T.n, T.inv_step,
+                                              T.max_nn_dist, T.x0[0] + (double)d[0],
+                                              T.x0[1] + (double)d[1], T.x0[2] + (double)d[2],
+                                              T.x0[3] + (double)d[3]);
+  *flags |= r.flags;
+  const float *row = T.grid + (r.node < 0 ? 0 : r.node) * T.stride;
+#pragma unroll
+  for (int p = 0; p < NP; ++p) out[p] = r.node < 0 ? __int_as_float(0x7fc00000) : __ldg(row + p);
 }
 
 constexpr int kWin32 = 4;                       // window nodes per axis (3 cells)
 constexpr int kWinNodes32 = kWin32 * kWin32 * kWin32 * kWin32;
 
-// Table value at X0 + d: from the shared window `win` when the point's cell
-// fits in it (win_lo = box origin), else from the global table; nearest row
-// outside the linear region.
-__device__ __forceinline__ void interp32(const Rate32 &P, const float d[S], const float4 *win,
-                                         const int *win_lo, float out[NP], unsigned *flags) {
+// Table value at X0 + d (sd = dsum32(d)): from the shared window `win` when
+// the point's cell fits in it (win_lo = box origin), else from the global
+// table; nearest row outside the linear region.
+__device__ __forceinline__ void interp32(const Rate32 &P, const float d[S], double sd,
+                                         const float4 *win, const int *win_lo, float out[NP],
+                                         unsigned *flags) {
   const Table32 &T = P.T;
   int ii[S];
   float tt[S];
-  if (cell32(T, d, ii, tt)) {
+  if (cell32(T, d, sd, ii, tt)) {
     const int off = win ? window_cell<kWin32>(ii, win_lo) : -1;
     if (off >= 0) {
       constexpr int w3 = 3, w2 = kWin32 * w3, w1 = kWin32 * w2, w0 = kWin32 * w1;
@@ -139,65 +193,68 @@ __device__ __forceinline__ void interp32(const Rate32 &P, const float d[S], cons
     }
     return;
   }
-  const NearestNode r = nearest_node_g<float>(T.grid, T.stride, T.coord, T.n, T.inv_step,
-                                              T.max_nn_dist, T.x0[0] + (double)d[0],
-                                              T.x0[1] + (double)d[1], T.x0[2] + (double)d[2],
-                                              T.x0[3] + (double)d[3]);
-  *flags |= r.flags;
-  const float *row = T.grid + (r.node < 0 ? 0 : r.node) * T.stride;
-#pragma unroll
-  for (int p = 0; p < NP; ++p) out[p] = r.node < 0 ? __int_as_float(0x7fc00000) : __ldg(row + p);
+  nearest_row32(T, d, out, flags);
 }
 
-// mu (relative to mu(X0)) and M at one point.
+// Gradient-energy and elastic parts of mu at one point: off = s' l - kappa lap
+// (spv = 0 without elasticity); mu = table value + off.
+__device__ __forceinline__ void mu_offset32(const Rate32 &P, const float lap[S], float spv,
+                                            float off[S]) {
+#pragma unroll
+  for (int c = 0; c < S; ++c) off[c] = fmaf(spv, P.lvec[c], -lap[c] * P.kappa[c]);
+}
+
+// Row layout of a point's mu/M values: mu (relative to mu(X0)) 0..3, M_Fe 4,
+// M_1..4 5..8, the closure X_Fe 9 (FP64 (1 - sum X0) - sum d, rounded).
 __device__ __forceinline__ void chem32(const Rate32 &P, const float d[S], const float lap[S],
                                        float spv, const float4 *win, const int *win_lo,
-                                       float mu[S], float M[NM], unsigned *flags) {
-  float v[NP];
-  interp32(P, d, win, win_lo, v, flags);
+                                       float out[NPM], unsigned *flags) {
+  const double sd = dsum32(d);
+  float v[NP], off[S];
+  interp32(P, d, sd, win, win_lo, v, flags);
+  mu_offset32(P, lap, spv, off);
 #pragma unroll
-  for (int c = 0; c < S; ++c) {
-    float m = fmaf(-lap[c], P.kappa[c], v[c]);
-    if (P.sp) m = fmaf(spv, P.lvec[c], m);
-    mu[c] = m;
-  }
+  for (int c = 0; c < S; ++c) out[c] = v[c] + off[c];
 #pragma unroll
-  for (int c = 0; c < NM; ++c) M[c] = v[S + c];
+  for (int c = 0; c < NM; ++c) out[S + c] = v[S + c];
+  out[NP] = (float)(P.c_fe - sd);
 }
 
-// Face flux (phasefield5d/solver/fluxes.py:128-160) in FP32 with the FP64
-// closure X_Fe = (1 - sum X0) - sum Dmid.
-__device__ __forceinline__ void face_flux32(const Rate32 &P, const float Dc[S], const float Mc[NM],
-                                            const float Dn[S], const float Mn[NM],
-                                            const float g[S], float J[S]) {
-  // Every operation explicitly rounded: a face evaluated from either side
-  // (or in any kernel) gives the same bits, so the flux form conserves mass
-  // exactly even when the two cells of a face each evaluate it.
-  float dm[S], xm[S], mm[NM], dk[S];
-#pragma unroll
-  for (int a = 0; a < S; ++a) {
-    dm[a] = __fmul_rn(0.5f, __fadd_rn(Dc[a], Dn[a]));
-    xm[a] = __fadd_rn(P.x0f[a], dm[a]);
-  }
-#pragma unroll
-  for (int a = 0; a < NM; ++a) mm[a] = __fmul_rn(0.5f, __fadd_rn(Mc[a], Mn[a]));
-  const double x_fe = __dsub_rn(P.c_fe, __dadd_rn(__dadd_rn(__dadd_rn((double)dm[0], (double)dm[1]),
-                                                           (double)dm[2]), (double)dm[3]));
-  const float w_fe = __fmul_rn((float)x_fe, mm[0]);
-  float dot = 0.f;
-#pragma unroll
-  for (int b = 0; b < S; ++b) dot = fmaf(xm[b], g[b], dot);
-#pragma unroll
-  for (int k = 0; k < S; ++k) dk[k] = __fsub_rn(g[k], dot);
-  float swk = 0.f;
-#pragma unroll
-  for (int k = 0; k < S; ++k) swk = fmaf(__fmul_rn(xm[k], mm[1 + k]), dk[k], swk);
-#pragma unroll
-  for (int a = 0; a < S; ++a) {
-    const float t1 = __fmul_rn(__fmul_rn(w_fe, xm[a]), dot);
-    const float t2 = __fmul_rn(__fmul_rn(xm[a], mm[1 + a]), dk[a]);
-    J[a] = __fsub_rn(__fadd_rn(t1, t2), __fmul_rn(xm[a], swk));
-  }
+// Face flux (phasefield5d/solver/fluxes.py:128-160) in FP32 between a lower
+// position c and an upper position n along one axis, from each position's
+// D = X - X0, mu, M_1..4 and (M_Fe, X_Fe):
+//   J_a = Xm_a (w_fe <Xm,g> - sum_k Xm_k M_k dk_k) + Xm_a M_a dk_a,
+//   dk = g - <Xm,g>, w_fe = X_Fe M_Fe,
+// which is the reference's expression regrouped.  The flux is linear in the
+// face mobilities and in the mu gradient, so it is evaluated with the sums
+// Mc + Mn (for 2 x the mean) and the difference mu_n - mu_c (for dx x the
+// gradient): the returned J is (2 dx) times the flux, and kernels scale the
+// divergence sum by flux_scale = 0.5 / dx^2.  X_Fe at the face is the mean
+// of the two positions' FP64-formed closures.  The units are built without
+// multiply-add contraction, so a face gives the same bits whichever of its
+// cells (or kernels) evaluates it, and the flux form conserves mass exactly.
+__device__ __forceinline__ float4 face_flux32(const Rate32 &P, const float4 &dc, const float4 &muc,
+                                              const float4 &mc, const float2 &fc, const float4 &dn,
+                                              const float4 &mun, const float4 &mn,
+                                              const float2 &fn) {
+  const float xm0 = fmaf(0.5f, dc.x + dn.x, P.x0f[0]), xm1 = fmaf(0.5f, dc.y + dn.y, P.x0f[1]),
+              xm2 = fmaf(0.5f, dc.z + dn.z, P.x0f[2]), xm3 = fmaf(0.5f, dc.w + dn.w, P.x0f[3]);
+  const float g0 = mun.x - muc.x, g1 = mun.y - muc.y, g2 = mun.z - muc.z, g3 = mun.w - muc.w;
+  const float w_fe = (0.5f * (fc.y + fn.y)) * (fc.x + fn.x);
+  float dot = xm0 * g0;
+  dot = fmaf(xm1, g1, dot);
+  dot = fmaf(xm2, g2, dot);
+  dot = fmaf(xm3, g3, dot);
+  const float dk0 = g0 - dot, dk1 = g1 - dot, dk2 = g2 - dot, dk3 = g3 - dot;
+  const float w0 = xm0 * (mc.x + mn.x), w1 = xm1 * (mc.y + mn.y), w2 = xm2 * (mc.z + mn.z),
+              w3 = xm3 * (mc.w + mn.w);
+  float swk = w0 * dk0;
+  swk = fmaf(w1, dk1, swk);
+  swk = fmaf(w2, dk2, swk);
+  swk = fmaf(w3, dk3, swk);
+  const float com = fmaf(w_fe, dot, -swk);
+  return make_float4(fmaf(w0, dk0, xm0 * com), fmaf(w1, dk1, xm1 * com), fmaf(w2, dk2, xm2 * com),
+                     fmaf(w3, dk3, xm3 * com));
 }
 
 // Fold this thread's max |dX/dt| into the block and store the block's max
@@ -241,23 +298,29 @@ __device__ __forceinline__ void dt_from_slots32(const Rate32 &P, const double *s
   }
 }
 
+// Face flux between two positions of shared-memory SoA planes: D rows at
+// XL[c * PX + pl] (lower) and XH[c * PX + ph] (upper), mu/M rows (NPM, in
+// chem32's order) at ML[r * PM + ql] and MH[r * PM + qh].
 template <int PX, int PM>
 __device__ __forceinline__ void face32_between(const Rate32 &P, const float *XL, const float *ML,
                                                int pl, int ql, const float *XH, const float *MH,
                                                int ph, int qh, float J[S]) {
-  float Dc[S], Dn[S], Mc[NM], Mn[NM], g[S];
-#pragma unroll
-  for (int c = 0; c < S; ++c) {
-    Dc[c] = XL[c * PX + pl];
-    Dn[c] = XH[c * PX + ph];
-    g[c] = __fmul_rn(__fsub_rn(MH[c * PM + qh], ML[c * PM + ql]), P.inv_dx);
-  }
-#pragma unroll
-  for (int c = 0; c < NM; ++c) {
-    Mc[c] = ML[(S + c) * PM + ql];
-    Mn[c] = MH[(S + c) * PM + qh];
-  }
-  face_flux32(P, Dc, Mc, Dn, Mn, g, J);
+  auto d4 = [](const float *X, int p) {
+    return make_float4(X[p], X[PX + p], X[2 * PX + p], X[3 * PX + p]);
+  };
+  auto mu4 = [](const float *M, int q) {
+    return make_float4(M[q], M[PM + q], M[2 * PM + q], M[3 * PM + q]);
+  };
+  auto m4 = [](const float *M, int q) {
+    return make_float4(M[5 * PM + q], M[6 * PM + q], M[7 * PM + q], M[8 * PM + q]);
+  };
+  auto f2 = [](const float *M, int q) { return make_float2(M[4 * PM + q], M[9 * PM + q]); };
+  const float4 j = face_flux32(P, d4(XL, pl), mu4(ML, ql), m4(ML, ql), f2(ML, ql), d4(XH, ph),
+                               mu4(MH, qh), m4(MH, qh), f2(MH, qh));
+  J[0] = j.x;
+  J[1] = j.y;
+  J[2] = j.z;
+  J[3] = j.w;
 }
 
 template <int TX, int TY>
@@ -358,7 +421,7 @@ __device__ __forceinline__ void mu_plane32(const Rate32 &P, const float *Xm, con
   const int cp = (TY / 2 + 2) * G::HX + (TX / 2 + 2);
 #pragma unroll
   for (int c = 0; c < S; ++c) dc[c] = Xc[c * G::PX + cp];
-  const bool use_win = WIN && cell32(P.T, dc, rep, tr);
+  const bool use_win = WIN && cell32(P.T, dc, dsum32(dc), rep, tr);
   int o[S] = {0, 0, 0, 0};
   if (use_win) {
     window_origin<kWin32>(rep, tr, o);
@@ -412,17 +475,15 @@ __device__ __forceinline__ void mu_plane32(const Rate32 &P, const float *Xm, con
       }
     }
     const float spv = P.sp ? __ldg(P.sp + zoff + (int64_t)wy[my + 1] * P.nx + wx[mx + 1]) : 0.f;
-    float mu[S], M[NM];
-    chem32(P, d, lap, spv, use_win ? win : nullptr, o, mu, M, flags);
+    float v[NPM];
+    chem32(P, d, lap, spv, use_win ? win : nullptr, o, v, flags);
 #pragma unroll
-    for (int c = 0; c < S; ++c) dst[c * G::PM + pos] = mu[c];
-#pragma unroll
-    for (int c = 0; c < NM; ++c) dst[(S + c) * G::PM + pos] = M[c];
+    for (int r = 0; r < NPM; ++r) dst[r * G::PM + pos] = v[r];
   }
 }
 
 // mu/M of one plane (tile + 1-cell halo, or the tile only) read from the
-// split buffer P.mm (written by k32_chem) into dst, in mu_plane32's layout.
+// split buffers (written by k32_chem) into dst, in mu_plane32's layout.
 template <int TX, int TY>
 __device__ __forceinline__ void load_mu_plane32(const Rate32 &P, int64_t zoff, const int *wx,
                                                 const int *wy, bool interior_only, float *dst,
@@ -431,9 +492,12 @@ __device__ __forceinline__ void load_mu_plane32(const Rate32 &P, int64_t zoff, c
   for (int pos = tid; pos < G::PM; pos += G::NT) {
     const int my = pos / G::MX, mx = pos - my * G::MX;
     if (skip_pos<G::MX, G::MY>(mx, my, interior_only)) continue;
-    const float *src = P.mm + zoff + (int64_t)wy[my + 1] * P.nx + wx[mx + 1];
+    const int64_t g = zoff + (int64_t)wy[my + 1] * P.nx + wx[mx + 1];
+    const float4 mu = __ldg(P.mm_mu + g), m = __ldg(P.mm_m + g);
+    const float2 f = __ldg(P.mm_f + g);
+    const float v[NPM] = {mu.x, mu.y, mu.z, mu.w, f.x, m.x, m.y, m.z, m.w, f.y};
 #pragma unroll
-    for (int c = 0; c < NP; ++c) dst[c * G::PM + pos] = __ldg(src + c * P.npts);
+    for (int r = 0; r < NPM; ++r) dst[r * G::PM + pos] = v[r];
   }
 }
 
@@ -493,7 +557,7 @@ template <int TX, int TY, bool SORT = false>
 struct Tile2dSmem32 {
   using G = PlaneGeom<TX, TY>;
   static constexpr size_t bytes = Smem32Tail<TX, TY>::bytes +
-      (S * G::PX + NP * G::PM + S * G::NFX + S * G::NFY) * sizeof(float) +
+      (S * G::PX + NPM * G::PM + S * G::NFX + S * G::NFY) * sizeof(float) +
       (SORT ? SortBytes32<TX, TY>::bytes : 0);
   static __device__ __forceinline__ double *red(float4 *sm4) {
     return reinterpret_cast<double *>(sm4 + kWinNodes32 * 3);
@@ -510,7 +574,7 @@ __device__ __forceinline__ float tile2d32_body(const Rate32 &P, int bx, int by, 
   double *red = Tile2dSmem32<TX, TY>::red(sm4);
   float *Xs = reinterpret_cast<float *>(red + G::NT / 32);
   float *Ms = Xs + S * G::PX;
-  float *Fx = Ms + NP * G::PM;
+  float *Fx = Ms + NPM * G::PM;
   float *Fy = Fx + S * G::NFX;
   int *wred = reinterpret_cast<int *>(Fy + S * G::NFY);
   int *win_lo = wred + S * (G::NT / 32);
@@ -548,7 +612,7 @@ __device__ __forceinline__ float tile2d32_body(const Rate32 &P, int bx, int by, 
 #pragma unroll
       for (int c = 0; c < S; ++c)
         out[c] = __fmul_rn(__fadd_rn(__fsub_rn(jyp[c], jym[c]), __fsub_rn(jxp[c], jxm[c])),
-                           P.inv_dx);
+                           P.flux_scale);
       store_rate(P.dX, (int64_t)(y0 + ty) * P.nx + (x0 + tx), out, vmax);
     }
     return vmax;                     // (shared memory still being read: callers sync first)
@@ -561,7 +625,7 @@ __device__ __forceinline__ float tile2d32_body(const Rate32 &P, int bx, int by, 
     for (int c = 0; c < S; ++c) {
       const float ay = __fsub_rn(Fy[c * G::NFY + (ty + 1) * TX + tx], Fy[c * G::NFY + ty * TX + tx]);
       const float ax = __fsub_rn(Fx[c * G::NFX + ty * (TX + 1) + tx + 1], Fx[c * G::NFX + ty * (TX + 1) + tx]);
-      out[c] = __fmul_rn(__fadd_rn(ay, ax), P.inv_dx);
+      out[c] = __fmul_rn(__fadd_rn(ay, ax), P.flux_scale);
     }
     store_rate(P.dX, (int64_t)(y0 + ty) * P.nx + (x0 + tx), out, vmax);
   }

@@ -69,8 +69,8 @@ __global__ void __launch_bounds__(TX * TY, MINB) k32_rate_march3d(Rate32 P, int 
   float4 *win = sm4;
   double *red = reinterpret_cast<double *>(win + kWinNodes32 * 3);
   float *Xs = reinterpret_cast<float *>(red + G::NT / 32);      // [3][S][PX]
-  float *Ms = Xs + 3 * S * G::PX;                                // [2][NP][PM]
-  float *Fx = Ms + 2 * NP * G::PM;
+  float *Ms = Xs + 3 * S * G::PX;                                // [2][NPM][PM]
+  float *Fx = Ms + 2 * NPM * G::PM;
   float *Fy = Fx + S * G::NFX;
   int *wred = reinterpret_cast<int *>(Fy + S * G::NFY);
   int *win_lo = wred + S * (G::NT / 32);
@@ -90,7 +90,7 @@ __global__ void __launch_bounds__(TX * TY, MINB) k32_rate_march3d(Rate32 P, int 
     else wy[i - G::HX] = wrap_any(y0 + (i - G::HX) - 2, P.ny);
   }
   auto xplane = [&](int z) { return Xs + ((z - zb + 3) % 3) * S * G::PX; };
-  auto mplane = [&](int z) { return Ms + ((z - zb + 2) & 1) * NP * G::PM; };
+  auto mplane = [&](int z) { return Ms + ((z - zb + 2) & 1) * NPM * G::PM; };
   auto load_x = [&](int z) {
     load_plane32<TX, TY>(P.D, (int64_t)wrap_any(z, P.nz) * plane, wx, wy, P.nx, xplane(z), tid);
   };
@@ -135,7 +135,7 @@ __global__ void __launch_bounds__(TX * TY, MINB) k32_rate_march3d(Rate32 P, int 
         const float ay = __fsub_rn(Fy[c * G::NFY + (ty + 1) * TX + tx], Fy[c * G::NFY + ty * TX + tx]);
         const float ax = __fsub_rn(Fx[c * G::NFX + ty * (TX + 1) + tx + 1],
                                    Fx[c * G::NFX + ty * (TX + 1) + tx]);
-        out[c] = __fmul_rn(__fadd_rn(__fadd_rn(__fsub_rn(Jz[c], Jm[c]), ay), ax), P.inv_dx);
+        out[c] = __fmul_rn(__fadd_rn(__fadd_rn(__fsub_rn(Jz[c], Jm[c]), ay), ax), P.flux_scale);
       }
       store_rate(P.dX, (int64_t)z * plane + (int64_t)(y0 + ty) * P.nx + (x0 + tx), out, vmax);
     }
@@ -150,7 +150,7 @@ template <int TX, int TY, bool SORT = false>
 constexpr size_t march3d32_smem() {
   using G = PlaneGeom<TX, TY>;
   return Smem32Tail<TX, TY>::bytes +
-         (3 * S * G::PX + 2 * NP * G::PM + S * G::NFX + S * G::NFY) * sizeof(float) +
+         (3 * S * G::PX + 2 * NPM * G::PM + S * G::NFX + S * G::NFY) * sizeof(float) +
          (SORT ? SortBytes32<TX, TY>::bytes : 0);
 }
 
@@ -160,7 +160,7 @@ __global__ void __launch_bounds__(TX) k32_rate_1d(Rate32 P) {
   if (P.st->halt) return;
   constexpr int HX = TX + 4, MX = TX + 2;
   __shared__ float Xs[S][HX];
-  __shared__ float Ms[NP][MX];
+  __shared__ float Ms[NPM][MX];
   __shared__ float Fx[S][TX + 1];
   __shared__ double red[(TX + 31) / 32];
   const int tx = threadIdx.x;
@@ -185,28 +185,16 @@ __global__ void __launch_bounds__(TX) k32_rate_1d(Rate32 P) {
       lap[c] = lap32<2>(nb, d[c], P.inv_dx2);
     }
     const float spv = P.sp ? __ldg(P.sp + wrap_any(x0 + pos - 1, n)) : 0.f;
-    float mu[S], M[NM];
-    chem32(P, d, lap, spv, nullptr, nullptr, mu, M, &flags);
+    float v[NPM];
+    chem32(P, d, lap, spv, nullptr, nullptr, v, &flags);
 #pragma unroll
-    for (int c = 0; c < S; ++c) Ms[c][pos] = mu[c];
-#pragma unroll
-    for (int c = 0; c < NM; ++c) Ms[S + c][pos] = M[c];
+    for (int r = 0; r < NPM; ++r) Ms[r][pos] = v[r];
   }
   __syncthreads();
   for (int f = tx; f < TX + 1; f += TX) {
-    float Dc[S], Dn[S], Mc[NM], Mn[NM], g[S], J[S];
-#pragma unroll
-    for (int c = 0; c < S; ++c) {
-      Dc[c] = Xs[c][f + 1];
-      Dn[c] = Xs[c][f + 2];
-      g[c] = (Ms[c][f + 1] - Ms[c][f]) * P.inv_dx;
-    }
-#pragma unroll
-    for (int c = 0; c < NM; ++c) {
-      Mc[c] = Ms[S + c][f];
-      Mn[c] = Ms[S + c][f + 1];
-    }
-    face_flux32(P, Dc, Mc, Dn, Mn, g, J);
+    float J[S];
+    face32_between<HX, MX>(P, &Xs[0][0], &Ms[0][0], f + 1, f, &Xs[0][0], &Ms[0][0], f + 2, f + 1,
+                           J);
 #pragma unroll
     for (int c = 0; c < S; ++c) Fx[c][f] = J[c];
   }
@@ -215,7 +203,7 @@ __global__ void __launch_bounds__(TX) k32_rate_1d(Rate32 P) {
   if (x0 + tx < n) {
     float out[S];
 #pragma unroll
-    for (int c = 0; c < S; ++c) out[c] = (Fx[c][tx + 1] - Fx[c][tx]) * P.inv_dx;
+    for (int c = 0; c < S; ++c) out[c] = (Fx[c][tx + 1] - Fx[c][tx]) * P.flux_scale;
     store_rate(P.dX, x0 + tx, out, vmax);
   }
   raise_rate_flags(P.st, flags);
@@ -360,39 +348,88 @@ __global__ void k32_mass_final(const double *partial, int nparts, double *out) {
   }
 }
 
-// Split rate evaluation, first kernel: mu/M at every point of a 2D/3D field
-// into P.mm, one point per thread, a 32 x 8 tile of a plane per block.  The
-// block orders its points by table cell (cell_hash counting sort) before
-// interpolating, so the lanes of a warp gather the same table nodes.  Same
-// Laplacian (lap32, neighbour order +axis0, -axis0, ...) and mu assembly
-// (chem32) as the fused kernels.
-template <int DIM, int MINB>
-__global__ void __launch_bounds__(256, MINB) k32_chem(Rate32 P) {
-  constexpr int NT = 256;
-  __shared__ float io[2 * S + 1][NT];       // inputs of each point: d, lap, s'
-  __shared__ int hist[NT];
-  __shared__ int wsum[NT / 32 + 1];
-  __shared__ unsigned short order[NT];
+// ------------------------------------------------------------------------
+// Split rate evaluation, first kernel: mu/M and the closure X_Fe at every
+// point of a 1D/2D/3D field into the split buffers (mm_mu, mm_m, mm_f).
+//
+// A block of 256 threads takes a brick of 256 K points (32 x 8 x K in 3D,
+// 32 x 8K in 2D, 256K in 1D) in six phases:
+//   1. per point: Laplacian (neighbour order +axis0, -axis0, ...), the mu
+//      offset s' l - kappa lap, the FP64 closure, the table cell and its
+//      fractions (the deviation itself for points outside the linear region);
+//   2. counting sort of the points by a hash of their exact cell (bin 255
+//      holds the points outside the linear region);
+//   3. each linear bin's run is cut into work items of up to K consecutive
+//      points;
+//   4. a thread evaluates a work item: the 16 corner nodes of the item's
+//      cell are loaded once and accumulated into every point of the item
+//      with the point's own weights, so the table traffic per point drops
+//      K-fold (the lanes of a warp hold neighbouring items, mostly of the
+//      same cell, so the loads are broadcasts).  A point whose exact cell
+//      differs from the item's first (a hash collision) is set aside;
+//   5. the points set aside and those outside the linear region (nearest
+//      table row), one per thread;
+//   6. the block's outputs are stored coalesced.
+// Every value is formed by the same routines, in the same order, as in the
+// fused kernels (weights32 / corner_acc32, mu_offset32, dsum32).
+// ------------------------------------------------------------------------
+constexpr int kChemThreads = 256;
+
+template <int DIM, int K>
+struct ChemGeom {
+  static constexpr int NPB = kChemThreads * K;                     // points per block
+  static constexpr int BX = DIM == 1 ? NPB : 32;
+  static constexpr int BY = DIM == 1 ? 1 : (DIM == 2 ? 8 * K : 8);
+  static constexpr int BZ = DIM == 3 ? K : 1;
+  static constexpr int NITEMS = NPB / K + 256;                      // upper bound on items
+  // io[NPM][NPB] floats; items[NITEMS] u32; order, prank, left [NPB] u16;
+  // skey, pkey [NPB] u8; hist / cnt / ibase [256] int; wsum[9], nleft int
+  static constexpr size_t smem = (size_t)NPM * NPB * 4 + NITEMS * 4 + 3 * NPB * 2 + 2 * NPB +
+                                 3 * 256 * 4 + 16 * 4;
+};
+
+__device__ __forceinline__ int cell_key32(const int ii[S]) {
+  return (int)((unsigned)(41 * ii[0] + 13 * ii[1] + 5 * ii[2] + ii[3]) % 255u);
+}
+
+template <int DIM, int K, int MINB>
+__global__ void __launch_bounds__(kChemThreads, MINB) k32_chem(Rate32 P) {
+  using G = ChemGeom<DIM, K>;
+  constexpr int NT = kChemThreads, NPB = G::NPB;
+  extern __shared__ float4 sm4[];
+  float *io = reinterpret_cast<float *>(sm4);                          // [NPM][NPB]
+  unsigned *items = reinterpret_cast<unsigned *>(io + NPM * NPB);
+  unsigned short *order = reinterpret_cast<unsigned short *>(items + G::NITEMS);
+  unsigned short *prank = order + NPB;
+  unsigned short *left = prank + NPB;
+  unsigned char *skey = reinterpret_cast<unsigned char *>(left + NPB);
+  unsigned char *pkey = skey + NPB;
+  int *hist = reinterpret_cast<int *>(pkey + NPB);                     // NPB % 4 == 0
+  int *cnt = hist + 256;
+  int *ibase = cnt + 256;
+  int *wsum = ibase + 256;
+  int *nleft = wsum + 12;
   pdl_wait();
   if (P.st->halt) return;
-  const int tid = threadIdx.y * 32 + threadIdx.x;
-  const int x = blockIdx.x * 32 + threadIdx.x;
-  const int y = blockIdx.y * 8 + threadIdx.y;
-  const int z = blockIdx.z;
-  const bool valid = x < P.nx && y < P.ny;
+  const int tid = threadIdx.x;
+  const Table32 &T = P.T;
   const int64_t plane = (int64_t)P.ny * P.nx;
-  const int64_t zo = (int64_t)z * plane;
-  const int64_t g = zo + (int64_t)y * P.nx + x;
   hist[tid] = 0;
-  int key = 0, rank = 0;
+  if (tid == 0) *nleft = 0;
   __syncthreads();
-  if (valid) {
+  // 1. per-point inputs
+#pragma unroll 1
+  for (int j = 0; j < K; ++j) {
+    const int q = tid + j * NT;
+    const int qx = q % G::BX, qy = (q / G::BX) % G::BY, qz = q / (G::BX * G::BY);
+    const int x = blockIdx.x * G::BX + qx, y = blockIdx.y * G::BY + qy, z = blockIdx.z * G::BZ + qz;
+    prank[q] = 0xFFFFu;
+    if (x >= P.nx || y >= P.ny || z >= P.nz) continue;
+    const int64_t zo = (int64_t)z * plane, g = zo + (int64_t)y * P.nx + x;
     auto ld = [&](int64_t gi, float v[S]) {
       const float4 a = __ldg(P.D + gi);
       v[0] = a.x; v[1] = a.y; v[2] = a.z; v[3] = a.w;
     };
-    const int xp = x + 1 == P.nx ? 0 : x + 1, xm = x == 0 ? P.nx - 1 : x - 1;
-    const int yp = y + 1 == P.ny ? 0 : y + 1, ym = y == 0 ? P.ny - 1 : y - 1;
     constexpr int NB = 2 * DIM;
     float d[S], nb[NB][S];
     ld(g, d);
@@ -403,176 +440,275 @@ __global__ void __launch_bounds__(256, MINB) k32_chem(Rate32 P) {
       ld((int64_t)zm * plane + (int64_t)y * P.nx + x, nb[k++]);
     }
     if (DIM >= 2) {
+      const int yp = y + 1 == P.ny ? 0 : y + 1, ym = y == 0 ? P.ny - 1 : y - 1;
       ld(zo + (int64_t)yp * P.nx + x, nb[k++]);
       ld(zo + (int64_t)ym * P.nx + x, nb[k++]);
     }
+    const int xp = x + 1 == P.nx ? 0 : x + 1, xm = x == 0 ? P.nx - 1 : x - 1;
     ld(zo + (int64_t)y * P.nx + xp, nb[k++]);
     ld(zo + (int64_t)y * P.nx + xm, nb[k]);
-    float u[S];
+    float lap[S], off[S];
 #pragma unroll
     for (int c = 0; c < S; ++c) {
       float n[NB];
 #pragma unroll
       for (int i = 0; i < NB; ++i) n[i] = nb[i][c];
-      io[c][tid] = d[c];
-      io[S + c][tid] = lap32<NB>(n, d[c], P.inv_dx2);
-      u[c] = fmaf(d[c], P.T.inv_step_f, P.T.fb[c]) + (float)P.T.ib[c];
+      lap[c] = lap32<NB>(n, d[c], P.inv_dx2);
     }
-    io[2 * S][tid] = P.sp ? __ldg(P.sp + g) : 0.f;
-    key = cell_hash_u(u);
-    rank = atomicAdd(&hist[key], 1);
-  }
-  __syncthreads();
-  const int count = block_exclusive_scan<NT, NT>(hist, wsum, tid);
-  if (valid) order[hist[key] + rank] = (unsigned short)tid;
-  __syncthreads();
-  unsigned flags = 0;
-  float mu[S], M[NM];
-  if (tid < count) {
-    const int q = order[tid];
-    float dq[S], lq[S];
+    mu_offset32(P, lap, P.sp ? __ldg(P.sp + g) : 0.f, off);
+    const double sd = dsum32(d);
+    int ii[S];
+    float tt[S];
+    int cell = -1, key = 255;
+    if (cell32(T, d, sd, ii, tt)) {
+      cell = ((ii[0] * T.n + ii[1]) * T.n + ii[2]) * T.n + ii[3];
+      key = cell_key32(ii);
+    } else {
+#pragma unroll
+      for (int c = 0; c < S; ++c) tt[c] = d[c];
+    }
 #pragma unroll
     for (int c = 0; c < S; ++c) {
-      dq[c] = io[c][q];
-      lq[c] = io[S + c][q];
+      io[c * NPB + q] = tt[c];
+      io[(S + c) * NPB + q] = off[c];
     }
-    const int o[S] = {0, 0, 0, 0};
-    chem32(P, dq, lq, io[2 * S][q], nullptr, o, mu, M, &flags);
-    // point q of the tile: row q / 32, column q % 32
-    const int64_t gq = zo + (int64_t)(blockIdx.y * 8 + (q >> 5)) * P.nx + blockIdx.x * 32 + (q & 31);
+    io[8 * NPB + q] = __int_as_float(cell);
+    io[9 * NPB + q] = (float)(P.c_fe - sd);
+    pkey[q] = (unsigned char)key;
+    prank[q] = (unsigned short)atomicAdd(&hist[key], 1);
+  }
+  __syncthreads();
+  // 2. counting sort by cell key
+  cnt[tid] = hist[tid];
+  const int nvalid = block_exclusive_scan<256, NT>(hist, wsum, tid);
+  for (int q = tid; q < NPB; q += NT) {
+    if (prank[q] == 0xFFFFu) continue;
+    const int b = pkey[q], s = hist[b] + prank[q];
+    order[s] = (unsigned short)q;
+    skey[s] = (unsigned char)b;
+  }
+  // 3. work items: runs of up to K points of one linear bin
+  ibase[tid] = tid == 255 ? 0 : (cnt[tid] + K - 1) / K;
+  const int nitems = block_exclusive_scan<256, NT>(ibase, wsum, tid);
+  const int lin_end = nvalid - cnt[255];            // bin 255 (nearest row) sorts last
+  for (int s = tid; s < lin_end; s += NT) {
+    const int b = skey[s], r = s - hist[b];
+    if (r % K == 0) items[ibase[b] + r / K] = (unsigned)s | ((unsigned)min(K, cnt[b] - r) << 16);
+  }
+  __syncthreads();
+  // 4. the work items
+  const float4 *g4 = reinterpret_cast<const float4 *>(T.grid);
+  const int64_t s3 = 3, s2 = 3 * (int64_t)T.n, s1 = s2 * T.n, s0 = s1 * T.n;
+  for (int it = tid; it < nitems; it += NT) {
+    const unsigned e = items[it];
+    const int s = (int)(e & 0xFFFFu), m = (int)(e >> 16);
+    int q[K];
+    bool use[K];
+    Weights32 W[K];
+    int cell0 = 0;
 #pragma unroll
-    for (int c = 0; c < S; ++c) P.mm[c * P.npts + gq] = mu[c];
+    for (int j = 0; j < K; ++j) {
+      q[j] = j < m ? (int)order[s + j] : 0;
+      const int cj = __float_as_int(io[8 * NPB + q[j]]);
+      if (j == 0) cell0 = cj;
+      use[j] = j < m && cj == cell0;
+      if (j < m && !use[j]) left[atomicAdd(nleft, 1)] = (unsigned short)q[j];
+      float tt[S];
 #pragma unroll
-    for (int c = 0; c < NM; ++c) P.mm[(S + c) * P.npts + gq] = M[c];
+      for (int c = 0; c < S; ++c) tt[c] = io[c * NPB + q[j]];
+      W[j] = weights32(tt);
+    }
+    float acc[K][NP];
+    const float4 *base = g4 + (int64_t)cell0 * 3;
+#pragma unroll
+    for (int c = 0; c < 16; ++c) {
+      const int b0 = (c >> 3) & 1, b1 = (c >> 2) & 1, b2 = (c >> 1) & 1, b3 = c & 1;
+      const float4 *node = base + b0 * s0 + b1 * s1 + b2 * s2 + b3 * s3;
+      const float4 a = __ldg(node), b = __ldg(node + 1), f = __ldg(node + 2);
+#pragma unroll
+      for (int j = 0; j < K; ++j) corner_acc32(c, W[j].wa[c >> 2] * W[j].wb[c & 3], a, b, f, acc[j]);
+    }
+    // mu = table value + offset; rows in chem32's order (X_Fe stays in row 9)
+#pragma unroll
+    for (int j = 0; j < K; ++j) {
+      if (!use[j]) continue;
+#pragma unroll
+      for (int c = 0; c < S; ++c) io[c * NPB + q[j]] = acc[j][c] + io[(S + c) * NPB + q[j]];
+#pragma unroll
+      for (int c = 0; c < NM; ++c) io[(S + c) * NPB + q[j]] = acc[j][S + c];
+    }
+  }
+  __syncthreads();
+  // 5. points set aside and points outside the linear region, one per thread
+  unsigned flags = 0;
+  const int nnn = cnt[255], nl = nnn + *nleft;
+  for (int l = tid; l < nl; l += NT) {
+    const int q = l < nnn ? (int)order[lin_end + l] : (int)left[l - nnn];
+    const int cell = __float_as_int(io[8 * NPB + q]);
+    float a[S], v[NP];
+#pragma unroll
+    for (int c = 0; c < S; ++c) a[c] = io[c * NPB + q];
+    if (cell < 0) nearest_row32(T, a, v, &flags);
+    else interp_nodes32(g4 + (int64_t)cell * 3, (int)s0, (int)s1, (int)s2, (int)s3, a, v);
+#pragma unroll
+    for (int c = 0; c < S; ++c) io[c * NPB + q] = v[c] + io[(S + c) * NPB + q];
+#pragma unroll
+    for (int c = 0; c < NM; ++c) io[(S + c) * NPB + q] = v[S + c];
   }
   raise_rate_flags(P.st, flags);
-}
-
-// Copies (cp.async) of one plane's composition hi and mu/M at the tile and
-// its 1-cell halo (corners skipped; the tile only when interior_only) into a
-// ring slot: X in the 2-halo SoA layout of the face routines, mu/M in the
-// mu_plane32 layout.  Commit and wait are the caller's.
-template <int TX, int TY>
-__device__ __forceinline__ void copy_plane_async32(const Rate32 &P, int64_t zoff, const int *wx,
-                                                   const int *wy, bool interior_only, float *xdst,
-                                                   float *mdst, int tid) {
-  using G = PlaneGeom<TX, TY>;
-  for (int pos = tid; pos < G::PM; pos += G::NT) {
-    const int my = pos / G::MX, mx = pos - my * G::MX;
-    if (skip_pos<G::MX, G::MY>(mx, my, interior_only)) continue;
-    const int64_t g = zoff + (int64_t)wy[my + 1] * P.nx + wx[mx + 1];
-    const int px = (my + 1) * G::HX + (mx + 1);
-    const float *src = reinterpret_cast<const float *>(P.D + g);
-#pragma unroll
-    for (int c = 0; c < S; ++c) __pipeline_memcpy_async(xdst + c * G::PX + px, src + c, 4);
-#pragma unroll
-    for (int c = 0; c < NP; ++c) __pipeline_memcpy_async(mdst + c * G::PM + pos, P.mm + c * P.npts + g, 4);
+  __syncthreads();
+  // 6. coalesced stores
+#pragma unroll 1
+  for (int j = 0; j < K; ++j) {
+    const int q = tid + j * NT;
+    const int qx = q % G::BX, qy = (q / G::BX) % G::BY, qz = q / (G::BX * G::BY);
+    const int x = blockIdx.x * G::BX + qx, y = blockIdx.y * G::BY + qy, z = blockIdx.z * G::BZ + qz;
+    if (x >= P.nx || y >= P.ny || z >= P.nz) continue;
+    const int64_t g = (int64_t)z * plane + (int64_t)y * P.nx + x;
+    const float *v = io + q;
+    P.mm_mu[g] = make_float4(v[0], v[NPB], v[2 * NPB], v[3 * NPB]);
+    P.mm_m[g] = make_float4(v[5 * NPB], v[6 * NPB], v[7 * NPB], v[8 * NPB]);
+    P.mm_f[g] = make_float2(v[4 * NPB], v[9 * NPB]);
   }
 }
 
+template <int DIM, int K, int MINB>
+void chem32_attrs() {
+  cudaFuncSetAttribute(k32_chem<DIM, K, MINB>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                       (int)ChemGeom<DIM, K>::smem);
+}
+
+template <int DIM, int K, int MINB>
+void launch_chem32(cudaStream_t s, const Rate32 &P) {
+  using G = ChemGeom<DIM, K>;
+  const dim3 g((unsigned)((P.nx + G::BX - 1) / G::BX), (unsigned)((P.ny + G::BY - 1) / G::BY),
+               (unsigned)((P.nz + G::BZ - 1) / G::BZ));
+  launch_pdl(k32_chem<DIM, K, MINB>, g, dim3(kChemThreads), G::smem, s, P);
+}
+
+// ------------------------------------------------------------------------
 // Split rate evaluation, second kernel in 3D: face fluxes and divergence of
-// a plane tile marching along axis 0, mu/M read from P.mm.  The copies of
-// plane z+2 are in flight while plane z is evaluated (three-slot rings for
-// X and mu/M).  Same face routine and divergence order as k32_rate_march3d.
-template <int TX, int TY, int MINB, bool PERPOINT = false>
-__global__ void __launch_bounds__(TX * TY, MINB) k32_flux_march3d(Rate32 P, int zc) {
-  using G = PlaneGeom<TX, TY>;
+// a TX x TY plane tile marching along axis 0, from the split buffers.  Each
+// plane position of the tile and its 1-cell halo (corners skipped) is
+// staged as it is stored -- float4 D, float4 mu, float4 M, float2 (M_Fe,
+// X_Fe) -- by cp.async into a three-slot ring, so plane z+2 is in flight
+// while plane z is evaluated.  PERPOINT: each point evaluates its four
+// in-plane faces (a face by both of its cells, with the same operands and
+// operation order); otherwise each in-plane face is evaluated once into
+// shared buffers.  Same face routine and divergence order as the fused
+// marching kernel.
+// ------------------------------------------------------------------------
+template <int TX, int TY>
+struct Flux3Geom {
+  static constexpr int MX = TX + 2, MY = TY + 2, PM = MX * MY, NT = TX * TY;
+  static constexpr int NFX = TY * (TX + 1), NFY = (TY + 1) * TX;
+  static constexpr size_t slot = (size_t)PM * (3 * 16 + 8);       // bytes per ring slot
+  static constexpr size_t smem(bool perpoint) {
+    return 3 * slot + (perpoint ? 0 : (size_t)(NFX + NFY) * 16) + (NT / 32) * 8 +
+           (MX + MY) * 4;
+  }
+};
+
+template <int TX, int TY, int MINB, bool PERPOINT>
+__global__ void __launch_bounds__(TX * TY, MINB) k32_flux3(Rate32 P, int zc) {
+  using G = Flux3Geom<TX, TY>;
+  static_assert(G::slot % 16 == 0, "ring slots must stay 16-byte aligned");
   pdl_wait();
   if (P.st->halt) return;
   extern __shared__ float4 sm4[];
-  double *red = reinterpret_cast<double *>(sm4);
-  float *Xs = reinterpret_cast<float *>(red + G::NT / 32);      // [3][S][PX]
-  float *Ms = Xs + 3 * S * G::PX;                                // [3][NP][PM]
-  float *Fx = Ms + 3 * NP * G::PM;
-  float *Fy = Fx + S * G::NFX;
-  int *wx = reinterpret_cast<int *>(Fy + S * G::NFY);
-  int *wy = wx + G::HX;
+  // ring slot r: D[PM], mu[PM], M[PM] (float4) then F[PM] (float2)
+  float4 *ring = sm4;
+  float4 *Fx = reinterpret_cast<float4 *>(reinterpret_cast<char *>(sm4) + 3 * G::slot);
+  float4 *Fy = Fx + (PERPOINT ? 0 : G::NFX);
+  double *red = reinterpret_cast<double *>(Fy + (PERPOINT ? 0 : G::NFY));
+  int *wx = reinterpret_cast<int *>(red + G::NT / 32);
+  int *wy = wx + G::MX;
   const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * TX + tx;
   const int x0 = blockIdx.x * TX, y0 = blockIdx.y * TY;
   const int zb = blockIdx.z * zc;
   const int ze = min(zb + zc, P.nz);
   const int64_t plane = (int64_t)P.ny * P.nx;
-  for (int i = tid; i < G::HX + G::HY; i += G::NT) {
-    if (i < G::HX) wx[i] = wrap_any(x0 + i - 2, P.nx);
-    else wy[i - G::HX] = wrap_any(y0 + (i - G::HX) - 2, P.ny);
+  for (int i = tid; i < G::MX + G::MY; i += G::NT) {
+    if (i < G::MX) wx[i] = wrap_any(x0 + i - 1, P.nx);
+    else wy[i - G::MX] = wrap_any(y0 + (i - G::MX) - 1, P.ny);
   }
   __syncthreads();
-  auto slot = [&](int z) { return (z - zb + 3) % 3; };
-  auto xplane = [&](int z) { return Xs + slot(z) * S * G::PX; };
-  auto mplane = [&](int z) { return Ms + slot(z) * NP * G::PM; };
+  auto sD = [&](int z) { return ring + ((z - zb + 3) % 3) * (G::slot / 16); };
+  auto sMu = [&](int z) { return sD(z) + G::PM; };
+  auto sM = [&](int z) { return sD(z) + 2 * G::PM; };
+  auto sF = [&](int z) { return reinterpret_cast<float2 *>(sD(z) + 3 * G::PM); };
   auto issue = [&](int z, bool interior_only) {
-    copy_plane_async32<TX, TY>(P, (int64_t)wrap_any(z, P.nz) * plane, wx, wy, interior_only,
-                               xplane(z), mplane(z), tid);
+    const int64_t zoff = (int64_t)wrap_any(z, P.nz) * plane;
+    float4 *d = sD(z), *mu = sMu(z), *m = sM(z);
+    float2 *f = sF(z);
+    for (int pos = tid; pos < G::PM; pos += G::NT) {
+      const int my = pos / G::MX, mx = pos - my * G::MX;
+      const bool ex = (mx == 0 || mx == G::MX - 1), ey = (my == 0 || my == G::MY - 1);
+      if (interior_only ? (ex || ey) : (ex && ey)) continue;
+      const int64_t g = zoff + (int64_t)wy[my] * P.nx + wx[mx];
+      __pipeline_memcpy_async(d + pos, P.D + g, 16);
+      __pipeline_memcpy_async(mu + pos, P.mm_mu + g, 16);
+      __pipeline_memcpy_async(m + pos, P.mm_m + g, 16);
+      __pipeline_memcpy_async(f + pos, P.mm_f + g, 8);
+    }
     __pipeline_commit();
   };
-  const int pX = (ty + 2) * G::HX + (tx + 2);
-  const int pM = (ty + 1) * G::MX + (tx + 1);
+  auto face = [&](int zl, int pl, int zh, int ph) {
+    return face_flux32(P, sD(zl)[pl], sMu(zl)[pl], sM(zl)[pl], sF(zl)[pl], sD(zh)[ph],
+                       sMu(zh)[ph], sM(zh)[ph], sF(zh)[ph]);
+  };
+  const int p = (ty + 1) * G::MX + (tx + 1);
   const bool in_tile = (x0 + tx < P.nx) && (y0 + ty < P.ny);
   issue(zb - 1, true);
   issue(zb, false);
   issue(zb + 1, false);
   __pipeline_wait_prior(1);
   __syncthreads();
-  float Jm[S];
-  face32_between<G::PX, G::PM>(P, xplane(zb - 1), mplane(zb - 1), pX, pM, xplane(zb), mplane(zb),
-                               pX, pM, Jm);
+  float4 Jm = face(zb - 1, p, zb, p);
   float vmax = 0.f;
   for (int z = zb; z < ze; ++z) {
     __pipeline_wait_prior(0);          // plane z+1 copied (this thread's part)
     __syncthreads();                   // ... and every thread's; slot of z-1 free
     if (z + 2 <= ze) issue(z + 2, false);
-    float Jz[S];
-    face32_between<G::PX, G::PM>(P, xplane(z), mplane(z), pX, pM, xplane(z + 1), mplane(z + 1),
-                                 pX, pM, Jz);
-    float jyp[S], jym[S], jxp[S], jxm[S];
+    const float4 Jz = face(z, p, z + 1, p);
+    float4 jyp, jym, jxp, jxm;
     if constexpr (PERPOINT) {
-      // each point evaluates its four in-plane faces (each face by both of
-      // its cells, identical operands and order): no face buffers, no barrier
-      const float *Xp = xplane(z), *Mp = mplane(z);
-      face32_between<G::PX, G::PM>(P, Xp, Mp, pX, pM, Xp, Mp, pX + G::HX, pM + G::MX, jyp);
-      face32_between<G::PX, G::PM>(P, Xp, Mp, pX - G::HX, pM - G::MX, Xp, Mp, pX, pM, jym);
-      face32_between<G::PX, G::PM>(P, Xp, Mp, pX, pM, Xp, Mp, pX + 1, pM + 1, jxp);
-      face32_between<G::PX, G::PM>(P, Xp, Mp, pX - 1, pM - 1, Xp, Mp, pX, pM, jxm);
+      jyp = face(z, p, z, p + G::MX);
+      jym = face(z, p - G::MX, z, p);
+      jxp = face(z, p, z, p + 1);
+      jxm = face(z, p - 1, z, p);
     } else {
-      plane_faces32<TX, TY>(P, xplane(z), mplane(z), Fx, Fy, tid);
-      __syncthreads();
-#pragma unroll
-      for (int c = 0; c < S; ++c) {
-        jyp[c] = Fy[c * G::NFY + (ty + 1) * TX + tx];
-        jym[c] = Fy[c * G::NFY + ty * TX + tx];
-        jxp[c] = Fx[c * G::NFX + ty * (TX + 1) + tx + 1];
-        jxm[c] = Fx[c * G::NFX + ty * (TX + 1) + tx];
+      for (int f = tid; f < G::NFX + G::NFY; f += G::NT) {
+        if (f < G::NFX) {
+          const int fy = f / (TX + 1), fx = f - fy * (TX + 1);
+          const int pl = (fy + 1) * G::MX + fx;
+          Fx[f] = face(z, pl, z, pl + 1);
+        } else {
+          const int f2 = f - G::NFX;
+          const int fy = f2 / TX, fx = f2 - fy * TX;
+          const int pl = fy * G::MX + (fx + 1);
+          Fy[f2] = face(z, pl, z, pl + G::MX);
+        }
       }
+      __syncthreads();
+      jyp = Fy[(ty + 1) * TX + tx];
+      jym = Fy[ty * TX + tx];
+      jxp = Fx[ty * (TX + 1) + tx + 1];
+      jxm = Fx[ty * (TX + 1) + tx];
     }
     if (in_tile) {
+      const float a[S] = {Jz.x - Jm.x, Jz.y - Jm.y, Jz.z - Jm.z, Jz.w - Jm.w};
+      const float ay[S] = {jyp.x - jym.x, jyp.y - jym.y, jyp.z - jym.z, jyp.w - jym.w};
+      const float ax[S] = {jxp.x - jxm.x, jxp.y - jxm.y, jxp.z - jxm.z, jxp.w - jxm.w};
       float out[S];
 #pragma unroll
-      for (int c = 0; c < S; ++c) {
-        const float a = __fadd_rn(__fadd_rn(__fsub_rn(Jz[c], Jm[c]), __fsub_rn(jyp[c], jym[c])),
-                                  __fsub_rn(jxp[c], jxm[c]));
-        out[c] = __fmul_rn(a, P.inv_dx);
-      }
+      for (int c = 0; c < S; ++c) out[c] = ((a[c] + ay[c]) + ax[c]) * P.flux_scale;
       store_rate(P.dX, (int64_t)z * plane + (int64_t)(y0 + ty) * P.nx + (x0 + tx), out, vmax);
     }
-#pragma unroll
-    for (int c = 0; c < S; ++c) Jm[c] = Jz[c];
+    Jm = Jz;
   }
   __pipeline_wait_prior(0);
   finish_rate32(P, vmax, red);
-}
-
-template <int TX, int TY>
-constexpr size_t flux_march3d32_smem() {
-  using G = PlaneGeom<TX, TY>;
-  return (G::NT / 32) * sizeof(double) +
-         (3 * S * G::PX + 3 * NP * G::PM + S * G::NFX + S * G::NFY) * sizeof(float) +
-         (G::HX + G::HY) * sizeof(int);
-}
-
-template <int DIM, int KMINB>
-void launch_chem32(cudaStream_t s, const Rate32 &P) {
-  const dim3 b(32, 8), g((unsigned)((P.nx + 31) / 32), (unsigned)((P.ny + 7) / 8), (unsigned)P.nz);
-  launch_pdl(k32_chem<DIM, KMINB>, g, b, 0, s, P);
 }
 
 // The dt controller after a rate launch of `nparts` blocks: a block-wide
@@ -658,9 +794,10 @@ Variant32 make_variant32() {
   return v;
 }
 
-// Split variant: k32_chem over all points, then the tile / marching kernel
-// reading mu/M back.
-template <int TX, int TY, int MINB, int KMINB, bool PP = false>
+// Split variant: k32_chem (K points per work item, KMINB resident blocks)
+// over all points, then the tile kernel (2D) or the marching flux kernel
+// (3D, PP: per-point faces) reading mu/M back.
+template <int TX, int TY, int MINB, int K, int KMINB, bool PP = false>
 Variant32 make_split_variant32() {
   Variant32 v;
   v.tx = TX;
@@ -668,25 +805,27 @@ Variant32 make_split_variant32() {
   v.minb = MINB;
   v.split = true;
   v.smem2d = tile2d32_smem<TX, TY>();
-  v.smem3d = flux_march3d32_smem<TX, TY>();
+  v.smem3d = Flux3Geom<TX, TY>::smem(PP);
   v.set_attrs = []() {
     const auto a = cudaFuncAttributeMaxDynamicSharedMemorySize;
     cudaFuncSetAttribute(k32_rate_tile2d<TX, TY, MINB, false, false, true>, a,
                          (int)tile2d32_smem<TX, TY>());
-    cudaFuncSetAttribute(k32_flux_march3d<TX, TY, MINB, PP>, a, (int)flux_march3d32_smem<TX, TY>());
+    cudaFuncSetAttribute(k32_flux3<TX, TY, MINB, PP>, a, (int)Flux3Geom<TX, TY>::smem(PP));
+    chem32_attrs<2, K, KMINB>();
+    chem32_attrs<3, K, KMINB>();
   };
   v.launch2d = [](dim3 g, dim3 b, size_t sm, cudaStream_t s, const Rate32 &P) {
-    launch_chem32<2, KMINB>(s, P);
+    launch_chem32<2, K, KMINB>(s, P);
     launch_pdl(k32_rate_tile2d<TX, TY, MINB, false, false, true>, g, b, sm, s, P);
   };
   v.launch3d = [](dim3 g, dim3 b, size_t sm, cudaStream_t s, const Rate32 &P, int zc) {
-    launch_chem32<3, KMINB>(s, P);
-    launch_pdl(k32_flux_march3d<TX, TY, MINB, PP>, g, b, sm, s, P, zc);
+    launch_chem32<3, K, KMINB>(s, P);
+    launch_pdl(k32_flux3<TX, TY, MINB, PP>, g, b, sm, s, P, zc);
   };
   v.kernels = [](int dim) {
-    const std::string chem = kname("k32_chem", {dim, KMINB}) + " + ";
+    const std::string chem = kname("k32_chem", {dim, K, KMINB}) + " + ";
     if (dim == 2) return chem + kname("k32_rate_tile2d", {TX, TY, MINB, 0, 0, 1, 0});
-    return chem + kname("k32_flux_march3d", {TX, TY, MINB, PP});
+    return chem + kname("k32_flux3", {TX, TY, MINB, PP});
   };
   return v;
 }
@@ -698,12 +837,12 @@ const std::vector<Variant32> &variants32() {
       make_variant32<32, 8, 2, false>(), make_variant32<32, 16, 2, false>(),
       make_variant32<32, 8, 2, true, true>(), make_variant32<32, 8, 3, false, true>(),
       make_variant32<32, 16, 2, false, true>(), make_variant32<32, 8, 2, false, true>(),
-      make_split_variant32<32, 8, 3, 3>(), make_split_variant32<32, 16, 2, 3>(),
-      make_split_variant32<32, 8, 4, 4>(), make_split_variant32<32, 16, 2, 4>(),
       make_variant32<32, 8, 3, false, true, true>(), make_variant32<32, 16, 2, false, true, true>(),
       make_variant32<32, 8, 3, false, false, true>(), make_variant32<32, 16, 2, false, false, true>(),
-      make_split_variant32<32, 8, 4, 4, true>(), make_split_variant32<32, 16, 2, 4, true>(),
-      make_split_variant32<32, 16, 2, 5, true>(), make_split_variant32<32, 16, 2, 6, true>()};
+      make_split_variant32<32, 8, 3, 2, 4, true>(), make_split_variant32<32, 8, 3, 4, 2, true>(),
+      make_split_variant32<32, 8, 3, 2, 4, false>(), make_split_variant32<32, 8, 3, 4, 2, false>(),
+      make_split_variant32<32, 16, 1, 4, 2, true>(), make_split_variant32<32, 4, 6, 4, 2, true>(),
+      make_split_variant32<64, 4, 3, 4, 2, true>(), make_split_variant32<32, 8, 3, 4, 3, true>()};
   return v;
 }
 
@@ -718,7 +857,7 @@ struct Stepper32 {
   bool plans = false;
   double *mass_ws = nullptr;
   double *partial = nullptr;     // rate kernel block maxima
-  float *mm = nullptr;           // split-rate mu/M buffer (2D/3D)
+  float *mm = nullptr;           // split-rate buffers: mu, M, (M_Fe, X_Fe) per point
   StepState32 *st = nullptr;
   Rate32 rp{};
   Update32 up{};
@@ -933,7 +1072,7 @@ pf5d_status s32_create(const pf5d_stepper_desc *desc, const double *X_init, void
   }
   T.sum_x0 = sx;
   P.c_fe = 1.0 - sx;
-  P.inv_dx = (float)(1.0 / desc->dx);
+  P.flux_scale = (float)(0.5 / (desc->dx * desc->dx));
   P.inv_dx2 = (float)(1.0 / (desc->dx * desc->dx));
   P.ctld = desc->ctld;
   P.t_cfl = desc->t_cfl;
@@ -948,11 +1087,14 @@ pf5d_status s32_create(const pf5d_stepper_desc *desc, const double *X_init, void
   }
   P.partial = h->partial;
   P.npts = npts;
-  if (cudaMalloc(&h->mm, (size_t)npts * NP * sizeof(float)) != cudaSuccess) {
+  // split buffers: mu (float4), M (float4), (M_Fe, X_Fe) (float2) per point
+  if (cudaMalloc(&h->mm, (size_t)npts * (2 * sizeof(float4) + sizeof(float2))) != cudaSuccess) {
     set_error("device allocation failed");
     return fail(PF5D_ERR_CUDA);
   }
-  P.mm = h->mm;
+  P.mm_mu = reinterpret_cast<float4 *>(h->mm);
+  P.mm_m = P.mm_mu + npts;
+  P.mm_f = reinterpret_cast<float2 *>(P.mm_m + npts);
   Update32 &U = h->up;
   U.hi = h->hi;
   U.lo = h->lo;
@@ -1022,6 +1164,19 @@ __global__ void k32_widen(const float *__restrict__ src, int64_t n, double *__re
     dst[i] = (double)src[i];
 }
 
+// FP64 mu/M rows (SoA, 9 rows: mu_1..4, M_Fe, M_1..4) from the split buffers.
+__global__ void k32_widen_mm(Rate32 P, double *__restrict__ dst) {
+  const int64_t n = P.npts;
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
+       i += (int64_t)gridDim.x * blockDim.x) {
+    const float4 mu = P.mm_mu[i], m = P.mm_m[i];
+    const float2 f = P.mm_f[i];
+    const float v[NP] = {mu.x, mu.y, mu.z, mu.w, f.x, m.x, m.y, m.z, m.w};
+#pragma unroll
+    for (int r = 0; r < NP; ++r) dst[r * n + i] = (double)v[r];
+  }
+}
+
 pf5d_status s32_step_save_inputs(Stepper32 *h, double *X_out, double *dX_out, double *mm_out,
                                  void *stream) {
   cudaStream_t s = as_stream(stream);
@@ -1036,9 +1191,9 @@ pf5d_status s32_step_save_inputs(Stepper32 *h, double *X_out, double *dX_out, do
   pf5d_status st = launch_rate32(h, s);
   if (st != PF5D_OK) return st;
   switch (h->d.dim) {
-    case 1: launch_chem32<1, 3>(s, h->rp); break;
-    case 2: launch_chem32<2, 3>(s, h->rp); break;
-    default: launch_chem32<3, 3>(s, h->rp);
+    case 1: chem32_attrs<1, 2, 3>(); launch_chem32<1, 2, 3>(s, h->rp); break;
+    case 2: chem32_attrs<2, 2, 3>(); launch_chem32<2, 2, 3>(s, h->rp); break;
+    default: chem32_attrs<3, 2, 3>(); launch_chem32<3, 2, 3>(s, h->rp);
   }
   PF5D_LAUNCHED();
   k32_join<<<grid_for(h->npts, 256, 4), 256, 0, s>>>(h->hi, h->lo, h->npts, h->up, X_out);
@@ -1046,7 +1201,7 @@ pf5d_status s32_step_save_inputs(Stepper32 *h, double *X_out, double *dX_out, do
   k32_widen<<<grid_for(4 * h->npts, 256, 4), 256, 0, s>>>(reinterpret_cast<const float *>(h->dX),
                                                           4 * h->npts, dX_out);
   PF5D_LAUNCHED();
-  k32_widen<<<grid_for(NP * h->npts, 256, 4), 256, 0, s>>>(h->mm, NP * h->npts, mm_out);
+  k32_widen_mm<<<grid_for(h->npts, 256, 4), 256, 0, s>>>(h->rp, mm_out);
   PF5D_LAUNCHED();
   return PF5D_OK;
 }
