@@ -385,6 +385,241 @@ __global__ void __launch_bounds__(256, MINB) k_chem64(RateParams P) {
   raise_rate_flags(P.st, flags);
 }
 
+// Split rate evaluation, first kernel, shared-gather form: the same values
+// as k_chem64 (bit for bit), with the table gathers of up to K points of one
+// table cell shared.  A block of 256 threads takes a brick of 256 K points
+// (32 x 8 x K in 3D, 32 x 8K in 2D, 256K in 1D):
+//   1. per point: x, the Laplacian (k_chem64's order) and s', the table
+//      cell (axis_coord of interpolation.py:110-121) or "nearest row";
+//   2. counting sort of the points by a hash of their cell (bin 255: points
+//      outside the linear region);
+//   3. each linear bin's run is cut into work items of up to K points;
+//   4. a thread evaluates an item: each corner node is loaded once and its
+//      term w * v accumulated into every point of the item, each point with
+//      its own weight ((w0 w1) w2) w3 and the reference's left-to-right
+//      16-term sum, so every value is the one k_chem64 computes.  Points
+//      whose cell differs from the item's first (hash collisions) are set
+//      aside;
+//   5. the points set aside and the nearest-row points, one per thread;
+//   6. coalesced stores of the SoA rows.
+constexpr int kChem64Threads = 256;
+
+template <int DIM, int K>
+struct Chem64Geom {
+  static constexpr int NPB = kChem64Threads * K;
+  static constexpr int BX = DIM == 1 ? NPB : 32;
+  static constexpr int BY = DIM == 1 ? 1 : (DIM == 2 ? 8 * K : 8);
+  static constexpr int BZ = DIM == 3 ? K : 1;
+  static constexpr int NITEMS = NPB / K + 256;
+  // io[9][NPB] doubles, cell[NPB] int, items[NITEMS] u32, order/prank/left
+  // [NPB] u16, skey/pkey [NPB] u8, hist/cnt/ibase [256] int, wsum + nleft
+  static constexpr size_t smem = (size_t)9 * NPB * 8 + NPB * 4 + NITEMS * 4 + 3 * NPB * 2 +
+                                 2 * NPB + 3 * 256 * 4 + 16 * 4;
+};
+
+template <int DIM, bool VEC, int K, int MINB>
+__global__ void __launch_bounds__(kChem64Threads, MINB) k_chem64i(RateParams P) {
+  using G = Chem64Geom<DIM, K>;
+  constexpr int NT = kChem64Threads, NPB = G::NPB;
+  extern __shared__ double2 smd[];
+  double *io = reinterpret_cast<double *>(smd);                        // [9][NPB]
+  int *cellv = reinterpret_cast<int *>(io + 9 * NPB);
+  unsigned *items = reinterpret_cast<unsigned *>(cellv + NPB);
+  unsigned short *order = reinterpret_cast<unsigned short *>(items + G::NITEMS);
+  unsigned short *prank = order + NPB;
+  unsigned short *left = prank + NPB;
+  unsigned char *skey = reinterpret_cast<unsigned char *>(left + NPB);
+  unsigned char *pkey = skey + NPB;
+  int *hist = reinterpret_cast<int *>(pkey + NPB);
+  int *cnt = hist + 256;
+  int *ibase = cnt + 256;
+  int *wsum = ibase + 256;
+  int *nleft = wsum + 12;
+  pdl_wait();
+  if (P.st->halt) return;
+  const int tid = threadIdx.x;
+  const Table &T = P.T;
+  const int64_t plane = (int64_t)P.ny * P.nx;
+  hist[tid] = 0;
+  if (tid == 0) *nleft = 0;
+  __syncthreads();
+  // 1. per-point inputs
+#pragma unroll 1
+  for (int j = 0; j < K; ++j) {
+    const int q = tid + j * NT;
+    const int qx = q % G::BX, qy = (q / G::BX) % G::BY, qz = q / (G::BX * G::BY);
+    const int x = blockIdx.x * G::BX + qx, y = blockIdx.y * G::BY + qy, z = blockIdx.z * G::BZ + qz;
+    prank[q] = kNoRank;
+    if (x >= P.nx || y >= P.ny || z >= P.nz) continue;
+    const int64_t zo = (int64_t)z * plane, g = zo + (int64_t)y * P.nx + x;
+    auto ld = [&](int64_t gi, double v[S]) {
+      const double2 a = __ldg(reinterpret_cast<const double2 *>(P.X + 4 * gi));
+      const double2 b = __ldg(reinterpret_cast<const double2 *>(P.X + 4 * gi) + 1);
+      v[0] = a.x; v[1] = a.y; v[2] = b.x; v[3] = b.y;
+    };
+    const int xp = x + 1 == P.nx ? 0 : x + 1, xm = x == 0 ? P.nx - 1 : x - 1;
+    double xc[S], lap[S], n0[S], n1[S];
+    ld(g, xc);
+    if (DIM == 3) {
+      const int zp = z + 1 == P.nz ? 0 : z + 1, zm = z == 0 ? P.nz - 1 : z - 1;
+      ld((int64_t)zp * plane + (int64_t)y * P.nx + x, n0);
+      ld((int64_t)zm * plane + (int64_t)y * P.nx + x, n1);
+#pragma unroll
+      for (int c = 0; c < S; ++c) lap[c] = n0[c] + n1[c];
+    }
+    if (DIM >= 2) {
+      const int yp = y + 1 == P.ny ? 0 : y + 1, ym = y == 0 ? P.ny - 1 : y - 1;
+      ld(zo + (int64_t)yp * P.nx + x, n0);
+      ld(zo + (int64_t)ym * P.nx + x, n1);
+#pragma unroll
+      for (int c = 0; c < S; ++c) lap[c] = DIM == 3 ? (lap[c] + n0[c]) + n1[c] : n0[c] + n1[c];
+    }
+    ld(zo + (int64_t)y * P.nx + xp, n0);
+    ld(zo + (int64_t)y * P.nx + xm, n1);
+#pragma unroll
+    for (int c = 0; c < S; ++c) {
+      if (DIM == 1)
+        lap[c] = ((n0[c] + n1[c]) - 2.0 * xc[c]) * P.inv_dx2;
+      else
+        lap[c] = (((lap[c] + n0[c]) + n1[c]) - (DIM == 3 ? 6.0 : 4.0) * xc[c]) * P.inv_dx2;
+      io[c * NPB + q] = xc[c];
+      io[(S + c) * NPB + q] = lap[c];
+    }
+    io[8 * NPB + q] = P.sp ? __ldg(P.sp + g) : 0.0;
+    int ii[S];
+    double tt[S];
+    int cell = -1, key = 255;
+    if (cell64(T, xc, ii, tt)) {
+      cell = ((ii[0] * T.n + ii[1]) * T.n + ii[2]) * T.n + ii[3];
+      key = (int)((unsigned)(41 * ii[0] + 13 * ii[1] + 5 * ii[2] + ii[3]) % 255u);
+    }
+    cellv[q] = cell;
+    pkey[q] = (unsigned char)key;
+    prank[q] = (unsigned short)atomicAdd(&hist[key], 1);
+  }
+  __syncthreads();
+  // 2. counting sort by cell key
+  cnt[tid] = hist[tid];
+  const int nvalid = block_exclusive_scan<256, NT>(hist, wsum, tid);
+  for (int q = tid; q < NPB; q += NT) {
+    if (prank[q] == kNoRank) continue;
+    const int b = pkey[q], s = hist[b] + prank[q];
+    order[s] = (unsigned short)q;
+    skey[s] = (unsigned char)b;
+  }
+  // 3. work items of up to K points of one linear bin
+  ibase[tid] = tid == 255 ? 0 : (cnt[tid] + K - 1) / K;
+  const int nitems = block_exclusive_scan<256, NT>(ibase, wsum, tid);
+  const int lin_end = nvalid - cnt[255];
+  for (int s = tid; s < lin_end; s += NT) {
+    const int b = skey[s], r = s - hist[b];
+    if (r % K == 0) items[ibase[b] + r / K] = (unsigned)s | ((unsigned)min(K, cnt[b] - r) << 16);
+  }
+  __syncthreads();
+  // 4. the work items
+  const int64_t s3 = T.stride, s2 = (int64_t)T.n * s3, s1 = (int64_t)T.n * s2,
+                s0 = (int64_t)T.n * s1;
+  for (int it = tid; it < nitems; it += NT) {
+    const unsigned e = items[it];
+    const int s = (int)(e & 0xFFFFu), m = (int)(e >> 16);
+    int q[K];
+    bool use[K];
+    double tt[K][S], qq[K][S];
+    int cell0 = 0;
+#pragma unroll
+    for (int j = 0; j < K; ++j) {
+      q[j] = j < m ? (int)order[s + j] : 0;
+      const int cj = cellv[q[j]];
+      if (j == 0) cell0 = cj;
+      use[j] = j < m && cj == cell0;
+      if (j < m && !use[j]) left[atomicAdd(nleft, 1)] = (unsigned short)q[j];
+#pragma unroll
+      for (int a = 0; a < S; ++a) {
+        int i;
+        axis_coord(io[a * NPB + q[j]] * T.inv_step, T.n, i, tt[j][a]);
+        qq[j][a] = 1.0 - tt[j][a];
+      }
+    }
+    double acc[K][NP];
+    const double *base = T.grid + (int64_t)cell0 * s3;
+#pragma unroll
+    for (int c = 0; c < 16; ++c) {
+      const int b0 = (c >> 3) & 1, b1 = (c >> 2) & 1, b2 = (c >> 1) & 1, b3 = c & 1;
+      const double *node = base + b0 * s0 + b1 * s1 + b2 * s2 + b3 * s3;
+      double v[NP + 1];
+      if (VEC) {
+        const double2 *n2 = reinterpret_cast<const double2 *>(node);
+#pragma unroll
+        for (int k = 0; k < (NP + 1) / 2; ++k) {
+          const double2 a = __ldg(n2 + k);
+          v[2 * k] = a.x;
+          v[2 * k + 1] = a.y;
+        }
+      } else {
+#pragma unroll
+        for (int p = 0; p < NP; ++p) v[p] = __ldg(node + p);
+      }
+#pragma unroll
+      for (int j = 0; j < K; ++j) {
+        const double w = (b0 ? tt[j][0] : qq[j][0]) * (b1 ? tt[j][1] : qq[j][1]) *
+                         (b2 ? tt[j][2] : qq[j][2]) * (b3 ? tt[j][3] : qq[j][3]);
+#pragma unroll
+        for (int p = 0; p < NP; ++p) {
+          const double term = w * v[p];
+          acc[j][p] = (c == 0) ? term : acc[j][p] + term;
+        }
+      }
+    }
+#pragma unroll
+    for (int j = 0; j < K; ++j) {
+      if (!use[j]) continue;
+#pragma unroll
+      for (int c = 0; c < S; ++c) {
+        const double lk = io[(S + c) * NPB + q[j]] * P.kappa.v[c];
+        double mu = acc[j][c] - lk;
+        if (P.sp) mu = mu + io[8 * NPB + q[j]] * P.lvec.v[c];
+        io[c * NPB + q[j]] = mu;
+      }
+#pragma unroll
+      for (int c = 0; c < NM; ++c) io[(S + c) * NPB + q[j]] = acc[j][S + c];
+    }
+  }
+  __syncthreads();
+  // 5. points set aside and points outside the linear region, one per thread
+  unsigned flags = 0;
+  const int nnn = cnt[255], nl = nnn + *nleft;
+  for (int l = tid; l < nl; l += NT) {
+    const int q = l < nnn ? (int)order[lin_end + l] : (int)left[l - nnn];
+    double xq[S], v[NP];
+#pragma unroll
+    for (int c = 0; c < S; ++c) xq[c] = io[c * NPB + q];
+    const int o[S] = {0, 0, 0, 0};
+    interp_win64<VEC>(T, xq, nullptr, o, v, &flags);
+#pragma unroll
+    for (int c = 0; c < S; ++c) {
+      const double lk = io[(S + c) * NPB + q] * P.kappa.v[c];
+      double mu = v[c] - lk;
+      if (P.sp) mu = mu + io[8 * NPB + q] * P.lvec.v[c];
+      io[c * NPB + q] = mu;
+    }
+#pragma unroll
+    for (int c = 0; c < NM; ++c) io[(S + c) * NPB + q] = v[S + c];
+  }
+  raise_rate_flags(P.st, flags);
+  __syncthreads();
+  // 6. coalesced stores of the SoA rows
+#pragma unroll 1
+  for (int j = 0; j < K; ++j) {
+    const int q = tid + j * NT;
+    const int qx = q % G::BX, qy = (q / G::BX) % G::BY, qz = q / (G::BX * G::BY);
+    const int x = blockIdx.x * G::BX + qx, y = blockIdx.y * G::BY + qy, z = blockIdx.z * G::BZ + qz;
+    if (x >= P.nx || y >= P.ny || z >= P.nz) continue;
+    const int64_t g = (int64_t)z * plane + (int64_t)y * P.nx + x;
+#pragma unroll
+    for (int c = 0; c < NP; ++c) P.mm[c * P.npts + g] = io[c * NPB + q];
+  }
+}
+
 // Fold this thread's max |dX/dt| into the block and store the block's max
 // in its own slot of P.partial (a plain store: no same-address atomics, no
 // fences); k_dt_finish reduces the slots and runs the dt controller.
@@ -1095,15 +1330,34 @@ RateVariant make_variant() {
   return v;
 }
 
-template <int DIM, int KMINB>
+// The split form's mu/M kernel: k_chem64 (K = 1) or its shared-gather form
+// k_chem64i with K points per work item.
+template <int DIM, int KMINB, int K = 1>
 void launch_chem(bool vec, cudaStream_t s, const RateParams &P) {
-  const dim3 b(32, 8), g((unsigned)((P.nx + 31) / 32), (unsigned)((P.ny + 7) / 8),
-                         (unsigned)P.nz);
-  if (vec) launch_pdl(k_chem64<DIM, true, KMINB>, g, b, 0, s, P);
-  else launch_pdl(k_chem64<DIM, false, KMINB>, g, b, 0, s, P);
+  if constexpr (K == 1) {
+    const dim3 b(32, 8), g((unsigned)((P.nx + 31) / 32), (unsigned)((P.ny + 7) / 8),
+                           (unsigned)P.nz);
+    if (vec) launch_pdl(k_chem64<DIM, true, KMINB>, g, b, 0, s, P);
+    else launch_pdl(k_chem64<DIM, false, KMINB>, g, b, 0, s, P);
+  } else {
+    using G = Chem64Geom<DIM, K>;
+    const dim3 g((unsigned)((P.nx + G::BX - 1) / G::BX), (unsigned)((P.ny + G::BY - 1) / G::BY),
+                 (unsigned)((P.nz + G::BZ - 1) / G::BZ));
+    if (vec) launch_pdl(k_chem64i<DIM, true, K, KMINB>, g, dim3(kChem64Threads), G::smem, s, P);
+    else launch_pdl(k_chem64i<DIM, false, K, KMINB>, g, dim3(kChem64Threads), G::smem, s, P);
+  }
 }
 
-template <int TX, int TY, int MINB, int KMINB, bool PP = false>
+template <int DIM, int KMINB, int K>
+void chem_attrs() {
+  if constexpr (K > 1) {
+    const auto a = cudaFuncAttributeMaxDynamicSharedMemorySize;
+    cudaFuncSetAttribute(k_chem64i<DIM, true, K, KMINB>, a, (int)Chem64Geom<DIM, K>::smem);
+    cudaFuncSetAttribute(k_chem64i<DIM, false, K, KMINB>, a, (int)Chem64Geom<DIM, K>::smem);
+  }
+}
+
+template <int TX, int TY, int MINB, int KMINB, bool PP = false, int K = 1>
 RateVariant make_split_variant() {
   RateVariant v;
   v.tx = TX;
@@ -1120,18 +1374,21 @@ RateVariant make_split_variant() {
                          (int)tile2d_smem<TX, TY>());
     cudaFuncSetAttribute(k_rate_march3d<TX, TY, MINB, true, false, true, false, PP>, a,
                          (int)march3d_smem<TX, TY>());
+    chem_attrs<2, KMINB, K>();
+    chem_attrs<3, KMINB, K>();
   };
   v.launch2d = [](bool vec, dim3 g, dim3 b, size_t sm, cudaStream_t s, const RateParams &P) {
-    launch_chem<2, KMINB>(vec, s, P);
+    launch_chem<2, KMINB, K>(vec, s, P);
     launch_pdl(k_rate_tile2d<TX, TY, MINB, true, false, true>, g, b, sm, s, P);
   };
   v.launch3d = [](bool vec, dim3 g, dim3 b, size_t sm, cudaStream_t s, const RateParams &P,
                   int zc) {
-    launch_chem<3, KMINB>(vec, s, P);
+    launch_chem<3, KMINB, K>(vec, s, P);
     launch_pdl(k_rate_march3d<TX, TY, MINB, true, false, true, false, PP>, g, b, sm, s, P, zc);
   };
   v.kernels = [](bool vec, int dim) {
-    const std::string chem = kname("k_chem64", {dim, vec, KMINB}) + " + ";
+    const std::string chem = (K == 1 ? kname("k_chem64", {dim, vec, KMINB})
+                                     : kname("k_chem64i", {dim, vec, K, KMINB})) + " + ";
     if (dim == 2) return chem + kname("k_rate_tile2d", {TX, TY, MINB, 1, 0, 1, TX * TY, 0, 0});
     return chem + kname("k_rate_march3d", {TX, TY, MINB, 1, 0, 1, 0, PP});
   };
@@ -1151,7 +1408,9 @@ const std::vector<RateVariant> &rate_variants() {
       make_variant<32, 4, 4, false, 224, true>(), make_variant<32, 16, 1, false, 608, true>(),
       make_variant<32, 8, 2, false, 352, true, true>(), make_variant<32, 8, 2, true, 352, false, true>(),
       make_variant<32, 8, 3, false, 256, false, true>(), make_variant<64, 4, 2, true, 256, false, true>(),
-      make_split_variant<32, 8, 3, 3, true>(), make_split_variant<32, 4, 4, 3, true>()};
+      make_split_variant<32, 8, 3, 3, true>(), make_split_variant<32, 4, 4, 3, true>(),
+      make_split_variant<32, 8, 3, 2, false, 2>(), make_split_variant<32, 4, 4, 2, false, 2>(),
+      make_split_variant<32, 8, 3, 2, true, 2>(), make_split_variant<32, 4, 4, 2, true, 2>()};
   return v;
 }
 
