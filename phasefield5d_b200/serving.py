@@ -8,11 +8,13 @@ next block as soon as its own last one is done, so a small request is never
 held by a large one's block:
 
 * 1D and 2D solves share one batched stepper (``batch.BatchStepper``), one
-  unit;
-  whenever membership changes (a request admitted, finished, halted or
-  cancelled) the batch is rebuilt and every continuing solve resumes its
-  exact FP32 state (hi/lo pair, dt, time, step), so a request's trajectory
-  does not depend on when others come and go;
+  unit.  When a request joins, the batch is rebuilt and every continuing
+  solve resumes its exact FP32 state (hi/lo pair, dt, time, step), so a
+  request's trajectory does not depend on when others come and go.  When
+  requests only leave (finished, halted, cancelled), the batch keeps
+  running with the departed solves advancing unobserved, until the next
+  join or until they are half the batch -- a rebuild per departure would
+  stall the device units;
 * 3D solves each get their own FP32-compensated ``Stepper`` on their own
   stream (one unit each), so their work overlaps the batch on the device;
 * the device tables of each temperature are built once and shared by the
@@ -248,6 +250,7 @@ class GpuBackend:
         self.table_mu: dict[tuple, object] = {}   # mu reference each FP32 table subtracts
         self.pending: dict[object, object] = {}   # unit ("batch" or rid) -> event of its block
         self.fresh = False                        # batch rebuilt: report its states
+        self.live: set[int] = set()               # batch solves still active
 
     def _table(self, prob):
         """Resident device table of the request's temperature (built once):
@@ -306,6 +309,14 @@ class GpuBackend:
         want = [r.rid for r in active if self.shares_batch(r)]
         if want == self.batch_ids:
             return
+        if (self.batch is not None and all(rid in self.batch_ids for rid in want)
+                and 2 * len(want) >= len(self.batch_ids)):
+            # Only retirements: the batch keeps running.  A retired solve (its
+            # result already collected) advances unobserved until the next
+            # rebuild, which saves a rebuild per retirement; the live solves'
+            # trajectories do not depend on it.
+            self.live = set(want)
+            return
         resume = {}
         if self.batch is not None:
             with torch.cuda.stream(self.batch_stream):
@@ -317,6 +328,7 @@ class GpuBackend:
             self.batch = None
             self.pending.pop("batch", None)
         self.batch_ids = want
+        self.live = set(want)
         if want:
             with torch.cuda.stream(self.batch_stream):
                 self.batch = self.BatchStepper([self.reqs[i].problem for i in want],
@@ -336,10 +348,14 @@ class GpuBackend:
                 out.add(unit)
         return out
 
+    def _batch_block(self, blocks):
+        """Steps of the next batch block: the live solves move in lockstep."""
+        return max([blocks.get(rid, 0) for rid in self.batch_ids if rid in self.live] + [0])
+
     def launch(self, blocks):
         torch = self.torch
         if self.batch is not None and self.batch_ids and "batch" not in self.pending:
-            n = blocks.get(self.batch_ids[0], 0)
+            n = self._batch_block(blocks)
             if n > 0:
                 self.batch.advance(n)
                 ev = torch.cuda.Event()
@@ -377,7 +393,7 @@ class GpuBackend:
     # -- synchronous protocol (every block waits for all units) -------------
     def advance(self, blocks):
         if self.batch is not None and self.batch_ids:
-            n = blocks[self.batch_ids[0]]
+            n = self._batch_block(blocks)
             if n > 0:
                 self.batch.advance(n)
         for rid, st in self.steppers.items():
