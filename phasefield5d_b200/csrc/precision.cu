@@ -370,8 +370,13 @@ __global__ void k32_mass_final(const double *partial, int nparts, double *out) {
 //   5. the points set aside and those outside the linear region (nearest
 //      table row), one per thread;
 //   6. the block's outputs are stored coalesced.
-// Every value is formed by the same routines, in the same order, as in the
-// fused kernels (weights32 / corner_acc32, mu_offset32, dsum32).
+// Per point the block keeps three float4 in shared memory (point-major, so a
+// thread reads or writes a point's values with vector loads): the cell
+// fractions (or the deviation d outside the linear region), the mu offset,
+// and (cell, X_Fe); the outputs overwrite them as (mu), (M_Fe, M_1..3),
+// (M_4, X_Fe).  Every value is formed by the same routines, in the same
+// order, as in the fused kernels (weights32 / corner_acc32, mu_offset32,
+// dsum32).
 // ------------------------------------------------------------------------
 constexpr int kChemThreads = 256;
 
@@ -382,9 +387,9 @@ struct ChemGeom {
   static constexpr int BY = DIM == 1 ? 1 : (DIM == 2 ? 8 * K : 8);
   static constexpr int BZ = DIM == 3 ? K : 1;
   static constexpr int NITEMS = NPB / K + 256;                      // upper bound on items
-  // io[NPM][NPB] floats; items[NITEMS] u32; order, prank, left [NPB] u16;
-  // skey, pkey [NPB] u8; hist / cnt / ibase [256] int; wsum[9], nleft int
-  static constexpr size_t smem = (size_t)NPM * NPB * 4 + NITEMS * 4 + 3 * NPB * 2 + 2 * NPB +
+  // pio[3][NPB] float4 (point-major); items[NITEMS] u32; order, prank, left
+  // [NPB] u16; skey, pkey [NPB] u8; hist / cnt / ibase [256] int; wsum, nleft
+  static constexpr size_t smem = (size_t)3 * 16 * NPB + NITEMS * 4 + 3 * NPB * 2 + 2 * NPB +
                                  3 * 256 * 4 + 16 * 4;
 };
 
@@ -397,8 +402,8 @@ __global__ void __launch_bounds__(kChemThreads, MINB) k32_chem(Rate32 P) {
   using G = ChemGeom<DIM, K>;
   constexpr int NT = kChemThreads, NPB = G::NPB;
   extern __shared__ float4 sm4[];
-  float *io = reinterpret_cast<float *>(sm4);                          // [NPM][NPB]
-  unsigned *items = reinterpret_cast<unsigned *>(io + NPM * NPB);
+  float4 *pio = sm4;                                                   // 3 per point
+  unsigned *items = reinterpret_cast<unsigned *>(pio + 3 * NPB);
   unsigned short *order = reinterpret_cast<unsigned short *>(items + G::NITEMS);
   unsigned short *prank = order + NPB;
   unsigned short *left = prank + NPB;
@@ -467,13 +472,9 @@ __global__ void __launch_bounds__(kChemThreads, MINB) k32_chem(Rate32 P) {
 #pragma unroll
       for (int c = 0; c < S; ++c) tt[c] = d[c];
     }
-#pragma unroll
-    for (int c = 0; c < S; ++c) {
-      io[c * NPB + q] = tt[c];
-      io[(S + c) * NPB + q] = off[c];
-    }
-    io[8 * NPB + q] = __int_as_float(cell);
-    io[9 * NPB + q] = (float)(P.c_fe - sd);
+    pio[3 * q] = make_float4(tt[0], tt[1], tt[2], tt[3]);
+    pio[3 * q + 1] = make_float4(off[0], off[1], off[2], off[3]);
+    pio[3 * q + 2] = make_float4(__int_as_float(cell), (float)(P.c_fe - sd), 0.f, 0.f);
     pkey[q] = (unsigned char)key;
     prank[q] = (unsigned short)atomicAdd(&hist[key], 1);
   }
@@ -509,13 +510,12 @@ __global__ void __launch_bounds__(kChemThreads, MINB) k32_chem(Rate32 P) {
 #pragma unroll
     for (int j = 0; j < K; ++j) {
       q[j] = j < m ? (int)order[s + j] : 0;
-      const int cj = __float_as_int(io[8 * NPB + q[j]]);
+      const int cj = __float_as_int(pio[3 * q[j] + 2].x);
       if (j == 0) cell0 = cj;
       use[j] = j < m && cj == cell0;
       if (j < m && !use[j]) left[atomicAdd(nleft, 1)] = (unsigned short)q[j];
-      float tt[S];
-#pragma unroll
-      for (int c = 0; c < S; ++c) tt[c] = io[c * NPB + q[j]];
+      const float4 t4 = pio[3 * q[j]];
+      const float tt[S] = {t4.x, t4.y, t4.z, t4.w};
       W[j] = weights32(tt);
     }
     float acc[K][NP];
@@ -532,10 +532,11 @@ __global__ void __launch_bounds__(kChemThreads, MINB) k32_chem(Rate32 P) {
 #pragma unroll
     for (int j = 0; j < K; ++j) {
       if (!use[j]) continue;
-#pragma unroll
-      for (int c = 0; c < S; ++c) io[c * NPB + q[j]] = acc[j][c] + io[(S + c) * NPB + q[j]];
-#pragma unroll
-      for (int c = 0; c < NM; ++c) io[(S + c) * NPB + q[j]] = acc[j][S + c];
+      float4 *o = pio + 3 * q[j];
+      const float4 off = o[1];
+      o[0] = make_float4(acc[j][0] + off.x, acc[j][1] + off.y, acc[j][2] + off.z, acc[j][3] + off.w);
+      o[1] = make_float4(acc[j][4], acc[j][5], acc[j][6], acc[j][7]);
+      o[2].x = acc[j][8];
     }
   }
   __syncthreads();
@@ -544,16 +545,17 @@ __global__ void __launch_bounds__(kChemThreads, MINB) k32_chem(Rate32 P) {
   const int nnn = cnt[255], nl = nnn + *nleft;
   for (int l = tid; l < nl; l += NT) {
     const int q = l < nnn ? (int)order[lin_end + l] : (int)left[l - nnn];
-    const int cell = __float_as_int(io[8 * NPB + q]);
-    float a[S], v[NP];
-#pragma unroll
-    for (int c = 0; c < S; ++c) a[c] = io[c * NPB + q];
+    float4 *o = pio + 3 * q;
+    const int cell = __float_as_int(o[2].x);
+    const float4 a4 = o[0];
+    const float a[S] = {a4.x, a4.y, a4.z, a4.w};
+    float v[NP];
     if (cell < 0) nearest_row32(T, a, v, &flags);
     else interp_nodes32(g4 + (int64_t)cell * 3, (int)s0, (int)s1, (int)s2, (int)s3, a, v);
-#pragma unroll
-    for (int c = 0; c < S; ++c) io[c * NPB + q] = v[c] + io[(S + c) * NPB + q];
-#pragma unroll
-    for (int c = 0; c < NM; ++c) io[(S + c) * NPB + q] = v[S + c];
+    const float4 off = o[1];
+    o[0] = make_float4(v[0] + off.x, v[1] + off.y, v[2] + off.z, v[3] + off.w);
+    o[1] = make_float4(v[4], v[5], v[6], v[7]);
+    o[2].x = v[8];
   }
   raise_rate_flags(P.st, flags);
   __syncthreads();
@@ -565,10 +567,10 @@ __global__ void __launch_bounds__(kChemThreads, MINB) k32_chem(Rate32 P) {
     const int x = blockIdx.x * G::BX + qx, y = blockIdx.y * G::BY + qy, z = blockIdx.z * G::BZ + qz;
     if (x >= P.nx || y >= P.ny || z >= P.nz) continue;
     const int64_t g = (int64_t)z * plane + (int64_t)y * P.nx + x;
-    const float *v = io + q;
-    P.mm_mu[g] = make_float4(v[0], v[NPB], v[2 * NPB], v[3 * NPB]);
-    P.mm_m[g] = make_float4(v[5 * NPB], v[6 * NPB], v[7 * NPB], v[8 * NPB]);
-    P.mm_f[g] = make_float2(v[4 * NPB], v[9 * NPB]);
+    const float4 a = pio[3 * q], b = pio[3 * q + 1], c = pio[3 * q + 2];
+    P.mm_mu[g] = a;
+    P.mm_m[g] = make_float4(b.y, b.z, b.w, c.x);
+    P.mm_f[g] = make_float2(b.x, c.y);
   }
 }
 
@@ -842,7 +844,7 @@ const std::vector<Variant32> &variants32() {
       make_split_variant32<32, 8, 3, 2, 4, true>(), make_split_variant32<32, 8, 3, 4, 2, true>(),
       make_split_variant32<32, 8, 3, 2, 4, false>(), make_split_variant32<32, 8, 3, 4, 2, false>(),
       make_split_variant32<32, 16, 1, 4, 2, true>(), make_split_variant32<32, 4, 6, 4, 2, true>(),
-      make_split_variant32<64, 4, 3, 4, 2, true>(), make_split_variant32<32, 8, 3, 4, 3, true>()};
+      make_split_variant32<64, 4, 3, 4, 2, true>(), make_split_variant32<32, 8, 3, 2, 3, true>()};
   return v;
 }
 
