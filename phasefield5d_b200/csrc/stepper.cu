@@ -403,6 +403,10 @@ __global__ void __launch_bounds__(256, MINB) k_chem64(RateParams P) {
 //   5. the points set aside and the nearest-row points, one per thread;
 //   6. coalesced stores of the SoA rows.
 constexpr int kChem64Threads = 256;
+// Doubles per point of k_chem64i's shared staging, point-major (80 bytes, so
+// a point's values move as 16-byte vectors without bank conflicts between
+// neighbouring points): x (4), lap (4), s' -- overwritten by mu (4), M (5).
+constexpr int kIo64 = 10;
 
 template <int DIM, int K>
 struct Chem64Geom {
@@ -411,9 +415,10 @@ struct Chem64Geom {
   static constexpr int BY = DIM == 1 ? 1 : (DIM == 2 ? 8 * K : 8);
   static constexpr int BZ = DIM == 3 ? K : 1;
   static constexpr int NITEMS = NPB / K + 256;
-  // io[9][NPB] doubles, cell[NPB] int, items[NITEMS] u32, order/prank/left
-  // [NPB] u16, skey/pkey [NPB] u8, hist/cnt/ibase [256] int, wsum + nleft
-  static constexpr size_t smem = (size_t)9 * NPB * 8 + NPB * 4 + NITEMS * 4 + 3 * NPB * 2 +
+  // io[kIo64 * NPB] doubles (point-major), cell[NPB] int, items[NITEMS] u32,
+  // order/prank/left [NPB] u16, skey/pkey [NPB] u8, hist/cnt/ibase [256] int,
+  // wsum + nleft
+  static constexpr size_t smem = (size_t)10 * NPB * 8 + NPB * 4 + NITEMS * 4 + 3 * NPB * 2 +
                                  2 * NPB + 3 * 256 * 4 + 16 * 4;
 };
 
@@ -422,8 +427,8 @@ __global__ void __launch_bounds__(kChem64Threads, MINB) k_chem64i(RateParams P) 
   using G = Chem64Geom<DIM, K>;
   constexpr int NT = kChem64Threads, NPB = G::NPB;
   extern __shared__ double2 smd[];
-  double *io = reinterpret_cast<double *>(smd);                        // [9][NPB]
-  int *cellv = reinterpret_cast<int *>(io + 9 * NPB);
+  double *io = reinterpret_cast<double *>(smd);             // kIo64 per point, point-major
+  int *cellv = reinterpret_cast<int *>(io + kIo64 * NPB);
   unsigned *items = reinterpret_cast<unsigned *>(cellv + NPB);
   unsigned short *order = reinterpret_cast<unsigned short *>(items + G::NITEMS);
   unsigned short *prank = order + NPB;
@@ -482,10 +487,10 @@ __global__ void __launch_bounds__(kChem64Threads, MINB) k_chem64i(RateParams P) 
         lap[c] = ((n0[c] + n1[c]) - 2.0 * xc[c]) * P.inv_dx2;
       else
         lap[c] = (((lap[c] + n0[c]) + n1[c]) - (DIM == 3 ? 6.0 : 4.0) * xc[c]) * P.inv_dx2;
-      io[c * NPB + q] = xc[c];
-      io[(S + c) * NPB + q] = lap[c];
+      io[q * kIo64 + c] = xc[c];
+      io[q * kIo64 + S + c] = lap[c];
     }
-    io[8 * NPB + q] = P.sp ? __ldg(P.sp + g) : 0.0;
+    io[q * kIo64 + 8] = P.sp ? __ldg(P.sp + g) : 0.0;
     int ii[S];
     double tt[S];
     int cell = -1, key = 255;
@@ -536,7 +541,7 @@ __global__ void __launch_bounds__(kChem64Threads, MINB) k_chem64i(RateParams P) 
 #pragma unroll
       for (int a = 0; a < S; ++a) {
         int i;
-        axis_coord(io[a * NPB + q[j]] * T.inv_step, T.n, i, tt[j][a]);
+        axis_coord(io[q[j] * kIo64 + a] * T.inv_step, T.n, i, tt[j][a]);
         qq[j][a] = 1.0 - tt[j][a];
       }
     }
@@ -575,13 +580,13 @@ __global__ void __launch_bounds__(kChem64Threads, MINB) k_chem64i(RateParams P) 
       if (!use[j]) continue;
 #pragma unroll
       for (int c = 0; c < S; ++c) {
-        const double lk = io[(S + c) * NPB + q[j]] * P.kappa.v[c];
+        const double lk = io[q[j] * kIo64 + S + c] * P.kappa.v[c];
         double mu = acc[j][c] - lk;
-        if (P.sp) mu = mu + io[8 * NPB + q[j]] * P.lvec.v[c];
-        io[c * NPB + q[j]] = mu;
+        if (P.sp) mu = mu + io[q[j] * kIo64 + 8] * P.lvec.v[c];
+        io[q[j] * kIo64 + c] = mu;
       }
 #pragma unroll
-      for (int c = 0; c < NM; ++c) io[(S + c) * NPB + q[j]] = acc[j][S + c];
+      for (int c = 0; c < NM; ++c) io[q[j] * kIo64 + S + c] = acc[j][S + c];
     }
   }
   __syncthreads();
@@ -592,18 +597,18 @@ __global__ void __launch_bounds__(kChem64Threads, MINB) k_chem64i(RateParams P) 
     const int q = l < nnn ? (int)order[lin_end + l] : (int)left[l - nnn];
     double xq[S], v[NP];
 #pragma unroll
-    for (int c = 0; c < S; ++c) xq[c] = io[c * NPB + q];
+    for (int c = 0; c < S; ++c) xq[c] = io[q * kIo64 + c];
     const int o[S] = {0, 0, 0, 0};
     interp_win64<VEC>(T, xq, nullptr, o, v, &flags);
 #pragma unroll
     for (int c = 0; c < S; ++c) {
-      const double lk = io[(S + c) * NPB + q] * P.kappa.v[c];
+      const double lk = io[q * kIo64 + S + c] * P.kappa.v[c];
       double mu = v[c] - lk;
-      if (P.sp) mu = mu + io[8 * NPB + q] * P.lvec.v[c];
-      io[c * NPB + q] = mu;
+      if (P.sp) mu = mu + io[q * kIo64 + 8] * P.lvec.v[c];
+      io[q * kIo64 + c] = mu;
     }
 #pragma unroll
-    for (int c = 0; c < NM; ++c) io[(S + c) * NPB + q] = v[S + c];
+    for (int c = 0; c < NM; ++c) io[q * kIo64 + S + c] = v[S + c];
   }
   raise_rate_flags(P.st, flags);
   __syncthreads();
@@ -616,7 +621,7 @@ __global__ void __launch_bounds__(kChem64Threads, MINB) k_chem64i(RateParams P) 
     if (x >= P.nx || y >= P.ny || z >= P.nz) continue;
     const int64_t g = (int64_t)z * plane + (int64_t)y * P.nx + x;
 #pragma unroll
-    for (int c = 0; c < NP; ++c) P.mm[c * P.npts + g] = io[c * NPB + q];
+    for (int c = 0; c < NP; ++c) P.mm[c * P.npts + g] = io[q * kIo64 + c];
   }
 }
 
