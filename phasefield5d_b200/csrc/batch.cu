@@ -132,7 +132,7 @@ __device__ __forceinline__ float tile1d32_body(const BSolve &B, const Rate32 &P,
   return vmax;
 }
 
-template <int TX, int TY, bool SORT = false>
+template <int TX, int TY, int SORT = 0>
 struct BatchSmem {
   static constexpr int NT = TX * TY;
   static constexpr size_t s1d = (S * (NT + 4) + NPM * (NT + 2) + S * (NT + 1)) * sizeof(float);
@@ -142,7 +142,7 @@ struct BatchSmem {
   static constexpr size_t rate = head + (s2d > s1d ? s2d : s1d);
 };
 
-template <int TX, int TY, int MINB, bool WIN, bool SORT = false, bool PP = false>
+template <int TX, int TY, int MINB, bool WIN, int SORT = 0, bool PP = false>
 __global__ void __launch_bounds__(TX * TY, MINB)
     kb_rate(const BSolve *__restrict__ solves, int nsolves, int tile_begin, int tile_end,
             double *tile_max) {
@@ -384,7 +384,7 @@ struct BatchVariant {
   int (*occupancy)();
 };
 
-template <int TX, int TY, int MINB, bool WIN, bool SORT = false, bool PP = false>
+template <int TX, int TY, int MINB, bool WIN, int SORT = 0, bool PP = false>
 BatchVariant make_bvariant() {
   using SM = BatchSmem<TX, TY, SORT>;
   BatchVariant v;
@@ -418,7 +418,9 @@ const std::vector<BatchVariant> &batch_variants() {
       make_bvariant<32, 4, 4, true>(), make_bvariant<64, 4, 2, true>(),
       make_bvariant<32, 8, 2, false, true>(), make_bvariant<32, 8, 3, false, true>(),
       make_bvariant<32, 16, 2, false, true>(), make_bvariant<32, 8, 3, false, false, true>(),
-      make_bvariant<32, 16, 2, false, false, true>(), make_bvariant<32, 8, 3, false, true, true>()};
+      make_bvariant<32, 16, 2, false, false, true>(), make_bvariant<32, 8, 3, false, true, true>(),
+      make_bvariant<32, 16, 2, false, 2, true>(), make_bvariant<32, 8, 3, false, 2, true>(),
+      make_bvariant<32, 16, 2, false, 2, false>()};
   return v;
 }
 

@@ -220,6 +220,58 @@ __device__ __forceinline__ void chem32(const Rate32 &P, const float d[S], const 
   out[NP] = (float)(P.c_fe - sd);
 }
 
+// chem32 of two points at once: when both lie in the linear region of one
+// table cell, each corner node is loaded once and accumulated into both
+// (the same terms in the same order as chem32, so the same bits); otherwise
+// each point takes chem32's own path.  hasB = false evaluates A alone.
+__device__ __forceinline__ void chem32_pair(const Rate32 &P, const float dA[S], const float lapA[S],
+                                            float spA, const float dB[S], const float lapB[S],
+                                            float spB, bool hasB, float outA[NPM],
+                                            float outB[NPM], unsigned *flags) {
+  const Table32 &T = P.T;
+  const double sdA = dsum32(dA), sdB = dsum32(dB);
+  int iA[S], iB[S];
+  float tA[S], tB[S];
+  const bool linA = cell32(T, dA, sdA, iA, tA);
+  const bool linB = hasB && cell32(T, dB, sdB, iB, tB);
+  const bool share = linA && linB && iA[0] == iB[0] && iA[1] == iB[1] && iA[2] == iB[2] &&
+                     iA[3] == iB[3];
+  float vA[NP], vB[NP];
+  if (share) {
+    const int s3 = 3, s2 = T.n * s3, s1 = T.n * s2;
+    const int64_t s0 = (int64_t)T.n * s1;
+    const float4 *base = reinterpret_cast<const float4 *>(T.grid) + iA[0] * s0 +
+                         (int64_t)iA[1] * s1 + (int64_t)iA[2] * s2 + iA[3] * s3;
+    const Weights32 WA = weights32(tA), WB = weights32(tB);
+#pragma unroll
+    for (int c = 0; c < 16; ++c) {
+      const int b0 = (c >> 3) & 1, b1 = (c >> 2) & 1, b2 = (c >> 1) & 1, b3 = c & 1;
+      const float4 *node = base + b0 * s0 + b1 * s1 + b2 * s2 + b3 * s3;
+      const float4 a = __ldg(node), b = __ldg(node + 1), e = __ldg(node + 2);
+      corner_acc32(c, WA.wa[c >> 2] * WA.wb[c & 3], a, b, e, vA);
+      corner_acc32(c, WB.wa[c >> 2] * WB.wb[c & 3], a, b, e, vB);
+    }
+  } else {
+    interp32(P, dA, sdA, nullptr, nullptr, vA, flags);
+    if (hasB) interp32(P, dB, sdB, nullptr, nullptr, vB, flags);
+  }
+  float off[S];
+  mu_offset32(P, lapA, spA, off);
+#pragma unroll
+  for (int c = 0; c < S; ++c) outA[c] = vA[c] + off[c];
+#pragma unroll
+  for (int c = 0; c < NM; ++c) outA[S + c] = vA[S + c];
+  outA[NP] = (float)(P.c_fe - sdA);
+  if (hasB) {
+    mu_offset32(P, lapB, spB, off);
+#pragma unroll
+    for (int c = 0; c < S; ++c) outB[c] = vB[c] + off[c];
+#pragma unroll
+    for (int c = 0; c < NM; ++c) outB[S + c] = vB[S + c];
+    outB[NP] = (float)(P.c_fe - sdB);
+  }
+}
+
 // Face flux (phasefield5d/solver/fluxes.py:128-160) in FP32 between a lower
 // position c and an upper position n along one axis, from each position's
 // D = X - X0, mu, M_1..4 and (M_Fe, X_Fe):
@@ -406,8 +458,10 @@ struct SortBytes32 {
 // y-neighbours sit in the same plane).  Stages the table window first.
 // SORT: positions evaluated in table-cell order (cell_hash counting sort),
 // so the lanes of a warp gather the same table nodes; only the thread that
-// evaluates a position changes.
-template <int TX, int TY, int DIM, bool WIN, bool SORT = false>
+// evaluates a position changes.  SORT = 2: a thread evaluates two
+// consecutive positions of that order with chem32_pair, which shares the
+// corner loads when they lie in one table cell (no table window).
+template <int TX, int TY, int DIM, bool WIN, int SORT = 0>
 __device__ __forceinline__ void mu_plane32(const Rate32 &P, const float *Xm, const float *Xc,
                                            const float *Xp, float *dst, int64_t zoff,
                                            const int *wx, const int *wy, bool interior_only,
@@ -455,6 +509,41 @@ __device__ __forceinline__ void mu_plane32(const Rate32 &P, const float *Xm, con
     __syncthreads();
   }
   // 3. interpolation + Laplacian + mu assembly.
+  auto inputs = [&](int pos, float d[S], float lap[S], float &spv) {
+    const int my = pos / G::MX, mx = pos - my * G::MX;
+    const int px = (my + 1) * G::HX + (mx + 1);
+#pragma unroll
+    for (int c = 0; c < S; ++c) {
+      const float *q = Xc + c * G::PX;
+      d[c] = q[px];
+      if (DIM == 3) {
+        const float nb[6] = {Xp[c * G::PX + px], Xm[c * G::PX + px], q[px + G::HX], q[px - G::HX],
+                             q[px + 1], q[px - 1]};
+        lap[c] = lap32<6>(nb, d[c], P.inv_dx2);
+      } else {
+        const float nb[4] = {q[px + G::HX], q[px - G::HX], q[px + 1], q[px - 1]};
+        lap[c] = lap32<4>(nb, d[c], P.inv_dx2);
+      }
+    }
+    spv = P.sp ? __ldg(P.sp + zoff + (int64_t)wy[my + 1] * P.nx + wx[mx + 1]) : 0.f;
+  };
+  if constexpr (SORT == 2) {
+    for (int w = 2 * tid; w < nwork; w += 2 * G::NT) {
+      const int posA = ss.order[w];
+      const bool hasB = w + 1 < nwork;
+      const int posB = hasB ? (int)ss.order[w + 1] : posA;
+      float dA[S], lapA[S], dB[S], lapB[S], spA, spB, vA[NPM], vB[NPM];
+      inputs(posA, dA, lapA, spA);
+      inputs(posB, dB, lapB, spB);
+      chem32_pair(P, dA, lapA, spA, dB, lapB, spB, hasB, vA, vB, flags);
+#pragma unroll
+      for (int r = 0; r < NPM; ++r) dst[r * G::PM + posA] = vA[r];
+      if (hasB) {
+#pragma unroll
+        for (int r = 0; r < NPM; ++r) dst[r * G::PM + posB] = vB[r];
+      }
+    }
+  } else {
   for (int w = tid; w < nwork; w += G::NT) {
     const int pos = SORT ? (int)ss.order[w] : w;
     const int my = pos / G::MX, mx = pos - my * G::MX;
@@ -479,6 +568,7 @@ __device__ __forceinline__ void mu_plane32(const Rate32 &P, const float *Xm, con
     chem32(P, d, lap, spv, use_win ? win : nullptr, o, v, flags);
 #pragma unroll
     for (int r = 0; r < NPM; ++r) dst[r * G::PM + pos] = v[r];
+  }
   }
 }
 
@@ -553,7 +643,7 @@ __device__ __forceinline__ void raise32(StepState32 *st, unsigned f) {
 // scratch, X (tile + 2 halo), mu/M (tile + 1 halo), x- and y-face fluxes,
 // window scratch/origin, halo index tables.
 // ------------------------------------------------------------------------
-template <int TX, int TY, bool SORT = false>
+template <int TX, int TY, int SORT = 0>
 struct Tile2dSmem32 {
   using G = PlaneGeom<TX, TY>;
   static constexpr size_t bytes = Smem32Tail<TX, TY>::bytes +
@@ -566,7 +656,7 @@ struct Tile2dSmem32 {
 
 // Evaluates tile (bx, by) of solve P and writes its dX/dt; returns this
 // thread's max |dX/dt|.  Ends with all threads past a barrier.
-template <int TX, int TY, bool WIN, bool SORT = false, bool SPLIT = false, bool PERPOINT = false>
+template <int TX, int TY, bool WIN, int SORT = 0, bool SPLIT = false, bool PERPOINT = false>
 __device__ __forceinline__ float tile2d32_body(const Rate32 &P, int bx, int by, float4 *sm4,
                                                unsigned *flags, int tid) {
   using G = PlaneGeom<TX, TY>;

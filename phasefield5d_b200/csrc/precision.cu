@@ -41,7 +41,7 @@ namespace pf5d {
 // Rate kernels (same tiling as the FP64 kernels)
 // ------------------------------------------------------------------------
 
-template <int TX, int TY, int MINB, bool WIN, bool SORT = false, bool SPLIT = false,
+template <int TX, int TY, int MINB, bool WIN, int SORT = 0, bool SPLIT = false,
           bool PERPOINT = false>
 __global__ void __launch_bounds__(TX * TY, MINB) k32_rate_tile2d(Rate32 P) {
   pdl_wait();
@@ -55,12 +55,12 @@ __global__ void __launch_bounds__(TX * TY, MINB) k32_rate_tile2d(Rate32 P) {
   finish_rate32(P, vmax, Tile2dSmem32<TX, TY, SORT>::red(sm4));
 }
 
-template <int TX, int TY, bool SORT = false>
+template <int TX, int TY, int SORT = 0>
 constexpr size_t tile2d32_smem() {
   return Tile2dSmem32<TX, TY, SORT>::bytes;
 }
 
-template <int TX, int TY, int MINB, bool WIN, bool SORT = false>
+template <int TX, int TY, int MINB, bool WIN, int SORT = 0>
 __global__ void __launch_bounds__(TX * TY, MINB) k32_rate_march3d(Rate32 P, int zc) {
   using G = PlaneGeom<TX, TY>;
   pdl_wait();
@@ -146,7 +146,7 @@ __global__ void __launch_bounds__(TX * TY, MINB) k32_rate_march3d(Rate32 P, int 
   finish_rate32(P, vmax, red);
 }
 
-template <int TX, int TY, bool SORT = false>
+template <int TX, int TY, int SORT = 0>
 constexpr size_t march3d32_smem() {
   using G = PlaneGeom<TX, TY>;
   return Smem32Tail<TX, TY>::bytes +
@@ -767,7 +767,7 @@ struct Variant32 {
   std::string (*kernels)(int dim);     // the kernel instances of a 2D/3D rate stage
 };
 
-template <int TX, int TY, int MINB, bool WIN = true, bool SORT = false, bool PP = false>
+template <int TX, int TY, int MINB, bool WIN = true, int SORT = 0, bool PP = false>
 Variant32 make_variant32() {
   Variant32 v;
   v.tx = TX;
@@ -840,6 +840,8 @@ const std::vector<Variant32> &variants32() {
       make_variant32<32, 8, 2, true, true>(), make_variant32<32, 8, 3, false, true>(),
       make_variant32<32, 16, 2, false, true>(), make_variant32<32, 8, 2, false, true>(),
       make_variant32<32, 8, 3, false, true, true>(), make_variant32<32, 16, 2, false, true, true>(),
+      make_variant32<32, 8, 3, false, 2, true>(), make_variant32<32, 16, 2, false, 2, true>(),
+      make_variant32<32, 16, 2, false, 2, false>(),
       make_variant32<32, 8, 3, false, false, true>(), make_variant32<32, 16, 2, false, false, true>(),
       make_split_variant32<32, 8, 3, 2, 4, true>(), make_split_variant32<32, 8, 3, 4, 2, true>(),
       make_split_variant32<32, 8, 3, 2, 4, false>(), make_split_variant32<32, 8, 3, 4, 2, false>(),

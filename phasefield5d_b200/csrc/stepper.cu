@@ -161,6 +161,54 @@ __device__ __forceinline__ void interp_win64(const Table &T, const double x[S], 
     out[p] = r.node < 0 ? __longlong_as_double(0x7ff8000000000000LL) : __ldg(row + p);
 }
 
+// Table values at two points at once (VEC tables): when both lie in the
+// linear region of one table cell, each corner node is loaded once and its
+// terms accumulated into both -- the same weights and left-to-right sums as
+// interp_nodes64, so the same bits; otherwise each point takes interp_win64's
+// path without a window.  hasB = false evaluates A alone.
+__device__ __forceinline__ void interp_pair64(const Table &T, const double xA[S],
+                                              const double xB[S], bool hasB, double vA[NP],
+                                              double vB[NP], unsigned *flags) {
+  int iA[S], iB[S];
+  double tA[S], tB[S];
+  const bool linA = cell64(T, xA, iA, tA);
+  const bool linB = hasB && cell64(T, xB, iB, tB);
+  if (linA && linB && iA[0] == iB[0] && iA[1] == iB[1] && iA[2] == iB[2] && iA[3] == iB[3]) {
+    const int64_t s3 = kNodeV64, s2 = (int64_t)T.n * s3, s1 = (int64_t)T.n * s2,
+                  s0 = (int64_t)T.n * s1;
+    const double2 *base = reinterpret_cast<const double2 *>(T.grid) + iA[0] * s0 + iA[1] * s1 +
+                          iA[2] * s2 + iA[3] * s3;
+    const double qA0 = 1.0 - tA[0], qA1 = 1.0 - tA[1], qA2 = 1.0 - tA[2], qA3 = 1.0 - tA[3];
+    const double qB0 = 1.0 - tB[0], qB1 = 1.0 - tB[1], qB2 = 1.0 - tB[2], qB3 = 1.0 - tB[3];
+#pragma unroll
+    for (int c = 0; c < 16; ++c) {
+      const int b0 = (c >> 3) & 1, b1 = (c >> 2) & 1, b2 = (c >> 1) & 1, b3 = c & 1;
+      const double wA = (b0 ? tA[0] : qA0) * (b1 ? tA[1] : qA1) * (b2 ? tA[2] : qA2) *
+                        (b3 ? tA[3] : qA3);
+      const double wB = (b0 ? tB[0] : qB0) * (b1 ? tB[1] : qB1) * (b2 ? tB[2] : qB2) *
+                        (b3 ? tB[3] : qB3);
+      const double2 *node = base + b0 * s0 + b1 * s1 + b2 * s2 + b3 * s3;
+      double v[NP + 1];
+#pragma unroll
+      for (int k = 0; k < kNodeV64; ++k) {
+        const double2 a = __ldg(node + k);
+        v[2 * k] = a.x;
+        v[2 * k + 1] = a.y;
+      }
+#pragma unroll
+      for (int p = 0; p < NP; ++p) {
+        const double ta = wA * v[p], tb = wB * v[p];
+        vA[p] = (c == 0) ? ta : vA[p] + ta;
+        vB[p] = (c == 0) ? tb : vB[p] + tb;
+      }
+    }
+    return;
+  }
+  const int o[S] = {0, 0, 0, 0};
+  interp_win64<true>(T, xA, nullptr, o, vA, flags);
+  if (hasB) interp_win64<true>(T, xB, nullptr, o, vB, flags);
+}
+
 // Shared-memory scratch of a per-tile cell sort: hist[256], wsum[NT/32+1],
 // order/rank/key per mu/M position.
 struct SortScratch {
@@ -179,7 +227,7 @@ constexpr unsigned short kNoRank = 0xFFFFu;
 // the positions are first put in table-cell order (cell_hash counting
 // sort) so the lanes of a warp gather the same table nodes; which thread
 // evaluates a position changes, the values do not.
-template <int TX, int TY, int DIM, bool VEC, bool WIN, int NTH = TX * TY, bool SORT = false>
+template <int TX, int TY, int DIM, bool VEC, bool WIN, int NTH = TX * TY, int SORT = 0>
 __device__ __forceinline__ void mu_plane64(const RateParams &P, const double *Xm, const double *Xc,
                                            const double *Xp, double *dst, int64_t zoff,
                                            const int *wx, const int *wy, bool interior_only,
@@ -230,6 +278,47 @@ __device__ __forceinline__ void mu_plane64(const RateParams &P, const double *Xm
       if (ss.rank[pos] != kNoRank) ss.order[ss.hist[ss.key[pos]] + ss.rank[pos]] = (unsigned short)pos;
     __syncthreads();
   }
+  if constexpr (SORT == 2 && VEC) {
+    // two consecutive positions of the cell order per thread, corner loads
+    // shared when they lie in one table cell (interp_pair64)
+    auto inputs = [&](int pos, double x[S], double lap[S], double &spv) {
+      const int my = pos / G::MX, mx = pos - my * G::MX;
+      const int px = (my + 1) * G::HX + (mx + 1);
+#pragma unroll
+      for (int c = 0; c < S; ++c) {
+        const double *q = Xc + c * G::PX;
+        x[c] = q[px];
+        if (DIM == 3)
+          lap[c] = (Xp[c * G::PX + px] + Xm[c * G::PX + px] + q[px + G::HX] + q[px - G::HX] +
+                    q[px + 1] + q[px - 1] - 6.0 * x[c]) * P.inv_dx2;
+        else
+          lap[c] = (q[px + G::HX] + q[px - G::HX] + q[px + 1] + q[px - 1] - 4.0 * x[c]) * P.inv_dx2;
+      }
+      spv = P.sp ? __ldg(P.sp + zoff + (int64_t)wy[my + 1] * P.nx + wx[mx + 1]) : 0.0;
+    };
+    auto store = [&](int pos, const double v[NP], const double lap[S], double spv) {
+#pragma unroll
+      for (int c = 0; c < S; ++c) {
+        const double lk = lap[c] * P.kappa.v[c];
+        double m = v[c] - lk;
+        if (P.sp) m = m + spv * P.lvec.v[c];
+        dst[c * G::PM + pos] = m;
+      }
+#pragma unroll
+      for (int c = 0; c < NM; ++c) dst[(S + c) * G::PM + pos] = v[S + c];
+    };
+    for (int w = 2 * tid; w < nwork; w += 2 * NTH) {
+      const int posA = ss.order[w];
+      const bool hasB = w + 1 < nwork;
+      const int posB = hasB ? (int)ss.order[w + 1] : posA;
+      double xA[S], lapA[S], xB[S], lapB[S], spA, spB, vA[NP], vB[NP];
+      inputs(posA, xA, lapA, spA);
+      inputs(posB, xB, lapB, spB);
+      interp_pair64(P.T, xA, xB, hasB, vA, vB, flags);
+      store(posA, vA, lapA, spA);
+      if (hasB) store(posB, vB, lapB, spB);
+    }
+  } else {
   for (int w = tid; w < nwork; w += NTH) {
     const int pos = SORT ? (int)ss.order[w] : w;
     const int my = pos / G::MX, mx = pos - my * G::MX;
@@ -258,6 +347,7 @@ __device__ __forceinline__ void mu_plane64(const RateParams &P, const double *Xm
     }
 #pragma unroll
     for (int c = 0; c < NM; ++c) dst[(S + c) * G::PM + pos] = v[S + c];
+  }
   }
 }
 
@@ -742,7 +832,7 @@ __device__ __forceinline__ void load_plane(const double *__restrict__ X, int64_t
 // NTH >= the mu/M position count every position takes one pass).  SORT:
 // mu/M positions evaluated in table-cell order.
 template <int TX, int TY, int MINB, bool VEC, bool WIN, bool SPLIT = false, int NTH = TX * TY,
-          bool SORT = false, bool PERPOINT = false>
+          int SORT = 0, bool PERPOINT = false>
 __global__ void __launch_bounds__(NTH, MINB) k_rate_tile2d(RateParams P) {
   using G = PlaneGeom<TX, TY, NTH>;
   static_assert(NTH >= TX * TY && NTH % 32 == 0, "one thread per tile point at least");
@@ -830,7 +920,7 @@ __global__ void __launch_bounds__(NTH, MINB) k_rate_tile2d(RateParams P) {
   finish_rate(P, vmax, red);
 }
 
-template <int TX, int TY, int NTH = TX * TY, bool SORT = false>
+template <int TX, int TY, int NTH = TX * TY, int SORT = 0>
 constexpr size_t tile2d_smem() {
   using G = PlaneGeom<TX, TY, NTH>;
   static_assert(S * (G::NFX + G::NFY) * sizeof(double) >= kWinNodes64 * kNodeV64 * sizeof(double2),
@@ -881,7 +971,7 @@ struct March64Geom {
   static constexpr int NFMAX = G::NFX > G::NFY ? G::NFX : G::NFY;
 };
 
-template <int TX, int TY, int MINB, bool VEC, bool WIN, bool SPLIT = false, bool SORT = false,
+template <int TX, int TY, int MINB, bool VEC, bool WIN, bool SPLIT = false, int SORT = 0,
           bool PERPOINT = false>
 __global__ void __launch_bounds__(TX * TY, MINB) k_rate_march3d(RateParams P, int zc) {
   using G = PlaneGeom<TX, TY>;
@@ -1034,7 +1124,7 @@ __global__ void __launch_bounds__(TX * TY, MINB) k_rate_march3d(RateParams P, in
   finish_rate(P, vmax, red);
 }
 
-template <int TX, int TY, bool SORT = false>
+template <int TX, int TY, int SORT = 0>
 constexpr size_t march3d_smem() {
   using G = PlaneGeom<TX, TY>;
   const size_t sort = SORT ? (256 + G::NT / 32 + 1) * sizeof(int) + G::PM * (2 * 2 + 1) : 0;
@@ -1296,7 +1386,7 @@ struct RateVariant {
 
 // NTH shapes the 2D kernel only (the 3D marching kernel has one thread per
 // tile point); SORT applies to both.
-template <int TX, int TY, int MINB, bool WIN = true, int NTH = TX * TY, bool SORT = false,
+template <int TX, int TY, int MINB, bool WIN = true, int NTH = TX * TY, int SORT = 0,
           bool PP = false>
 RateVariant make_variant() {
   RateVariant v;
@@ -1412,6 +1502,8 @@ const std::vector<RateVariant> &rate_variants() {
       make_variant<32, 8, 2, true, 352, false>(), make_variant<32, 4, 4, true, 224, true>(),
       make_variant<32, 4, 4, false, 224, true>(), make_variant<32, 16, 1, false, 608, true>(),
       make_variant<32, 8, 2, false, 352, true, true>(), make_variant<32, 8, 2, true, 352, false, true>(),
+      make_variant<32, 8, 2, false, 256, 2, true>(), make_variant<32, 8, 2, false, 256, 2, false>(),
+      make_variant<32, 4, 4, false, 128, 2, true>(),
       make_variant<32, 8, 3, false, 256, false, true>(), make_variant<64, 4, 2, true, 256, false, true>(),
       make_split_variant<32, 8, 3, 3, true>(), make_split_variant<32, 4, 4, 3, true>(),
       make_split_variant<32, 8, 3, 2, false, 2>(), make_split_variant<32, 4, 4, 2, false, 2>(),
