@@ -26,7 +26,6 @@
 
 #include <cufft.h>
 
-#include "pf5d_fft.h"
 #include "pf5d_fp32c.cuh"
 #include "pf5d_host.h"
 
@@ -449,8 +448,6 @@ struct ShapeGroup {
   int64_t s_off, k_off, nk;
   cufftHandle fwd = 0, inv = 0;
   float *bk = nullptr;
-  bool fused = false;        // the inverse plan applies B(k)/N (load callback)
-  void *cb_info = nullptr;   // device argument block of that callback
 };
 
 }  // namespace pf5d
@@ -560,11 +557,9 @@ pf5d_status enqueue_lane_step(pf5d_batch *h, int L, cudaStream_t s, cudaEvent_t 
       set_error("batch cuFFT R2C failed");
       return PF5D_ERR_CUFFT;
     }
-    if (!g.fused) {
-      const int64_t total = g.nk * g.count;
-      kb_bmul<<<grid_for(total, 256), 256, 0, gs>>>(h->k + g.k_off, g.bk, g.nk, total);
-      PF5D_LAUNCHED();
-    }
+    const int64_t total = g.nk * g.count;
+    kb_bmul<<<grid_for(total, 256), 256, 0, gs>>>(h->k + g.k_off, g.bk, g.nk, total);
+    PF5D_LAUNCHED();
     if (cufftSetStream(g.inv, gs) != CUFFT_SUCCESS ||
         cufftExecC2R(g.inv, h->k + g.k_off, h->s + g.s_off) != CUFFT_SUCCESS) {
       set_error("batch cuFFT C2R failed");
@@ -721,6 +716,14 @@ pf5d_status pf5d_batch_create(const pf5d_batch_solve *solves, int32_t nsolves,
     long long n2[2] = {g.ny, g.nx};
     size_t ws = 0;
     const long long idist = (long long)g.ny * g.nx, odist = g.nk;
+    if (cufftCreate(&g.fwd) != CUFFT_SUCCESS || cufftCreate(&g.inv) != CUFFT_SUCCESS ||
+        cufftMakePlanMany64(g.fwd, 2, n2, nullptr, 1, idist, nullptr, 1, odist, CUFFT_R2C, g.count,
+                            &ws) != CUFFT_SUCCESS ||
+        cufftMakePlanMany64(g.inv, 2, n2, nullptr, 1, odist, nullptr, 1, idist, CUFFT_C2R, g.count,
+                            &ws) != CUFFT_SUCCESS) {
+      set_error("cuFFT plan creation failed for %dx%d", g.ny, g.nx);
+      return fail(PF5D_ERR_CUFFT);
+    }
     // B(k) of the first solve of the group (the same for all: it depends only
     // on the direction of k), scaled by 1/N.
     const pf5d_batch_solve *first = nullptr;
@@ -735,14 +738,6 @@ pf5d_status pf5d_batch_create(const pf5d_batch_solve *solves, int32_t nsolves,
         cudaMemcpy(g.bk, b.data(), g.nk * sizeof(float), cudaMemcpyHostToDevice) != cudaSuccess) {
       set_error("device allocation failed");
       return fail(PF5D_ERR_CUDA);
-    }
-    if (cufftCreate(&g.fwd) != CUFFT_SUCCESS ||
-        cufftMakePlanMany64(g.fwd, 2, n2, nullptr, 1, idist, nullptr, 1, odist, CUFFT_R2C, g.count,
-                            &ws) != CUFFT_SUCCESS ||
-        make_inverse_plan(&g.inv, 2, n2, odist, idist, CUFFT_C2R, g.count, g.bk, g.nk,
-                          &g.cb_info, &g.fused) != CUFFT_SUCCESS) {
-      set_error("cuFFT plan creation failed for %dx%d", g.ny, g.nx);
-      return fail(PF5D_ERR_CUFFT);
     }
   }
   // --- lanes: shape groups largest first to the lighter lane, then the
@@ -1042,7 +1037,6 @@ pf5d_status pf5d_batch_destroy(pf5d_batch *h) {
   for (auto &g : h->groups) {
     if (g.fwd) cufftDestroy(g.fwd);
     if (g.inv) cufftDestroy(g.inv);
-    if (g.cb_info) cudaFree(g.cb_info);
     cudaFree(g.bk);
   }
   cudaFree(h->hi);

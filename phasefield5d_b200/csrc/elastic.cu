@@ -21,28 +21,22 @@ namespace pf5d {
     }                                                                              \
   } while (0)
 
-void fft_sizes(int dim, const int64_t *shape, int64_t *npts, int64_t *nk) {
-  int64_t n = 1;
-  for (int d = 0; d < dim; ++d) n *= shape[d];
-  *npts = n;
-  *nk = n / shape[dim - 1] * (shape[dim - 1] / 2 + 1);
-}
-
-pf5d_status fft_create(int dim, const int64_t *shape, FFTPair *p, const double *bk_dev) {
+pf5d_status fft_create(int dim, const int64_t *shape, FFTPair *p) {
   PF5D_REQUIRE(dim >= 1 && dim <= 3, PF5D_ERR_DIM,
                "make_elastic_updater not implemented for spatial_dim=%d", dim);
   long long n[3];
+  int64_t npts = 1;
   for (int d = 0; d < dim; ++d) {
     PF5D_REQUIRE(shape[d] > 0, PF5D_ERR_ARG, "bad shape");
     n[d] = shape[d];
+    npts *= shape[d];
   }
-  int64_t npts, nk;
-  fft_sizes(dim, shape, &npts, &nk);
+  const int64_t nk = npts / shape[dim - 1] * (shape[dim - 1] / 2 + 1);
   size_t ws = 0;
   PF5D_CUFFT(cufftCreate(&p->fwd));
   PF5D_CUFFT(cufftMakePlanMany64(p->fwd, dim, n, nullptr, 1, 0, nullptr, 1, 0, CUFFT_D2Z, 1, &ws));
-  PF5D_CUFFT(make_inverse_plan(&p->inv, dim, n, 0, 0, CUFFT_Z2D, 1, bk_dev, nk, &p->cb_info,
-                               &p->fused));
+  PF5D_CUFFT(cufftCreate(&p->inv));
+  PF5D_CUFFT(cufftMakePlanMany64(p->inv, dim, n, nullptr, 1, 0, nullptr, 1, 0, CUFFT_Z2D, 1, &ws));
   p->npts = npts;
   p->nk = nk;
   p->ready = true;
@@ -54,8 +48,6 @@ void fft_destroy(FFTPair *p) {
     cufftDestroy(p->fwd);
     cufftDestroy(p->inv);
   }
-  if (p->cb_info) cudaFree(p->cb_info);
-  p->cb_info = nullptr;
   p->ready = false;
 }
 

@@ -17,24 +17,9 @@ struct FFTPair {
   cufftHandle fwd = 0, inv = 0;
   int64_t npts = 0, nk = 0;
   bool ready = false;
-  bool fused = false;        // the inverse plan applies B(k)/N itself (load callback)
-  void *cb_info = nullptr;   // device argument block of that callback
 };
 
-// Points and half-spectrum length of a real field of `shape`.
-void fft_sizes(int dim, const int64_t *shape, int64_t *npts, int64_t *nk);
-// bk_dev (optional, device B(k)/N on the half-spectrum): fuse the multiply
-// into the inverse plan when cuFFT can link the callback (p->fused).
-pf5d_status fft_create(int dim, const int64_t *shape, FFTPair *p, const double *bk_dev = nullptr);
-
-// An inverse (half-spectrum -> real) plan of `batch` transforms whose load
-// callback multiplies each element by bk_dev[offset mod nk] (fp32 or fp64 by
-// `type`); *fused reports whether the callback is in.  Without it (or when
-// bk_dev is null) the plan is a plain one.  *info_dev: device memory of the
-// callback's arguments, freed by the caller (null when not fused).
-cufftResult make_inverse_plan(cufftHandle *plan, int rank, long long *n, long long idist,
-                              long long odist, cufftType type, long long batch,
-                              const void *bk_dev, long long nk, void **info_dev, bool *fused);
+pf5d_status fft_create(int dim, const int64_t *shape, FFTPair *p);
 void fft_destroy(FFTPair *p);
 // s (real, npts) -> k (complex, nk); k -> s.  Both on `stream`.
 pf5d_status fft_forward(FFTPair *p, double *s, cufftDoubleComplex *k, cudaStream_t stream);

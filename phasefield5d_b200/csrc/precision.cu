@@ -31,7 +31,6 @@
 #include "pf5d_device.cuh"
 #include "pf5d_fp32c.h"
 #include "pf5d_fp32c.cuh"
-#include "pf5d_fft.h"
 #include "pf5d_host.h"
 #include "pf5d_tiles.cuh"
 #include "pf5d_window.cuh"
@@ -860,8 +859,6 @@ struct Stepper32 {
   cufftComplex *k = nullptr;
   cufftHandle fwd = 0, inv = 0;
   bool plans = false;
-  bool fused = false;            // the inverse plan applies B(k)/N (load callback)
-  void *cb_info = nullptr;       // device argument block of that callback
   double *mass_ws = nullptr;
   double *partial = nullptr;     // rate kernel block maxima
   float *mm = nullptr;           // split-rate buffers: mu, M, (M_Fe, X_Fe) per point
@@ -951,10 +948,8 @@ static pf5d_status enqueue32(Stepper32 *h, cudaStream_t s) {
   if (h->d.elastic) {
     PF5D_CUFFT32(cufftSetStream(h->fwd, s));
     PF5D_CUFFT32(cufftExecR2C(h->fwd, h->s, h->k));
-    if (!h->fused) {
-      k32_bmul<<<grid_for(h->nk, 256), 256, 0, s>>>(h->k, h->bk, h->nk, &h->st->halt);
-      PF5D_LAUNCHED();
-    }
+    k32_bmul<<<grid_for(h->nk, 256), 256, 0, s>>>(h->k, h->bk, h->nk, &h->st->halt);
+    PF5D_LAUNCHED();
     PF5D_CUFFT32(cufftSetStream(h->inv, s));
     PF5D_CUFFT32(cufftExecC2R(h->inv, h->k, h->s));
   }
@@ -1026,6 +1021,16 @@ pf5d_status s32_create(const pf5d_stepper_desc *desc, const double *X_init, void
     long long n[3];
     for (int d = 0; d < desc->dim; ++d) n[d] = desc->shape[d];
     h->nk = npts / desc->shape[desc->dim - 1] * (desc->shape[desc->dim - 1] / 2 + 1);
+    size_t ws = 0;
+    if (cufftCreate(&h->fwd) != CUFFT_SUCCESS || cufftCreate(&h->inv) != CUFFT_SUCCESS ||
+        cufftMakePlanMany64(h->fwd, desc->dim, n, nullptr, 1, 0, nullptr, 1, 0, CUFFT_R2C, 1,
+                            &ws) != CUFFT_SUCCESS ||
+        cufftMakePlanMany64(h->inv, desc->dim, n, nullptr, 1, 0, nullptr, 1, 0, CUFFT_C2R, 1,
+                            &ws) != CUFFT_SUCCESS) {
+      set_error("cuFFT plan creation failed");
+      return fail(PF5D_ERR_CUFFT);
+    }
+    h->plans = true;
     std::vector<float> b(h->nk);
     const double inv_n = 1.0 / (double)npts;
     for (int64_t i = 0; i < h->nk; ++i) b[i] = (float)(desc->bk[i] * inv_n);
@@ -1036,16 +1041,6 @@ pf5d_status s32_create(const pf5d_stepper_desc *desc, const double *X_init, void
       set_error("device allocation failed");
       return fail(PF5D_ERR_CUDA);
     }
-    size_t ws = 0;
-    if (cufftCreate(&h->fwd) != CUFFT_SUCCESS ||
-        cufftMakePlanMany64(h->fwd, desc->dim, n, nullptr, 1, 0, nullptr, 1, 0, CUFFT_R2C, 1,
-                            &ws) != CUFFT_SUCCESS ||
-        make_inverse_plan(&h->inv, desc->dim, n, 0, 0, CUFFT_C2R, 1, h->bk, h->nk, &h->cb_info,
-                          &h->fused) != CUFFT_SUCCESS) {
-      set_error("cuFFT plan creation failed");
-      return fail(PF5D_ERR_CUFFT);
-    }
-    h->plans = true;
   }
   Rate32 &P = h->rp;
   if (desc->dim == 1) {
@@ -1192,10 +1187,8 @@ pf5d_status s32_step_save_inputs(Stepper32 *h, double *X_out, double *dX_out, do
   if (h->d.elastic) {
     PF5D_CUFFT32(cufftSetStream(h->fwd, s));
     PF5D_CUFFT32(cufftExecR2C(h->fwd, h->s, h->k));
-    if (!h->fused) {
-      k32_bmul<<<grid_for(h->nk, 256), 256, 0, s>>>(h->k, h->bk, h->nk, &h->st->halt);
-      PF5D_LAUNCHED();
-    }
+    k32_bmul<<<grid_for(h->nk, 256), 256, 0, s>>>(h->k, h->bk, h->nk, &h->st->halt);
+    PF5D_LAUNCHED();
     PF5D_CUFFT32(cufftSetStream(h->inv, s));
     PF5D_CUFFT32(cufftExecC2R(h->inv, h->k, h->s));
   }
@@ -1257,8 +1250,7 @@ const char *s32_rate_kernels(Stepper32 *h) {
 
 int32_t s32_launches_per_step(const Stepper32 *h) {
   const bool split = h->d.dim >= 2 && variants32()[h->variant].split;
-  // rate (+chem), dt, update, and the B(k) multiply unless cuFFT applies it
-  return (split ? 4 : 3) + (h->d.elastic && !h->fused ? 1 : 0);
+  return (split ? 4 : 3) + (h->d.elastic ? 1 : 0);   // rate (+chem), dt, update (+ B(k))
 }
 
 pf5d_status s32_set_variant(Stepper32 *h, int32_t variant) {
@@ -1328,7 +1320,6 @@ pf5d_status s32_launch_stage(Stepper32 *h, int32_t stage, void *stream) {
       return PF5D_OK;
     case PF5D_STAGE_BMUL:
       PF5D_REQUIRE(h->d.elastic, PF5D_ERR_ARG, "elasticity is off");
-      if (h->fused) return PF5D_OK;        // the inverse transform applies B(k)/N
       k32_bmul<<<grid_for(h->nk, 256), 256, 0, s>>>(h->k, h->bk, h->nk, &h->st->halt);
       PF5D_LAUNCHED();
       return PF5D_OK;
@@ -1351,7 +1342,6 @@ void s32_destroy(Stepper32 *h) {
   if (h->plans) {
     cufftDestroy(h->fwd);
     cufftDestroy(h->inv);
-    if (h->cb_info) cudaFree(h->cb_info);
   }
   cudaFree(h->hi);
   cudaFree(h->lo);

@@ -1683,8 +1683,7 @@ pf5d_status enqueue_step(pf5d_stepper *h, cudaStream_t s) {
   pf5d_status st;
   if (h->d.elastic) {
     if ((st = fft_forward(&h->fft, h->s, h->k, s)) != PF5D_OK) return st;
-    if (!h->fft.fused && (st = launch_bmul(h->k, h->bk, h->fft.nk, &h->st->halt, s)) != PF5D_OK)
-      return st;
+    if ((st = launch_bmul(h->k, h->bk, h->fft.nk, &h->st->halt, s)) != PF5D_OK) return st;
     if ((st = fft_inverse(&h->fft, h->k, h->s, s)) != PF5D_OK) return st;
   }
   if ((st = launch_rate(h, s)) != PF5D_OK) return st;
@@ -1782,10 +1781,8 @@ pf5d_status pf5d_stepper_create(const pf5d_stepper_desc *desc, double *X, void *
     return fail(PF5D_ERR_CUDA);
   }
   if (desc->elastic) {
-    int64_t fft_npts, fft_nk;
-    fft_sizes(desc->dim, h->shape, &fft_npts, &fft_nk);
-    if ((st = upload_bk_scaled(desc->bk, fft_nk, npts, &h->bk)) != PF5D_OK) return fail(st);
-    if ((st = fft_create(desc->dim, h->shape, &h->fft, h->bk)) != PF5D_OK) return fail(st);
+    if ((st = fft_create(desc->dim, h->shape, &h->fft)) != PF5D_OK) return fail(st);
+    if ((st = upload_bk_scaled(desc->bk, h->fft.nk, npts, &h->bk)) != PF5D_OK) return fail(st);
     if (cudaMalloc(&h->s, npts * sizeof(double)) != cudaSuccess ||
         cudaMalloc(&h->k, h->fft.nk * sizeof(cufftDoubleComplex)) != cudaSuccess) {
       set_error("device allocation failed");
@@ -2004,9 +2001,7 @@ pf5d_status pf5d_stepper_step_save(pf5d_stepper *h, pf5d_save_diag *out, void *s
     // the step up to its rate evaluation, as enqueue_step
     if (h->d.elastic) {
       if ((st = fft_forward(&h->fft, h->s, h->k, s)) != PF5D_OK) return st;
-      if (!h->fft.fused &&
-          (st = launch_bmul(h->k, h->bk, h->fft.nk, &h->st->halt, s)) != PF5D_OK)
-        return st;
+      if ((st = launch_bmul(h->k, h->bk, h->fft.nk, &h->st->halt, s)) != PF5D_OK) return st;
       if ((st = fft_inverse(&h->fft, h->k, h->s, s)) != PF5D_OK) return st;
     }
     if ((st = launch_rate(h, s)) != PF5D_OK) return st;
@@ -2083,8 +2078,7 @@ int32_t pf5d_stepper_launches_per_step(const pf5d_stepper *h) {
   if (!h) return 0;
   if (h->s32) return s32_launches_per_step(h->s32);
   const bool split = h->d.dim >= 2 && rate_variants()[h->variant].split;
-  // rate (+chem), dt, update, and the B(k) multiply unless cuFFT applies it
-  return (split ? 2 : 1) + 2 + (h->d.elastic && !h->fft.fused ? 1 : 0);
+  return (split ? 2 : 1) + 2 + (h->d.elastic ? 1 : 0);   // rate (+chem), dt, update, bmul
 }
 
 const char *pf5d_stepper_rate_kernels(pf5d_stepper *h) {
@@ -2117,7 +2111,6 @@ pf5d_status pf5d_stepper_launch_stage(pf5d_stepper *h, int32_t stage, void *stre
       return fft_forward(&h->fft, h->s, h->k, s);
     case PF5D_STAGE_BMUL:
       PF5D_REQUIRE(h->d.elastic, PF5D_ERR_ARG, "elasticity is off");
-      if (h->fft.fused) return PF5D_OK;    // the inverse transform applies B(k)/N
       return launch_bmul(h->k, h->bk, h->fft.nk, &h->st->halt, s);
     case PF5D_STAGE_FFT_INV:
       PF5D_REQUIRE(h->d.elastic, PF5D_ERR_ARG, "elasticity is off");
