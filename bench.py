@@ -214,17 +214,18 @@ def cpu_threads():
     return O.num_threads()
 
 
-def time_oracle(prob, steps, warmup, budget_s=None):
+def time_oracle(prob, steps, warmup, budget_s=None, min_s=0.0):
     """Reference algorithm on the host cores: (grid-point steps/s, seconds,
-    steps timed).  With ``budget_s`` the sample stops early once that much
-    time has passed (at least one step is timed)."""
+    steps timed).  The sample runs ``steps`` steps and keeps going until
+    ``min_s`` seconds have passed; with ``budget_s`` it stops early once that
+    much time has passed (at least one step is timed)."""
     from oracle.oracle import OracleStepper
     st = OracleStepper.from_problem(prob, fft_workers=-1)
     for _ in range(warmup):
         st.step()
     t0 = time.perf_counter()
     done = 0
-    while done < steps:
+    while done < steps or time.perf_counter() - t0 < min_s:
         st.step()
         done += 1
         if budget_s is not None and time.perf_counter() - t0 > budget_s:
@@ -233,10 +234,12 @@ def time_oracle(prob, steps, warmup, budget_s=None):
     return prob.n_points * done / dt, dt, done
 
 
-def cpu_baseline(prob, args, workload_name, budget_s=20.0):
-    """The oracle on the host cores, on a bounded sample of the workload."""
+def cpu_baseline(prob, args, workload_name, budget_s=20.0, min_s=10.0):
+    """The oracle on the host cores, on a bounded sample of the workload:
+    at least ``--cpu-steps`` (default ``--steps``) steps and 10 s of work,
+    at most 20 s."""
     steps = args.cpu_steps if args.cpu_steps is not None else args.steps
-    val, secs, done = time_oracle(prob, steps, 1, budget_s=budget_s)
+    val, secs, done = time_oracle(prob, steps, 1, budget_s=budget_s, min_s=min_s)
     return {"value": val, "unit": "grid-point steps/s", "cores": cpu_threads(), "kind": "port",
             "sample": f"{done} steps ({secs:.1f} s) of the full {workload_name} after 1 warm-up "
                       f"(oracle C restatement + scipy FFT, all host threads)"}
