@@ -34,6 +34,8 @@
 #include <map>
 #include <vector>
 
+#include <cuda_pipeline_primitives.h>
+
 #include "pf5d_device.cuh"
 #include "pf5d_fft.h"
 #include "pf5d_fp32c.h"
@@ -1124,6 +1126,148 @@ __global__ void __launch_bounds__(TX * TY, MINB) k_rate_march3d(RateParams P, in
   finish_rate(P, vmax, red);
 }
 
+// ------------------------------------------------------------------------
+// Split rate evaluation, second kernel in 3D: faces and divergence of a
+// TY x TX plane tile marching along axis 0, from X and the mu/M rows that
+// k_chem64 wrote.  The X and mu/M of each plane (tile + 1-cell halo) go
+// through a three-plane ring in shared memory that cp.async fills two
+// planes ahead, so the loads of plane z+2 run under the faces of plane z.
+// Faces and the divergence sum in k_rate_march3d's order (fluxes.py:352-395:
+// axis 0, then 1, then 2), so the same bits.
+// ------------------------------------------------------------------------
+template <int TX, int TY>
+struct Flux3Geom64 {
+  static constexpr int MX = TX + 2, MY = TY + 2, PM = MX * MY, NT = TX * TY;
+  static constexpr int NFX = TY * (TX + 1), NFY = (TY + 1) * TX;
+  static constexpr size_t slot = (size_t)(S + NP) * PM;          // doubles: X rows, then mu/M rows
+  static constexpr size_t smem(bool perpoint) {
+    return (3 * slot + (perpoint ? 0 : (size_t)S * (NFX + NFY)) + NT / 32) * sizeof(double) +
+           (MX + MY) * sizeof(int);
+  }
+};
+
+template <int TX, int TY, int MINB, bool PERPOINT>
+__global__ void __launch_bounds__(TX * TY, MINB) k_flux3_64(RateParams P, int zc) {
+  using G = Flux3Geom64<TX, TY>;
+  pdl_wait();
+  if (P.st->halt) return;
+  extern __shared__ double sm[];
+  double *ring = sm;                                         // [3][S + NP][PM]
+  double *Fx = ring + 3 * G::slot;                           // [S][NFX] (flat faces)
+  double *Fy = Fx + (PERPOINT ? 0 : S * G::NFX);             // [S][NFY]
+  double *red = Fy + (PERPOINT ? 0 : S * G::NFY);            // [NT/32]
+  int *wx = reinterpret_cast<int *>(red + G::NT / 32);
+  int *wy = wx + G::MX;
+  const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * TX + tx;
+  const int x0 = blockIdx.x * TX, y0 = blockIdx.y * TY;
+  const int zb = blockIdx.z * zc;
+  const int ze = min(zb + zc, P.nz);
+  const int64_t plane = (int64_t)P.ny * P.nx;
+  for (int i = tid; i < G::MX + G::MY; i += G::NT) {
+    if (i < G::MX) wx[i] = wrap_any(x0 + i - 1, P.nx);
+    else wy[i - G::MX] = wrap_any(y0 + (i - G::MX) - 1, P.ny);
+  }
+  __syncthreads();
+  auto sX = [&](int z) { return ring + ((z - zb + 3) % 3) * G::slot; };
+  auto sM = [&](int z) { return sX(z) + S * G::PM; };
+  auto issue = [&](int z, bool interior_only) {
+    const int64_t zoff = (int64_t)wrap_any(z, P.nz) * plane;
+    double *x = sX(z), *m = sM(z);
+    for (int pos = tid; pos < G::PM; pos += G::NT) {
+      const int my = pos / G::MX, mx = pos - my * G::MX;
+      const bool ex = (mx == 0 || mx == G::MX - 1), ey = (my == 0 || my == G::MY - 1);
+      if (interior_only ? (ex || ey) : (ex && ey)) continue;
+      const int64_t g = zoff + (int64_t)wy[my] * P.nx + wx[mx];
+#pragma unroll
+      for (int c = 0; c < S; ++c) __pipeline_memcpy_async(x + c * G::PM + pos, P.X + 4 * g + c, 8);
+#pragma unroll
+      for (int r = 0; r < NP; ++r)
+        __pipeline_memcpy_async(m + r * G::PM + pos, P.mm + r * P.npts + g, 8);
+    }
+    __pipeline_commit();
+  };
+  auto face = [&](int zl, int pl, int zh, int ph, double J[S]) {
+    face_between<G::PM, G::PM>(sX(zl), sM(zl), pl, pl, sX(zh), sM(zh), ph, ph, P.inv_dx, J);
+  };
+  const int p = (ty + 1) * G::MX + (tx + 1);
+  const bool in_tile = (x0 + tx < P.nx) && (y0 + ty < P.ny);
+  issue(zb - 1, true);
+  issue(zb, false);
+  issue(zb + 1, false);
+  __pipeline_wait_prior(1);
+  __syncthreads();
+  double Jm[S];
+  face(zb - 1, p, zb, p, Jm);
+  double vmax = 0.0;
+  for (int z = zb; z < ze; ++z) {
+    __pipeline_wait_prior(0);          // plane z+1 copied (this thread's part)
+    __syncthreads();                   // ... and every thread's; the slot of z-1 is free
+    if (z + 2 <= ze) issue(z + 2, false);
+    double a[S];
+    face(z, p, z + 1, p, a);
+#pragma unroll
+    for (int c = 0; c < S; ++c) {
+      const double jz = a[c];
+      a[c] = jz - Jm[c];
+      Jm[c] = jz;
+    }
+    double jyp[S], jym[S], jxp[S], jxm[S];
+    if constexpr (PERPOINT) {
+      // each point evaluates its four in-plane faces (each face by both of
+      // its cells, identical operands and order)
+      face(z, p, z, p + G::MX, jyp);
+      face(z, p - G::MX, z, p, jym);
+      face(z, p, z, p + 1, jxp);
+      face(z, p - 1, z, p, jxm);
+    } else {
+      for (int f = tid; f < G::NFX + G::NFY; f += G::NT) {
+        double J[S];
+        if (f < G::NFX) {
+          const int fy = f / (TX + 1), fx = f - fy * (TX + 1);
+          const int pl = (fy + 1) * G::MX + fx;
+          face(z, pl, z, pl + 1, J);
+#pragma unroll
+          for (int c = 0; c < S; ++c) Fx[c * G::NFX + f] = J[c];
+        } else {
+          const int f2 = f - G::NFX;
+          const int fy = f2 / TX, fx = f2 - fy * TX;
+          const int pl = fy * G::MX + (fx + 1);
+          face(z, pl, z, pl + G::MX, J);
+#pragma unroll
+          for (int c = 0; c < S; ++c) Fy[c * G::NFY + f2] = J[c];
+        }
+      }
+      __syncthreads();
+#pragma unroll
+      for (int c = 0; c < S; ++c) {
+        jyp[c] = Fy[c * G::NFY + (ty + 1) * TX + tx];
+        jym[c] = Fy[c * G::NFY + ty * TX + tx];
+        jxp[c] = Fx[c * G::NFX + ty * (TX + 1) + tx + 1];
+        jxm[c] = Fx[c * G::NFX + ty * (TX + 1) + tx];
+      }
+    }
+    if (in_tile) {
+      double out[S];
+#pragma unroll
+      for (int c = 0; c < S; ++c) {
+        double v = a[c] + jyp[c];
+        v = v - jym[c];
+        v = v + jxp[c];
+        v = v - jxm[c];
+        out[c] = v * P.inv_dx;
+        const double m = fabs(out[c]);
+        if (m > vmax) vmax = m;
+      }
+      const int64_t g = (int64_t)z * plane + (int64_t)(y0 + ty) * P.nx + (x0 + tx);
+      double2 *o = reinterpret_cast<double2 *>(P.dX + 4 * g);
+      o[0] = make_double2(out[0], out[1]);
+      o[1] = make_double2(out[2], out[3]);
+    }
+  }
+  __pipeline_wait_prior(0);
+  finish_rate(P, vmax, red);
+}
+
 template <int TX, int TY, int SORT = 0>
 constexpr size_t march3d_smem() {
   using G = PlaneGeom<TX, TY>;
@@ -1376,6 +1520,7 @@ struct RateVariant {
   int nth;          // threads of a 2D block (1D block; >= tx * ty)
   bool win;
   bool split;
+  bool only3d = false;   // 2D runs another variant's kernels: not tuned there
   size_t smem2d, smem3d;
   void (*set_attrs)(bool vec);
   void (*launch2d)(bool vec, dim3 g, dim3 b, size_t sm, cudaStream_t s, const RateParams &P);
@@ -1490,6 +1635,34 @@ RateVariant make_split_variant() {
   return v;
 }
 
+// Split variant for 3D with the cp.async marching flux kernel k_flux3_64
+// (PP: per-point faces); in 2D it runs make_split_variant's kernels.
+template <int TX, int TY, int MINB, int KMINB, bool PP>
+RateVariant make_split3_variant() {
+  RateVariant v = make_split_variant<TX, TY, MINB, KMINB>();
+  v.only3d = true;
+  v.smem3d = Flux3Geom64<TX, TY>::smem(PP);
+  v.set_attrs = [](bool) {
+    const auto a = cudaFuncAttributeMaxDynamicSharedMemorySize;
+    cudaFuncSetAttribute(k_rate_tile2d<TX, TY, MINB, true, false, true>, a,
+                         (int)tile2d_smem<TX, TY>());
+    cudaFuncSetAttribute(k_flux3_64<TX, TY, MINB, PP>, a, (int)Flux3Geom64<TX, TY>::smem(PP));
+    chem_attrs<2, KMINB, 1>();
+    chem_attrs<3, KMINB, 1>();
+  };
+  v.launch3d = [](bool vec, dim3 g, dim3 b, size_t sm, cudaStream_t s, const RateParams &P,
+                  int zc) {
+    launch_chem<3, KMINB, 1>(vec, s, P);
+    launch_pdl(k_flux3_64<TX, TY, MINB, PP>, g, b, sm, s, P, zc);
+  };
+  v.kernels = [](bool vec, int dim) {
+    const std::string chem = kname("k_chem64", {dim, vec, KMINB}) + " + ";
+    if (dim == 2) return chem + kname("k_rate_tile2d", {TX, TY, MINB, 1, 0, 1, TX * TY, 0, 0});
+    return chem + kname("k_flux3_64", {TX, TY, MINB, PP});
+  };
+  return v;
+}
+
 const std::vector<RateVariant> &rate_variants() {
   static const std::vector<RateVariant> v = {
       make_variant<32, 8, 2>(), make_variant<32, 8, 3>(), make_variant<32, 4, 4>(),
@@ -1507,7 +1680,10 @@ const std::vector<RateVariant> &rate_variants() {
       make_variant<32, 8, 3, false, 256, false, true>(), make_variant<64, 4, 2, true, 256, false, true>(),
       make_split_variant<32, 8, 3, 3, true>(), make_split_variant<32, 4, 4, 3, true>(),
       make_split_variant<32, 8, 3, 2, false, 2>(), make_split_variant<32, 4, 4, 2, false, 2>(),
-      make_split_variant<32, 8, 3, 2, true, 2>(), make_split_variant<32, 4, 4, 2, true, 2>()};
+      make_split_variant<32, 8, 3, 2, true, 2>(), make_split_variant<32, 4, 4, 2, true, 2>(),
+      make_split3_variant<32, 4, 3, 3, true>(), make_split3_variant<32, 4, 3, 3, false>(),
+      make_split3_variant<32, 8, 2, 3, true>(), make_split3_variant<32, 8, 2, 3, false>(),
+      make_split3_variant<64, 4, 1, 3, true>(), make_split3_variant<32, 4, 2, 3, true>()};
   return v;
 }
 
@@ -1611,6 +1787,7 @@ pf5d_status autotune_rate(pf5d_stepper *h, cudaStream_t s, float *best_ms) {
   const int reps = 5;
   std::vector<std::pair<float, int>> rate_t;
   for (int v = 0; v < (int)rate_variants().size(); ++v) {
+    if (rate_variants()[v].only3d && h->d.dim != 3) continue;
     pf5d_status st = configure_rate(h, v);
     if (st != PF5D_OK) continue;
     if (launch_rate(h, s) != PF5D_OK) {           // warm-up (e.g. too much smem)
