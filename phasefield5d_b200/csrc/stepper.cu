@@ -1146,6 +1146,32 @@ struct Flux3Geom64 {
   }
 };
 
+// X, mu and M of one position read out of a plane's rows (stride PM), and
+// the face flux between two such positions, lower -> upper: the operands
+// and operation order of face_between, so the same bits.
+struct Pt64 {
+  double x[S], mu[S], m[NM];
+};
+
+template <int PM>
+__device__ __forceinline__ void load_pt64(const double *X, const double *M, int p, Pt64 &q) {
+#pragma unroll
+  for (int c = 0; c < S; ++c) {
+    q.x[c] = X[c * PM + p];
+    q.mu[c] = M[c * PM + p];
+  }
+#pragma unroll
+  for (int c = 0; c < NM; ++c) q.m[c] = M[(S + c) * PM + p];
+}
+
+__device__ __forceinline__ void face_pts64(const Pt64 &lo, const Pt64 &hi, double inv_dx,
+                                           double J[S]) {
+  double g[S];
+#pragma unroll
+  for (int c = 0; c < S; ++c) g[c] = (hi.mu[c] - lo.mu[c]) * inv_dx;
+  face_flux(lo.x, lo.m, hi.x, hi.m, g, J);
+}
+
 template <int TX, int TY, int MINB, bool PERPOINT>
 __global__ void __launch_bounds__(TX * TY, MINB) k_flux3_64(RateParams P, int zc) {
   using G = Flux3Geom64<TX, TY>;
@@ -1196,30 +1222,51 @@ __global__ void __launch_bounds__(TX * TY, MINB) k_flux3_64(RateParams P, int zc
   issue(zb + 1, false);
   __pipeline_wait_prior(1);
   __syncthreads();
+  // PERPOINT: this point's X/mu/M at plane z stay in registers (cur) and
+  // become the lower side of the next plane's axis-0 face.
+  Pt64 cur;
   double Jm[S];
-  face(zb - 1, p, zb, p, Jm);
+  if constexpr (PERPOINT) {
+    Pt64 below;
+    load_pt64<G::PM>(sX(zb - 1), sM(zb - 1), p, below);
+    load_pt64<G::PM>(sX(zb), sM(zb), p, cur);
+    face_pts64(below, cur, P.inv_dx, Jm);
+  } else {
+    face(zb - 1, p, zb, p, Jm);
+  }
   double vmax = 0.0;
   for (int z = zb; z < ze; ++z) {
     __pipeline_wait_prior(0);          // plane z+1 copied (this thread's part)
     __syncthreads();                   // ... and every thread's; the slot of z-1 is free
     if (z + 2 <= ze) issue(z + 2, false);
     double a[S];
-    face(z, p, z + 1, p, a);
+    double jyp[S], jym[S], jxp[S], jxm[S];
+    if constexpr (PERPOINT) {
+      // each point evaluates its four in-plane faces (each face by both of
+      // its cells, identical operands and order)
+      Pt64 up, nb;
+      load_pt64<G::PM>(sX(z + 1), sM(z + 1), p, up);
+      face_pts64(cur, up, P.inv_dx, a);
+      const double *Xz = sX(z), *Mz = sM(z);
+      load_pt64<G::PM>(Xz, Mz, p + G::MX, nb);
+      face_pts64(cur, nb, P.inv_dx, jyp);
+      load_pt64<G::PM>(Xz, Mz, p - G::MX, nb);
+      face_pts64(nb, cur, P.inv_dx, jym);
+      load_pt64<G::PM>(Xz, Mz, p + 1, nb);
+      face_pts64(cur, nb, P.inv_dx, jxp);
+      load_pt64<G::PM>(Xz, Mz, p - 1, nb);
+      face_pts64(nb, cur, P.inv_dx, jxm);
+      cur = up;
+    } else {
+      face(z, p, z + 1, p, a);
+    }
 #pragma unroll
     for (int c = 0; c < S; ++c) {
       const double jz = a[c];
       a[c] = jz - Jm[c];
       Jm[c] = jz;
     }
-    double jyp[S], jym[S], jxp[S], jxm[S];
-    if constexpr (PERPOINT) {
-      // each point evaluates its four in-plane faces (each face by both of
-      // its cells, identical operands and order)
-      face(z, p, z, p + G::MX, jyp);
-      face(z, p - G::MX, z, p, jym);
-      face(z, p, z, p + 1, jxp);
-      face(z, p - 1, z, p, jxm);
-    } else {
+    if constexpr (!PERPOINT) {
       for (int f = tid; f < G::NFX + G::NFY; f += G::NT) {
         double J[S];
         if (f < G::NFX) {
