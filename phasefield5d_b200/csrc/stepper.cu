@@ -477,6 +477,105 @@ __global__ void __launch_bounds__(256, MINB) k_chem64(RateParams P) {
   raise_rate_flags(P.st, flags);
 }
 
+// Split rate evaluation, first kernel, staged form (VEC tables, 2D/3D): the
+// values of k_chem64 bit for bit, with each thread's results put back in
+// the shared input rows at its point's tile position, so the mu/M rows of
+// P.mm are written in tile order (coalesced) rather than in the table-cell
+// order the gathers run in.
+template <int DIM, int MINB>
+__global__ void __launch_bounds__(256, MINB) k_chem64s(RateParams P) {
+  constexpr int NT = 256;
+  static_assert(DIM >= 2, "plane tiles");
+  __shared__ double io[2 * S + 1][NT];   // inputs of each point (x, lap, s'), then its mu/M
+  __shared__ int hist[NT];
+  __shared__ int wsum[NT / 32 + 1];
+  __shared__ unsigned short order[NT];
+  pdl_wait();
+  if (P.st->halt) return;
+  const int tid = threadIdx.y * 32 + threadIdx.x;
+  const int x = blockIdx.x * 32 + threadIdx.x;
+  const int y = blockIdx.y * 8 + threadIdx.y;
+  const int z = blockIdx.z;
+  const bool valid = x < P.nx && y < P.ny;
+  const int64_t plane = (int64_t)P.ny * P.nx;
+  const int64_t zo = (int64_t)z * plane;
+  const int64_t g = zo + (int64_t)y * P.nx + x;
+  hist[tid] = 0;
+  int key = 0, rank = 0;
+  __syncthreads();
+  if (valid) {
+    auto ld = [&](int64_t gi, double v[S]) {
+      const double2 a = __ldg(reinterpret_cast<const double2 *>(P.X + 4 * gi));
+      const double2 b = __ldg(reinterpret_cast<const double2 *>(P.X + 4 * gi) + 1);
+      v[0] = a.x; v[1] = a.y; v[2] = b.x; v[3] = b.y;
+    };
+    const int xp = x + 1 == P.nx ? 0 : x + 1, xm = x == 0 ? P.nx - 1 : x - 1;
+    const int yp = y + 1 == P.ny ? 0 : y + 1, ym = y == 0 ? P.ny - 1 : y - 1;
+    double xc[S], lap[S], n0[S], n1[S];
+    ld(g, xc);
+    if (DIM == 3) {
+      const int zp = z + 1 == P.nz ? 0 : z + 1, zm = z == 0 ? P.nz - 1 : z - 1;
+      ld((int64_t)zp * plane + (int64_t)y * P.nx + x, n0);
+      ld((int64_t)zm * plane + (int64_t)y * P.nx + x, n1);
+#pragma unroll
+      for (int c = 0; c < S; ++c) lap[c] = n0[c] + n1[c];
+      ld(zo + (int64_t)yp * P.nx + x, n0);
+      ld(zo + (int64_t)ym * P.nx + x, n1);
+#pragma unroll
+      for (int c = 0; c < S; ++c) lap[c] = (lap[c] + n0[c]) + n1[c];
+    } else {
+      ld(zo + (int64_t)yp * P.nx + x, n0);
+      ld(zo + (int64_t)ym * P.nx + x, n1);
+#pragma unroll
+      for (int c = 0; c < S; ++c) lap[c] = n0[c] + n1[c];
+    }
+    ld(zo + (int64_t)y * P.nx + xp, n0);
+    ld(zo + (int64_t)y * P.nx + xm, n1);
+#pragma unroll
+    for (int c = 0; c < S; ++c) {
+      lap[c] = (((lap[c] + n0[c]) + n1[c]) - (DIM == 3 ? 6.0 : 4.0) * xc[c]) * P.inv_dx2;
+      io[c][tid] = xc[c];
+      io[S + c][tid] = lap[c];
+    }
+    io[2 * S][tid] = P.sp ? __ldg(P.sp + g) : 0.0;
+    key = cell_hash(xc, (float)P.T.inv_step);
+    rank = atomicAdd(&hist[key], 1);
+  }
+  __syncthreads();
+  const int count = block_exclusive_scan<NT, NT>(hist, wsum, tid);
+  if (valid) order[hist[key] + rank] = (unsigned short)tid;
+  __syncthreads();
+  unsigned flags = 0;
+  if (tid < count) {
+    const int q = order[tid];
+    double xq[S], lq[S], v[NP];
+#pragma unroll
+    for (int c = 0; c < S; ++c) {
+      xq[c] = io[c][q];
+      lq[c] = io[S + c][q];
+    }
+    const double spv = io[2 * S][q];
+    const int o[S] = {0, 0, 0, 0};
+    interp_win64<true>(P.T, xq, nullptr, o, v, &flags);
+    // column q is this thread's alone: its inputs are read, now its results
+#pragma unroll
+    for (int c = 0; c < S; ++c) {
+      const double lk = lq[c] * P.kappa.v[c];
+      double m = v[c] - lk;
+      if (P.sp) m = m + spv * P.lvec.v[c];
+      io[c][q] = m;
+    }
+#pragma unroll
+    for (int c = 0; c < NM; ++c) io[S + c][q] = v[S + c];
+  }
+  raise_rate_flags(P.st, flags);
+  __syncthreads();
+  if (valid) {
+#pragma unroll
+    for (int r = 0; r < NP; ++r) P.mm[r * P.npts + g] = io[r][tid];
+  }
+}
+
 // Split rate evaluation, first kernel, shared-gather form: the same values
 // as k_chem64 (bit for bit), with the table gathers of up to K points of one
 // table cell shared.  A block of 256 threads takes a brick of 256 K points
@@ -1683,8 +1782,20 @@ RateVariant make_split_variant() {
 }
 
 // Split variant for 3D with the cp.async marching flux kernel k_flux3_64
-// (PP: per-point faces); in 2D it runs make_split_variant's kernels.
-template <int TX, int TY, int MINB, int KMINB, bool PP>
+// (PP: per-point faces) after the mu/M kernel CHEM (0: k_chem64, 1:
+// k_chem64s; k_chem64 for tables that are not double2-aligned); in 2D it
+// runs make_split_variant's kernels.
+template <int DIM, int KMINB, int CHEM>
+void launch_chem3(bool vec, cudaStream_t s, const RateParams &P) {
+  if (CHEM == 0 || !vec) {
+    launch_chem<DIM, KMINB, 1>(vec, s, P);
+    return;
+  }
+  const dim3 b(32, 8), g((unsigned)((P.nx + 31) / 32), (unsigned)((P.ny + 7) / 8), (unsigned)P.nz);
+  launch_pdl(k_chem64s<DIM, KMINB>, g, b, 0, s, P);
+}
+
+template <int TX, int TY, int MINB, int KMINB, bool PP, int CHEM = 0>
 RateVariant make_split3_variant() {
   RateVariant v = make_split_variant<TX, TY, MINB, KMINB>();
   v.only3d = true;
@@ -1694,16 +1805,16 @@ RateVariant make_split3_variant() {
     cudaFuncSetAttribute(k_rate_tile2d<TX, TY, MINB, true, false, true>, a,
                          (int)tile2d_smem<TX, TY>());
     cudaFuncSetAttribute(k_flux3_64<TX, TY, MINB, PP>, a, (int)Flux3Geom64<TX, TY>::smem(PP));
-    chem_attrs<2, KMINB, 1>();
-    chem_attrs<3, KMINB, 1>();
   };
   v.launch3d = [](bool vec, dim3 g, dim3 b, size_t sm, cudaStream_t s, const RateParams &P,
                   int zc) {
-    launch_chem<3, KMINB, 1>(vec, s, P);
+    launch_chem3<3, KMINB, CHEM>(vec, s, P);
     launch_pdl(k_flux3_64<TX, TY, MINB, PP>, g, b, sm, s, P, zc);
   };
   v.kernels = [](bool vec, int dim) {
-    const std::string chem = kname("k_chem64", {dim, vec, KMINB}) + " + ";
+    const std::string chem =
+        (CHEM == 0 || !vec ? kname("k_chem64", {dim, vec, KMINB})
+                           : kname("k_chem64s", {dim, KMINB})) + " + ";
     if (dim == 2) return chem + kname("k_rate_tile2d", {TX, TY, MINB, 1, 0, 1, TX * TY, 0, 0});
     return chem + kname("k_flux3_64", {TX, TY, MINB, PP});
   };
@@ -1730,7 +1841,9 @@ const std::vector<RateVariant> &rate_variants() {
       make_split_variant<32, 8, 3, 2, true, 2>(), make_split_variant<32, 4, 4, 2, true, 2>(),
       make_split3_variant<32, 4, 3, 3, true>(), make_split3_variant<32, 4, 3, 3, false>(),
       make_split3_variant<32, 8, 2, 3, true>(), make_split3_variant<32, 8, 2, 3, false>(),
-      make_split3_variant<64, 4, 1, 3, true>(), make_split3_variant<32, 4, 2, 3, true>()};
+      make_split3_variant<64, 4, 1, 3, true>(), make_split3_variant<32, 4, 2, 3, true>(),
+      make_split3_variant<32, 4, 3, 3, true, 1>(), make_split3_variant<32, 4, 3, 4, true, 1>(),
+      make_split3_variant<32, 4, 2, 3, true, 1>()};
   return v;
 }
 
