@@ -1667,6 +1667,7 @@ struct RateVariant {
   bool win;
   bool split;
   bool only3d = false;   // 2D runs another variant's kernels: not tuned there
+  bool only2d = false;   // 3D runs another variant's kernels: not tuned there
   size_t smem2d, smem3d;
   void (*set_attrs)(bool vec);
   void (*launch2d)(bool vec, dim3 g, dim3 b, size_t sm, cudaStream_t s, const RateParams &P);
@@ -1795,6 +1796,26 @@ void launch_chem3(bool vec, cudaStream_t s, const RateParams &P) {
   launch_pdl(k_chem64s<DIM, KMINB>, g, b, 0, s, P);
 }
 
+// Split variant for 2D with k_chem64s (coalesced mu/M rows) before the
+// split tile kernel; in 3D it runs make_split_variant's kernels.
+template <int TX, int TY, int MINB, int KMINB>
+RateVariant make_split2s_variant() {
+  RateVariant v = make_split_variant<TX, TY, MINB, KMINB>();
+  v.only2d = true;
+  v.launch2d = [](bool vec, dim3 g, dim3 b, size_t sm, cudaStream_t s, const RateParams &P) {
+    launch_chem3<2, KMINB, 1>(vec, s, P);
+    launch_pdl(k_rate_tile2d<TX, TY, MINB, true, false, true>, g, b, sm, s, P);
+  };
+  v.kernels = [](bool vec, int dim) {
+    if (dim == 2)
+      return (vec ? kname("k_chem64s", {2, KMINB}) : kname("k_chem64", {2, vec, KMINB})) + " + " +
+             kname("k_rate_tile2d", {TX, TY, MINB, 1, 0, 1, TX * TY, 0, 0});
+    return kname("k_chem64", {dim, vec, KMINB}) + " + " +
+           kname("k_rate_march3d", {TX, TY, MINB, 1, 0, 1, 0, 0});
+  };
+  return v;
+}
+
 template <int TX, int TY, int MINB, int KMINB, bool PP, int CHEM = 0>
 RateVariant make_split3_variant() {
   RateVariant v = make_split_variant<TX, TY, MINB, KMINB>();
@@ -1843,7 +1864,8 @@ const std::vector<RateVariant> &rate_variants() {
       make_split3_variant<32, 8, 2, 3, true>(), make_split3_variant<32, 8, 2, 3, false>(),
       make_split3_variant<64, 4, 1, 3, true>(), make_split3_variant<32, 4, 2, 3, true>(),
       make_split3_variant<32, 4, 3, 3, true, 1>(), make_split3_variant<32, 4, 3, 4, true, 1>(),
-      make_split3_variant<32, 4, 2, 3, true, 1>()};
+      make_split3_variant<32, 4, 2, 3, true, 1>(),
+      make_split2s_variant<32, 8, 3, 4>()};
   return v;
 }
 
@@ -1948,6 +1970,7 @@ pf5d_status autotune_rate(pf5d_stepper *h, cudaStream_t s, float *best_ms) {
   std::vector<std::pair<float, int>> rate_t;
   for (int v = 0; v < (int)rate_variants().size(); ++v) {
     if (rate_variants()[v].only3d && h->d.dim != 3) continue;
+    if (rate_variants()[v].only2d && h->d.dim != 2) continue;
     pf5d_status st = configure_rate(h, v);
     if (st != PF5D_OK) continue;
     if (launch_rate(h, s) != PF5D_OK) {           // warm-up (e.g. too much smem)
