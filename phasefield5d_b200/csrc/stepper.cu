@@ -1623,6 +1623,36 @@ __global__ void k_mean_final(const double *partial, int nparts, double *out) {
 
 using namespace pf5d;
 
+namespace pf5d {
+
+// The 1D elastic term in closed form, in place: s (the misfit) ->
+// s' = bn (s - mean s) + b0 mean s, where bn is B(k) for every k != 0 and
+// b0 is B(0).  That is irfft(B rfft(s)) (elastic.py:250-263) exactly, for a
+// B(k) that depends on k only through its sign, as every 1D B(k) does.  One
+// block: per-thread sums over a fixed stride, then a fixed tree, so the
+// mean has the same bits on every run.
+constexpr int kElastic1dThreads = 1024;
+constexpr int64_t kElastic1dMax = 16384;     // points of a 1D solve that use it
+__global__ void __launch_bounds__(kElastic1dThreads)
+    k_elastic1d(double *s, int64_t n, double bn, double b0, const unsigned *halt) {
+  __shared__ double red[kElastic1dThreads / 32];
+  pdl_wait();
+  if (*halt) return;
+  const int t = threadIdx.x;
+  double acc = 0.0;
+  for (int64_t i = t; i < n; i += kElastic1dThreads) acc = acc + s[i];
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) acc = acc + __shfl_xor_sync(0xffffffffu, acc, o);
+  if ((t & 31) == 0) red[t >> 5] = acc;
+  __syncthreads();
+  double tot = red[0];
+  for (int w = 1; w < kElastic1dThreads / 32; ++w) tot = tot + red[w];
+  const double mean = tot / (double)n;
+  for (int64_t i = t; i < n; i += kElastic1dThreads) s[i] = bn * (s[i] - mean) + b0 * mean;
+}
+
+}  // namespace pf5d
+
 struct pf5d_stepper {
   pf5d_stepper_desc d{};
   int64_t shape[3] = {1, 1, 1};
@@ -1648,6 +1678,8 @@ struct pf5d_stepper {
   double *mm = nullptr;          // split-rate mu/M buffer (also save-step diagnostics)
   double *diag_ws = nullptr;     // save-step partial rows + mean
   double *partial = nullptr;     // rate kernel block maxima
+  bool closed1d = false;         // 1D elastic term in closed form (k_elastic1d)
+  double bn = 0.0, b0 = 0.0;     // its B(k): bn for every k != 0, b0 at k = 0
   double *save_x = nullptr;      // FP32C save steps: FP64 field, dX/dt, mu/M
   std::string kernels;           // text returned by pf5d_stepper_rate_kernels
 };
@@ -2039,13 +2071,25 @@ pf5d_status autotune_rate(pf5d_stepper *h, cudaStream_t s, float *best_ms) {
   return PF5D_OK;
 }
 
+// The elastic term of a step: s (the misfit the update wrote) -> s' in
+// place, by cuFFT D2Z, the B(k)/N multiply and Z2D, or in 1D by
+// k_elastic1d (elastic.py:250-263 with a B(k) that is one constant for
+// every k != 0: irfft(B rfft(s)) = bn (s - mean s) + b0 mean s exactly).
+pf5d_status elastic_stage(pf5d_stepper *h, cudaStream_t s) {
+  if (h->closed1d) {
+    PF5D_CUDA(launch_pdl(k_elastic1d, dim3(1), dim3(kElastic1dThreads), 0, s, h->s, h->npts,
+                         h->bn, h->b0, (const unsigned *)&h->st->halt));
+    return PF5D_OK;
+  }
+  pf5d_status st;
+  if ((st = fft_forward(&h->fft, h->s, h->k, s)) != PF5D_OK) return st;
+  if ((st = launch_bmul(h->k, h->bk, h->fft.nk, &h->st->halt, s)) != PF5D_OK) return st;
+  return fft_inverse(&h->fft, h->k, h->s, s);
+}
+
 pf5d_status enqueue_step(pf5d_stepper *h, cudaStream_t s) {
   pf5d_status st;
-  if (h->d.elastic) {
-    if ((st = fft_forward(&h->fft, h->s, h->k, s)) != PF5D_OK) return st;
-    if ((st = launch_bmul(h->k, h->bk, h->fft.nk, &h->st->halt, s)) != PF5D_OK) return st;
-    if ((st = fft_inverse(&h->fft, h->k, h->s, s)) != PF5D_OK) return st;
-  }
+  if (h->d.elastic && (st = elastic_stage(h, s)) != PF5D_OK) return st;
   if ((st = launch_rate(h, s)) != PF5D_OK) return st;
   PF5D_CUDA(launch_pdl(k_update_step, dim3(grid_for(h->npts, 256, 4)), dim3(256), 0, s, h->up));
   return PF5D_OK;
@@ -2139,6 +2183,16 @@ pf5d_status pf5d_stepper_create(const pf5d_stepper_desc *desc, double *X, void *
   if (cudaMalloc(&h->mm, (size_t)npts * NP * sizeof(double)) != cudaSuccess) {
     set_error("device allocation failed");
     return fail(PF5D_ERR_CUDA);
+  }
+  if (desc->elastic && desc->dim == 1 && npts <= kElastic1dMax) {
+    // B(k) of a 1D solve depends on k only through its sign: one value for
+    // every k != 0 (checked exactly here), so the closed form applies
+    const int64_t nk = npts / 2 + 1;
+    bool flat = true;
+    for (int64_t i = 2; i < nk && flat; ++i) flat = desc->bk[i] == desc->bk[1];
+    h->closed1d = flat;
+    h->bn = nk > 1 ? desc->bk[1] : 0.0;
+    h->b0 = desc->bk[0];
   }
   if (desc->elastic) {
     if ((st = fft_create(desc->dim, h->shape, &h->fft)) != PF5D_OK) return fail(st);
@@ -2359,11 +2413,7 @@ pf5d_status pf5d_stepper_step_save(pf5d_stepper *h, pf5d_save_diag *out, void *s
     Xpost = sx;
   } else {
     // the step up to its rate evaluation, as enqueue_step
-    if (h->d.elastic) {
-      if ((st = fft_forward(&h->fft, h->s, h->k, s)) != PF5D_OK) return st;
-      if ((st = launch_bmul(h->k, h->bk, h->fft.nk, &h->st->halt, s)) != PF5D_OK) return st;
-      if ((st = fft_inverse(&h->fft, h->k, h->s, s)) != PF5D_OK) return st;
-    }
+    if (h->d.elastic && (st = elastic_stage(h, s)) != PF5D_OK) return st;
     if ((st = launch_rate(h, s)) != PF5D_OK) return st;
     // mu and M of this step at every point, then the "before" reductions
     switch (dim) {
@@ -2466,14 +2516,18 @@ pf5d_status pf5d_stepper_launch_stage(pf5d_stepper *h, int32_t stage, void *stre
       k_update_step<<<grid_for(h->npts, 256, 4), 256, 0, s>>>(h->up);
       PF5D_LAUNCHED();
       return PF5D_OK;
+    // 1D closed form: the whole elastic term is the FFT_FWD stage
     case PF5D_STAGE_FFT_FWD:
       PF5D_REQUIRE(h->d.elastic, PF5D_ERR_ARG, "elasticity is off");
+      if (h->closed1d) return elastic_stage(h, s);
       return fft_forward(&h->fft, h->s, h->k, s);
     case PF5D_STAGE_BMUL:
       PF5D_REQUIRE(h->d.elastic, PF5D_ERR_ARG, "elasticity is off");
+      if (h->closed1d) return PF5D_OK;
       return launch_bmul(h->k, h->bk, h->fft.nk, &h->st->halt, s);
     case PF5D_STAGE_FFT_INV:
       PF5D_REQUIRE(h->d.elastic, PF5D_ERR_ARG, "elasticity is off");
+      if (h->closed1d) return PF5D_OK;
       return fft_inverse(&h->fft, h->k, h->s, s);
     default:
       set_error("unknown stage %d", stage);
