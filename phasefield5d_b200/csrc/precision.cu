@@ -738,6 +738,31 @@ __global__ void __launch_bounds__(kDt32Threads) k32_dt(Rate32 P, int nparts) {
   }
 }
 
+// The 1D elastic term in closed form, in place: s -> s' = bn (s - mean s) +
+// b0 mean s (bn: B(k) for every k != 0, b0: B(0)), i.e. irfft(B rfft(s))
+// exactly (elastic.py:250-263); the mean and the product in FP64, s' rounded
+// once to FP32.  One block, a fixed summation order.
+constexpr int kElastic1dThreads32 = 1024;
+constexpr int64_t kElastic1dMax32 = 16384;
+__global__ void __launch_bounds__(kElastic1dThreads32)
+    k32_elastic1d(float *s, int64_t n, double bn, double b0, const unsigned *halt) {
+  __shared__ double red[kElastic1dThreads32 / 32];
+  pdl_wait();
+  if (*halt) return;
+  const int t = threadIdx.x;
+  double acc = 0.0;
+  for (int64_t i = t; i < n; i += kElastic1dThreads32) acc = acc + (double)s[i];
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) acc = acc + __shfl_xor_sync(0xffffffffu, acc, o);
+  if ((t & 31) == 0) red[t >> 5] = acc;
+  __syncthreads();
+  double tot = red[0];
+  for (int w = 1; w < kElastic1dThreads32 / 32; ++w) tot = tot + red[w];
+  const double mean = tot / (double)n;
+  for (int64_t i = t; i < n; i += kElastic1dThreads32)
+    s[i] = (float)(bn * ((double)s[i] - mean) + b0 * mean);
+}
+
 __global__ void k32_bmul(cufftComplex *__restrict__ k, const float *__restrict__ bk, int64_t nk,
                          const unsigned *halt) {
   if (halt && *halt) return;
@@ -852,6 +877,8 @@ const std::vector<Variant32> &variants32() {
 
 struct Stepper32 {
   pf5d_stepper_desc d{};
+  bool closed1d = false;         // 1D elastic term in closed form (k32_elastic1d)
+  double bn = 0.0, b0 = 0.0;     // its B(k): bn for every k != 0, b0 at k = 0
   int64_t shape[3] = {1, 1, 1};
   int64_t npts = 0, nk = 0;
   float4 *hi = nullptr, *lo = nullptr, *dX = nullptr;
@@ -944,14 +971,27 @@ static pf5d_status launch_rate32(Stepper32 *h, cudaStream_t s) {
   return PF5D_OK;
 }
 
-static pf5d_status enqueue32(Stepper32 *h, cudaStream_t s) {
-  if (h->d.elastic) {
+// The elastic term of a step: s -> s' in place, by cuFFT R2C, the B(k)/N
+// multiply and C2R, or in 1D by k32_elastic1d (the closed form).
+static pf5d_status elastic32(Stepper32 *h, cudaStream_t s) {
+  if (h->closed1d) {
+    PF5D_CUDA(launch_pdl(k32_elastic1d, dim3(1), dim3(kElastic1dThreads32), 0, s, h->s, h->npts,
+                         h->bn, h->b0, (const unsigned *)&h->st->halt));
+    return PF5D_OK;
+  }
     PF5D_CUFFT32(cufftSetStream(h->fwd, s));
     PF5D_CUFFT32(cufftExecR2C(h->fwd, h->s, h->k));
     k32_bmul<<<grid_for(h->nk, 256), 256, 0, s>>>(h->k, h->bk, h->nk, &h->st->halt);
     PF5D_LAUNCHED();
     PF5D_CUFFT32(cufftSetStream(h->inv, s));
     PF5D_CUFFT32(cufftExecC2R(h->inv, h->k, h->s));
+  return PF5D_OK;
+}
+
+static pf5d_status enqueue32(Stepper32 *h, cudaStream_t s) {
+  if (h->d.elastic) {
+    const pf5d_status e = elastic32(h, s);
+    if (e != PF5D_OK) return e;
   }
   pf5d_status st = launch_rate32(h, s);
   if (st != PF5D_OK) return st;
@@ -1031,6 +1071,14 @@ pf5d_status s32_create(const pf5d_stepper_desc *desc, const double *X_init, void
       return fail(PF5D_ERR_CUFFT);
     }
     h->plans = true;
+    if (desc->dim == 1 && npts <= kElastic1dMax32) {
+      // 1D B(k) is one value for every k != 0 (checked exactly): closed form
+      bool flat = true;
+      for (int64_t i = 2; i < h->nk && flat; ++i) flat = desc->bk[i] == desc->bk[1];
+      h->closed1d = flat;
+      h->bn = h->nk > 1 ? desc->bk[1] : 0.0;
+      h->b0 = desc->bk[0];
+    }
     std::vector<float> b(h->nk);
     const double inv_n = 1.0 / (double)npts;
     for (int64_t i = 0; i < h->nk; ++i) b[i] = (float)(desc->bk[i] * inv_n);
@@ -1185,12 +1233,8 @@ pf5d_status s32_step_save_inputs(Stepper32 *h, double *X_out, double *dX_out, do
                                  void *stream) {
   cudaStream_t s = as_stream(stream);
   if (h->d.elastic) {
-    PF5D_CUFFT32(cufftSetStream(h->fwd, s));
-    PF5D_CUFFT32(cufftExecR2C(h->fwd, h->s, h->k));
-    k32_bmul<<<grid_for(h->nk, 256), 256, 0, s>>>(h->k, h->bk, h->nk, &h->st->halt);
-    PF5D_LAUNCHED();
-    PF5D_CUFFT32(cufftSetStream(h->inv, s));
-    PF5D_CUFFT32(cufftExecC2R(h->inv, h->k, h->s));
+    const pf5d_status e = elastic32(h, s);
+    if (e != PF5D_OK) return e;
   }
   pf5d_status st = launch_rate32(h, s);
   if (st != PF5D_OK) return st;
@@ -1313,18 +1357,22 @@ pf5d_status s32_launch_stage(Stepper32 *h, int32_t stage, void *stream) {
       k32_update<<<grid_for(h->npts, 256, 4), 256, 0, s>>>(h->up);
       PF5D_LAUNCHED();
       return PF5D_OK;
+    // 1D closed form: the whole elastic term is the FFT_FWD stage
     case PF5D_STAGE_FFT_FWD:
       PF5D_REQUIRE(h->d.elastic, PF5D_ERR_ARG, "elasticity is off");
+      if (h->closed1d) return elastic32(h, s);
       PF5D_CUFFT32(cufftSetStream(h->fwd, s));
       PF5D_CUFFT32(cufftExecR2C(h->fwd, h->s, h->k));
       return PF5D_OK;
     case PF5D_STAGE_BMUL:
       PF5D_REQUIRE(h->d.elastic, PF5D_ERR_ARG, "elasticity is off");
+      if (h->closed1d) return PF5D_OK;
       k32_bmul<<<grid_for(h->nk, 256), 256, 0, s>>>(h->k, h->bk, h->nk, &h->st->halt);
       PF5D_LAUNCHED();
       return PF5D_OK;
     case PF5D_STAGE_FFT_INV:
       PF5D_REQUIRE(h->d.elastic, PF5D_ERR_ARG, "elasticity is off");
+      if (h->closed1d) return PF5D_OK;
       PF5D_CUFFT32(cufftSetStream(h->inv, s));
       PF5D_CUFFT32(cufftExecC2R(h->inv, h->k, h->s));
       return PF5D_OK;
