@@ -25,6 +25,28 @@ void fft_destroy(FFTPair *p);
 pf5d_status fft_forward(FFTPair *p, double *s, cufftDoubleComplex *k, cudaStream_t stream);
 pf5d_status fft_inverse(FFTPair *p, cufftDoubleComplex *k, double *s, cudaStream_t stream);
 
+// 2D elastic term in three passes instead of cuFFT's four plus the multiply:
+// row D2Z over axis 1 (cuFFT, batched over the n0 rows), then ONE kernel per
+// group of spectrum columns that runs the length-n0 transform along axis 0,
+// multiplies by B(k)/N and runs the inverse transform back (k_colpass), then
+// row Z2D.  Used when n0 is a power of two in [8, 1024].
+struct ColPass2D {
+  cufftHandle rfwd = 0, rinv = 0;     // batched row transforms
+  int n0 = 0, nk1 = 0;                // rows, spectrum columns (n1/2 + 1)
+  double2 *tw = nullptr;              // exp(-2 pi i m / n0), m < n0
+  bool ready = false;
+};
+
+pf5d_status colpass_create(const int64_t *shape, ColPass2D *c);
+void colpass_destroy(ColPass2D *c);
+// s -> s' in place through k (scratch spectrum), bk = B(k)/N on the half grid.
+pf5d_status colpass_rows_forward(ColPass2D *c, double *s, cufftDoubleComplex *k,
+                                 cudaStream_t stream);
+pf5d_status colpass_columns(ColPass2D *c, cufftDoubleComplex *k, const double *bk,
+                            const unsigned *halt, cudaStream_t stream);
+pf5d_status colpass_rows_inverse(ColPass2D *c, cufftDoubleComplex *k, double *s,
+                                 cudaStream_t stream);
+
 struct Vec4 {
   double v[4];
 };

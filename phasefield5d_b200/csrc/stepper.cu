@@ -1679,6 +1679,8 @@ struct pf5d_stepper {
   double *diag_ws = nullptr;     // save-step partial rows + mean
   double *partial = nullptr;     // rate kernel block maxima
   bool closed1d = false;         // 1D elastic term in closed form (k_elastic1d)
+  ColPass2D colp;                // 2D elastic term: row transforms + one column kernel
+  bool use_colpass = false;
   double bn = 0.0, b0 = 0.0;     // its B(k): bn for every k != 0, b0 at k = 0
   double *save_x = nullptr;      // FP32C save steps: FP64 field, dX/dt, mu/M
   std::string kernels;           // text returned by pf5d_stepper_rate_kernels
@@ -2082,6 +2084,11 @@ pf5d_status elastic_stage(pf5d_stepper *h, cudaStream_t s) {
     return PF5D_OK;
   }
   pf5d_status st;
+  if (h->use_colpass) {
+    if ((st = colpass_rows_forward(&h->colp, h->s, h->k, s)) != PF5D_OK) return st;
+    if ((st = colpass_columns(&h->colp, h->k, h->bk, &h->st->halt, s)) != PF5D_OK) return st;
+    return colpass_rows_inverse(&h->colp, h->k, h->s, s);
+  }
   if ((st = fft_forward(&h->fft, h->s, h->k, s)) != PF5D_OK) return st;
   if ((st = launch_bmul(h->k, h->bk, h->fft.nk, &h->st->halt, s)) != PF5D_OK) return st;
   return fft_inverse(&h->fft, h->k, h->s, s);
@@ -2197,6 +2204,11 @@ pf5d_status pf5d_stepper_create(const pf5d_stepper_desc *desc, double *X, void *
   if (desc->elastic) {
     if ((st = fft_create(desc->dim, h->shape, &h->fft)) != PF5D_OK) return fail(st);
     if ((st = upload_bk_scaled(desc->bk, h->fft.nk, npts, &h->bk)) != PF5D_OK) return fail(st);
+    const int64_t n0 = h->shape[0];
+    if (desc->dim == 2 && n0 >= 8 && n0 <= 1024 && (n0 & (n0 - 1)) == 0) {
+      h->use_colpass = colpass_create(h->shape, &h->colp) == PF5D_OK;
+      if (!h->use_colpass) colpass_destroy(&h->colp);
+    }
     if (cudaMalloc(&h->s, npts * sizeof(double)) != cudaSuccess ||
         cudaMalloc(&h->k, h->fft.nk * sizeof(cufftDoubleComplex)) != cudaSuccess) {
       set_error("device allocation failed");
@@ -2520,14 +2532,17 @@ pf5d_status pf5d_stepper_launch_stage(pf5d_stepper *h, int32_t stage, void *stre
     case PF5D_STAGE_FFT_FWD:
       PF5D_REQUIRE(h->d.elastic, PF5D_ERR_ARG, "elasticity is off");
       if (h->closed1d) return elastic_stage(h, s);
+      if (h->use_colpass) return colpass_rows_forward(&h->colp, h->s, h->k, s);
       return fft_forward(&h->fft, h->s, h->k, s);
     case PF5D_STAGE_BMUL:
       PF5D_REQUIRE(h->d.elastic, PF5D_ERR_ARG, "elasticity is off");
       if (h->closed1d) return PF5D_OK;
+      if (h->use_colpass) return colpass_columns(&h->colp, h->k, h->bk, &h->st->halt, s);
       return launch_bmul(h->k, h->bk, h->fft.nk, &h->st->halt, s);
     case PF5D_STAGE_FFT_INV:
       PF5D_REQUIRE(h->d.elastic, PF5D_ERR_ARG, "elasticity is off");
       if (h->closed1d) return PF5D_OK;
+      if (h->use_colpass) return colpass_rows_inverse(&h->colp, h->k, h->s, s);
       return fft_inverse(&h->fft, h->k, h->s, s);
     default:
       set_error("unknown stage %d", stage);
@@ -2549,6 +2564,7 @@ pf5d_status pf5d_stepper_destroy(pf5d_stepper *h) {
   cudaFree(h->s);
   cudaFree(h->k);
   cudaFree(h->bk);
+  colpass_destroy(&h->colp);
   cudaFree(h->st);
   if (h->cap) cudaStreamDestroy(h->cap);
   delete h;
