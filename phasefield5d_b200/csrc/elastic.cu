@@ -73,8 +73,8 @@ pf5d_status fft_inverse(FFTPair *p, cufftDoubleComplex *k, double *s, cudaStream
 // inverse exp(+2 pi i jk/N0), both unnormalised like cuFFT's (the 1/N is
 // in B).
 // ------------------------------------------------------------------------
-constexpr int kColGroup = 2;
-constexpr int kColThreads = 128;
+constexpr int kColGroup = 1;
+constexpr int kColThreads = 64;
 
 __device__ __forceinline__ double2 cmul(double2 a, double2 b) {
   return make_double2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
