@@ -74,7 +74,7 @@ pf5d_status fft_inverse(FFTPair *p, cufftDoubleComplex *k, double *s, cudaStream
 // in B).
 // ------------------------------------------------------------------------
 constexpr int kColGroup = 1;
-constexpr int kColThreads = 64;
+constexpr int kColThreads = 256;
 
 __device__ __forceinline__ double2 cmul(double2 a, double2 b) {
   return make_double2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
