@@ -225,10 +225,13 @@ pf5d_status pf5d_stepper_mass(pf5d_stepper *h, double *mean_out, void *stream);
  * stepper's state exactly as that stage does inside a step. */
 #define PF5D_STAGE_RATE 0        /* rate kernel(s) (mu/M + flux divergence) and the dt controller */
 #define PF5D_STAGE_UPDATE 1      /* update, clamp, next misfit, OOB test       */
-#define PF5D_STAGE_FFT_FWD 2     /* cuFFT D2Z of the misfit; 1D solves up to 16384 points:
-                                    the whole elastic term in closed form        */
-#define PF5D_STAGE_BMUL 3        /* B(k) multiply (nothing in the 1D closed form) */
-#define PF5D_STAGE_FFT_INV 4     /* cuFFT Z2D (nothing in the 1D closed form)   */
+#define PF5D_STAGE_FFT_FWD 2     /* cuFFT D2Z of the misfit (2D with a power-of-two
+                                    axis 0 up to 1024: the row D2Z); 1D solves up to
+                                    16384 points: the whole elastic term in closed form */
+#define PF5D_STAGE_BMUL 3        /* B(k) multiply (2D column pass: axis-0 transform,
+                                    multiply, inverse; nothing in the 1D closed form) */
+#define PF5D_STAGE_FFT_INV 4     /* cuFFT Z2D (2D column pass: the row Z2D; nothing in
+                                    the 1D closed form)                          */
 pf5d_status pf5d_stepper_launch_stage(pf5d_stepper *h, int32_t stage, void *stream);
 /* Autotuner: time every rate-kernel variant (plane tile shape x resident
  * blocks per SM, ...) on this solve; the plain FP64 form then times the
