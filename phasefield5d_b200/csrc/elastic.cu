@@ -76,21 +76,36 @@ pf5d_status fft_inverse(FFTPair *p, cufftDoubleComplex *k, double *s, cudaStream
 constexpr int kColGroup = 1;
 constexpr int kColThreads = 256;
 
-__device__ __forceinline__ double2 cmul(double2 a, double2 b) {
-  return make_double2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
-}
-__device__ __forceinline__ double2 cadd(double2 a, double2 b) { return make_double2(a.x + b.x, a.y + b.y); }
-__device__ __forceinline__ double2 csub(double2 a, double2 b) { return make_double2(a.x - b.x, a.y - b.y); }
-// times -i (forward) or +i (inverse)
-template <bool INV>
-__device__ __forceinline__ double2 crot(double2 a) {
-  return INV ? make_double2(-a.y, a.x) : make_double2(a.y, -a.x);
+// complex type traits of the column pass (FP64 double2, FP32c float2)
+template <typename C> struct CT;
+template <> struct CT<double2> { using R = double; };
+template <> struct CT<float2> { using R = float; };
+template <typename C>
+__device__ __forceinline__ C cmk(typename CT<C>::R a, typename CT<C>::R b) {
+  C c;
+  c.x = a;
+  c.y = b;
+  return c;
 }
 
-template <bool INV>
-__device__ __forceinline__ void dft4(double2 *u) {
-  const double2 c0 = cadd(u[0], u[2]), c1 = cadd(u[1], u[3]);
-  const double2 d0 = csub(u[0], u[2]), d1 = crot<INV>(csub(u[1], u[3]));
+template <typename C>
+__device__ __forceinline__ C cmul(C a, C b) {
+  return cmk<C>(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
+}
+template <typename C>
+__device__ __forceinline__ C cadd(C a, C b) { return cmk<C>(a.x + b.x, a.y + b.y); }
+template <typename C>
+__device__ __forceinline__ C csub(C a, C b) { return cmk<C>(a.x - b.x, a.y - b.y); }
+// times -i (forward) or +i (inverse)
+template <typename C, bool INV>
+__device__ __forceinline__ C crot(C a) {
+  return INV ? cmk<C>(-a.y, a.x) : cmk<C>(a.y, -a.x);
+}
+
+template <typename C, bool INV>
+__device__ __forceinline__ void dft4(C *u) {
+  const C c0 = cadd(u[0], u[2]), c1 = cadd(u[1], u[3]);
+  const C d0 = csub(u[0], u[2]), d1 = crot<C, INV>(csub(u[1], u[3]));
   u[0] = cadd(c0, c1);
   u[1] = cadd(d0, d1);
   u[2] = csub(c0, c1);
@@ -99,20 +114,20 @@ __device__ __forceinline__ void dft4(double2 *u) {
 
 // Radix-8 by decimation in frequency: two length-4 transforms of the sums
 // and of the twiddled differences (W8^n, n < 4).
-template <bool INV>
-__device__ __forceinline__ void dft8(double2 *v) {
-  constexpr double h = 0.70710678118654752440;
-  double2 a[4], b[4];
+template <typename C, bool INV>
+__device__ __forceinline__ void dft8(C *v) {
+  constexpr typename CT<C>::R h = (typename CT<C>::R)0.70710678118654752440;
+  C a[4], b[4];
 #pragma unroll
   for (int n = 0; n < 4; ++n) {
     a[n] = cadd(v[n], v[n + 4]);
     b[n] = csub(v[n], v[n + 4]);
   }
-  b[1] = cmul(b[1], make_double2(h, INV ? h : -h));
-  b[2] = crot<INV>(b[2]);
-  b[3] = cmul(b[3], make_double2(-h, INV ? h : -h));
-  dft4<INV>(a);
-  dft4<INV>(b);
+  b[1] = cmul(b[1], cmk<C>(h, INV ? h : -h));
+  b[2] = crot<C, INV>(b[2]);
+  b[3] = cmul(b[3], cmk<C>(-h, INV ? h : -h));
+  dft4<C, INV>(a);
+  dft4<C, INV>(b);
 #pragma unroll
   for (int k = 0; k < 4; ++k) {
     v[2 * k] = a[k];
@@ -120,14 +135,14 @@ __device__ __forceinline__ void dft8(double2 *v) {
   }
 }
 
-template <int R, bool INV>
-__device__ __forceinline__ void dftr(double2 *v) {
+template <typename C, int R, bool INV>
+__device__ __forceinline__ void dftr(C *v) {
   if constexpr (R == 8) {
-    dft8<INV>(v);
+    dft8<C, INV>(v);
   } else if constexpr (R == 4) {
-    dft4<INV>(v);
+    dft4<C, INV>(v);
   } else {
-    const double2 a = v[0];
+    const C a = v[0];
     v[0] = cadd(a, v[1]);
     v[1] = csub(a, v[1]);
   }
@@ -135,27 +150,27 @@ __device__ __forceinline__ void dftr(double2 *v) {
 
 // One Stockham stage of radix R over span ns, x -> y, then a barrier.
 // tw[t] = exp(-2 pi i t / N0), t < N0.
-template <int N0, int R, bool INV>
-__device__ __forceinline__ void stockham_stage(const double2 *x, double2 *y,
-                                               const double2 *__restrict__ tw, int ns, int tid) {
+template <typename C, int N0, int R, bool INV>
+__device__ __forceinline__ void stockham_stage(const C *x, C *y,
+                                               const C *__restrict__ tw, int ns, int tid) {
   constexpr int Q = N0 / R;
   for (int b = tid; b < kColGroup * Q; b += kColThreads) {
     const int cc = b / Q, j = b - cc * Q;
-    const double2 *xc = x + cc * N0;
-    double2 *yc = y + cc * N0;
+    const C *xc = x + cc * N0;
+    C *yc = y + cc * N0;
     const int m = j & (ns - 1);
     const int step = m * (N0 / (R * ns));
-    double2 v[R];
+    C v[R];
 #pragma unroll
     for (int r = 0; r < R; ++r) {
       v[r] = xc[j + r * Q];
       if (r > 0) {
-        double2 w = tw[r * step];
+        C w = tw[r * step];
         if (INV) w.y = -w.y;
         v[r] = cmul(v[r], w);
       }
     }
-    dftr<R, INV>(v);
+    dftr<C, R, INV>(v);
     const int d = (j - m) * R + m;
 #pragma unroll
     for (int r = 0; r < R; ++r) yc[d + r * ns] = v[r];
@@ -163,81 +178,97 @@ __device__ __forceinline__ void stockham_stage(const double2 *x, double2 *y,
   __syncthreads();
 }
 
-template <int N0, bool INV>
-__device__ __forceinline__ double2 *stockham(double2 *x, double2 *y, const double2 *__restrict__ tw,
+template <typename C, int N0, bool INV>
+__device__ __forceinline__ C *stockham(C *x, C *y, const C *__restrict__ tw,
                                              int tid) {
   int ns = 1;
 #pragma unroll 1
   for (; ns * 8 <= N0; ns *= 8) {
-    stockham_stage<N0, 8, INV>(x, y, tw, ns, tid);
-    double2 *t = x;
+    stockham_stage<C, N0, 8, INV>(x, y, tw, ns, tid);
+    C *t = x;
     x = y;
     y = t;
   }
   if (ns < N0) {
-    if (N0 / ns >= 4) stockham_stage<N0, 4, INV>(x, y, tw, ns, tid);
-    else stockham_stage<N0, 2, INV>(x, y, tw, ns, tid);
-    double2 *t = x;
+    if (N0 / ns >= 4) stockham_stage<C, N0, 4, INV>(x, y, tw, ns, tid);
+    else stockham_stage<C, N0, 2, INV>(x, y, tw, ns, tid);
+    C *t = x;
     x = y;
     y = t;
   }
   return x;
 }
 
-template <int N0>
+template <typename C, int N0>
 __global__ void __launch_bounds__(kColThreads)
-    k_colpass(cufftDoubleComplex *__restrict__ k, const double *__restrict__ bk, int nk1,
-              const double2 *__restrict__ tw, const unsigned *halt) {
-  extern __shared__ double2 cbuf[];                  // [2][kColGroup][N0]
+    k_colpass(C *__restrict__ k, const typename CT<C>::R *__restrict__ bk, int nk1,
+              const C *__restrict__ tw, const unsigned *halt) {
+  extern __shared__ __align__(16) unsigned char craw[];
+  C *cbuf = reinterpret_cast<C *>(craw);             // [2][kColGroup][N0]
   if (halt && *halt) return;
   const int tid = threadIdx.x, c0 = blockIdx.x * kColGroup;
-  double2 *a = cbuf, *b = cbuf + kColGroup * N0;
-  double2 *kk = reinterpret_cast<double2 *>(k);
+  C *a = cbuf, *b = cbuf + kColGroup * N0;
+  C *kk = k;
   for (int e = tid; e < kColGroup * N0; e += kColThreads) {
     const int r = e / kColGroup, cc = e - r * kColGroup, c = c0 + cc;
-    a[cc * N0 + r] = c < nk1 ? kk[(int64_t)r * nk1 + c] : make_double2(0.0, 0.0);
+    a[cc * N0 + r] = c < nk1 ? kk[(int64_t)r * nk1 + c] : cmk<C>(0, 0);
   }
   __syncthreads();
-  double2 *f = stockham<N0, false>(a, b, tw, tid);
-  double2 *g = f == a ? b : a;
+  C *f = stockham<C, N0, false>(a, b, tw, tid);
+  C *g = f == a ? b : a;
   for (int e = tid; e < kColGroup * N0; e += kColThreads) {
     const int cc = e / N0, r = e - cc * N0, c = c0 + cc;
-    const double m = c < nk1 ? bk[(int64_t)r * nk1 + c] : 0.0;
-    double2 v = f[e];
+    const typename CT<C>::R m = c < nk1 ? bk[(int64_t)r * nk1 + c] : 0;
+    C v = f[e];
     v.x = v.x * m;
     v.y = v.y * m;
     f[e] = v;
   }
   __syncthreads();
-  f = stockham<N0, true>(f, g, tw, tid);
+  f = stockham<C, N0, true>(f, g, tw, tid);
   for (int e = tid; e < kColGroup * N0; e += kColThreads) {
     const int r = e / kColGroup, cc = e - r * kColGroup, c = c0 + cc;
     if (c < nk1) kk[(int64_t)r * nk1 + c] = f[cc * N0 + r];
   }
 }
 
-pf5d_status colpass_create(const int64_t *shape, ColPass2D *c) {
+template <typename C>
+static pf5d_status colpass_dispatch(const ColPass2D *c, C *k, const typename CT<C>::R *bk,
+                                    const C *tw, const unsigned *halt, cudaStream_t stream);
+
+pf5d_status colpass_create(const int64_t *shape, ColPass2D *c, bool fp32) {
   const int64_t n0 = shape[0], n1 = shape[1];
   PF5D_REQUIRE(n0 >= 8 && n0 <= 1024 && (n0 & (n0 - 1)) == 0 && n1 >= 2, PF5D_ERR_ARG,
                "column pass needs a power-of-two axis 0 in [8, 1024]");
   c->n0 = (int)n0;
   c->nk1 = (int)(n1 / 2 + 1);
+  c->fp32 = fp32;
   long long n[1] = {(long long)n1};
   size_t ws = 0;
   PF5D_CUFFT(cufftCreate(&c->rfwd));
-  PF5D_CUFFT(cufftMakePlanMany64(c->rfwd, 1, n, nullptr, 1, 0, nullptr, 1, 0, CUFFT_D2Z, n0, &ws));
+  PF5D_CUFFT(cufftMakePlanMany64(c->rfwd, 1, n, nullptr, 1, 0, nullptr, 1, 0,
+                                 fp32 ? CUFFT_R2C : CUFFT_D2Z, n0, &ws));
   PF5D_CUFFT(cufftCreate(&c->rinv));
-  PF5D_CUFFT(cufftMakePlanMany64(c->rinv, 1, n, nullptr, 1, 0, nullptr, 1, 0, CUFFT_Z2D, n0, &ws));
+  PF5D_CUFFT(cufftMakePlanMany64(c->rinv, 1, n, nullptr, 1, 0, nullptr, 1, 0,
+                                 fp32 ? CUFFT_C2R : CUFFT_Z2D, n0, &ws));
   c->ready = true;
+  // exp(-2 pi i m / n0) in FP64, rounded once for the FP32 form
   std::vector<double2> tw(n0);
+  std::vector<float2> tw32(n0);
   const double pi = 3.14159265358979323846;
   for (int64_t m = 0; m < n0; ++m) {
     const double ang = 2.0 * pi * (double)m / (double)n0;
     tw[m] = make_double2(std::cos(ang), -std::sin(ang));
+    tw32[m] = make_float2((float)tw[m].x, (float)tw[m].y);
+  }
+  if (fp32) {
+    PF5D_CUDA(cudaMalloc(&c->tw32, tw32.size() * sizeof(float2)));
+    PF5D_CUDA(cudaMemcpy(c->tw32, tw32.data(), tw32.size() * sizeof(float2), cudaMemcpyHostToDevice));
+    return colpass_dispatch<float2>(c, nullptr, nullptr, nullptr, nullptr, nullptr);
   }
   PF5D_CUDA(cudaMalloc(&c->tw, tw.size() * sizeof(double2)));
   PF5D_CUDA(cudaMemcpy(c->tw, tw.data(), tw.size() * sizeof(double2), cudaMemcpyHostToDevice));
-  return colpass_columns(c, nullptr, nullptr, nullptr, nullptr);   // shared-memory attribute
+  return colpass_dispatch<double2>(c, nullptr, nullptr, nullptr, nullptr, nullptr);
 }
 
 void colpass_destroy(ColPass2D *c) {
@@ -246,7 +277,9 @@ void colpass_destroy(ColPass2D *c) {
     cufftDestroy(c->rinv);
   }
   cudaFree(c->tw);
+  cudaFree(c->tw32);
   c->tw = nullptr;
+  c->tw32 = nullptr;
   c->ready = false;
 }
 
@@ -264,33 +297,56 @@ pf5d_status colpass_rows_inverse(ColPass2D *c, cufftDoubleComplex *k, double *s,
   return PF5D_OK;
 }
 
-template <int N0>
-static pf5d_status launch_colpass(ColPass2D *c, cufftDoubleComplex *k, const double *bk,
-                                  const unsigned *halt, cudaStream_t stream) {
-  const int smem = 2 * kColGroup * N0 * (int)sizeof(double2);
+template <typename C, int N0>
+static pf5d_status launch_colpass(const ColPass2D *c, C *k, const typename CT<C>::R *bk,
+                                  const C *tw, const unsigned *halt, cudaStream_t stream) {
+  const int smem = 2 * N0 * (int)sizeof(C);
   if (!k) {                          // set-up call from colpass_create
-    PF5D_CUDA(cudaFuncSetAttribute(k_colpass<N0>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+    PF5D_CUDA(cudaFuncSetAttribute(k_colpass<C, N0>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                   smem));
     return PF5D_OK;
   }
-  const unsigned nb = (unsigned)((c->nk1 + kColGroup - 1) / kColGroup);
-  k_colpass<N0><<<nb, kColThreads, smem, stream>>>(k, bk, c->nk1, c->tw, halt);
+  k_colpass<C, N0><<<(unsigned)c->nk1, kColThreads, smem, stream>>>(k, bk, c->nk1, tw, halt);
   PF5D_LAUNCHED();
   return PF5D_OK;
 }
 
-pf5d_status colpass_columns(ColPass2D *c, cufftDoubleComplex *k, const double *bk,
-                            const unsigned *halt, cudaStream_t stream) {
+template <typename C>
+static pf5d_status colpass_dispatch(const ColPass2D *c, C *k, const typename CT<C>::R *bk,
+                                    const C *tw, const unsigned *halt, cudaStream_t stream) {
   switch (c->n0) {
-    case 8: return launch_colpass<8>(c, k, bk, halt, stream);
-    case 16: return launch_colpass<16>(c, k, bk, halt, stream);
-    case 32: return launch_colpass<32>(c, k, bk, halt, stream);
-    case 64: return launch_colpass<64>(c, k, bk, halt, stream);
-    case 128: return launch_colpass<128>(c, k, bk, halt, stream);
-    case 256: return launch_colpass<256>(c, k, bk, halt, stream);
-    case 512: return launch_colpass<512>(c, k, bk, halt, stream);
-    case 1024: return launch_colpass<1024>(c, k, bk, halt, stream);
+    case 8: return launch_colpass<C, 8>(c, k, bk, tw, halt, stream);
+    case 16: return launch_colpass<C, 16>(c, k, bk, tw, halt, stream);
+    case 32: return launch_colpass<C, 32>(c, k, bk, tw, halt, stream);
+    case 64: return launch_colpass<C, 64>(c, k, bk, tw, halt, stream);
+    case 128: return launch_colpass<C, 128>(c, k, bk, tw, halt, stream);
+    case 256: return launch_colpass<C, 256>(c, k, bk, tw, halt, stream);
+    case 512: return launch_colpass<C, 512>(c, k, bk, tw, halt, stream);
+    case 1024: return launch_colpass<C, 1024>(c, k, bk, tw, halt, stream);
     default: set_error("column pass: unsupported n0 %d", c->n0); return PF5D_ERR_ARG;
   }
+}
+
+pf5d_status colpass_columns(ColPass2D *c, cufftDoubleComplex *k, const double *bk,
+                            const unsigned *halt, cudaStream_t stream) {
+  return colpass_dispatch<double2>(c, reinterpret_cast<double2 *>(k), bk, c->tw, halt, stream);
+}
+
+pf5d_status colpass_columns32(ColPass2D *c, cufftComplex *k, const float *bk,
+                              const unsigned *halt, cudaStream_t stream) {
+  return colpass_dispatch<float2>(c, reinterpret_cast<float2 *>(k), bk, c->tw32, halt, stream);
+}
+
+pf5d_status colpass_rows_forward32(ColPass2D *c, float *s, cufftComplex *k, cudaStream_t stream) {
+  PF5D_CUFFT(cufftSetStream(c->rfwd, stream));
+  PF5D_CUFFT(cufftExecR2C(c->rfwd, s, k));
+  return PF5D_OK;
+}
+
+pf5d_status colpass_rows_inverse32(ColPass2D *c, cufftComplex *k, float *s, cudaStream_t stream) {
+  PF5D_CUFFT(cufftSetStream(c->rinv, stream));
+  PF5D_CUFFT(cufftExecC2R(c->rinv, k, s));
+  return PF5D_OK;
 }
 
 __global__ void k_misfit(const double *__restrict__ X, int64_t npts, Vec4 x0, Vec4 l,

@@ -33,11 +33,13 @@ pf5d_status fft_inverse(FFTPair *p, cufftDoubleComplex *k, double *s, cudaStream
 struct ColPass2D {
   cufftHandle rfwd = 0, rinv = 0;     // batched row transforms
   int n0 = 0, nk1 = 0;                // rows, spectrum columns (n1/2 + 1)
-  double2 *tw = nullptr;              // exp(-2 pi i m / n0), m < n0
+  double2 *tw = nullptr;              // exp(-2 pi i m / n0), m < n0 (FP64 form)
+  float2 *tw32 = nullptr;             // the same rounded to FP32 (FP32c form)
+  bool fp32 = false;                  // FP32c: R2C / C2R rows, float2 spectrum
   bool ready = false;
 };
 
-pf5d_status colpass_create(const int64_t *shape, ColPass2D *c);
+pf5d_status colpass_create(const int64_t *shape, ColPass2D *c, bool fp32);
 void colpass_destroy(ColPass2D *c);
 // s -> s' in place through k (scratch spectrum), bk = B(k)/N on the half grid.
 pf5d_status colpass_rows_forward(ColPass2D *c, double *s, cufftDoubleComplex *k,
@@ -46,6 +48,11 @@ pf5d_status colpass_columns(ColPass2D *c, cufftDoubleComplex *k, const double *b
                             const unsigned *halt, cudaStream_t stream);
 pf5d_status colpass_rows_inverse(ColPass2D *c, cufftDoubleComplex *k, double *s,
                                  cudaStream_t stream);
+// The FP32c form's passes (float field, cufftComplex spectrum, B(k)/N in FP32).
+pf5d_status colpass_rows_forward32(ColPass2D *c, float *s, cufftComplex *k, cudaStream_t stream);
+pf5d_status colpass_columns32(ColPass2D *c, cufftComplex *k, const float *bk,
+                              const unsigned *halt, cudaStream_t stream);
+pf5d_status colpass_rows_inverse32(ColPass2D *c, cufftComplex *k, float *s, cudaStream_t stream);
 
 struct Vec4 {
   double v[4];

@@ -29,6 +29,7 @@
 #include <cufft.h>
 
 #include "pf5d_device.cuh"
+#include "pf5d_fft.h"
 #include "pf5d_fp32c.h"
 #include "pf5d_fp32c.cuh"
 #include "pf5d_host.h"
@@ -878,6 +879,8 @@ const std::vector<Variant32> &variants32() {
 struct Stepper32 {
   pf5d_stepper_desc d{};
   bool closed1d = false;         // 1D elastic term in closed form (k32_elastic1d)
+  ColPass2D colp;                // 2D elastic term: row transforms + one column kernel
+  bool use_colpass = false;
   double bn = 0.0, b0 = 0.0;     // its B(k): bn for every k != 0, b0 at k = 0
   int64_t shape[3] = {1, 1, 1};
   int64_t npts = 0, nk = 0;
@@ -978,6 +981,12 @@ static pf5d_status elastic32(Stepper32 *h, cudaStream_t s) {
     PF5D_CUDA(launch_pdl(k32_elastic1d, dim3(1), dim3(kElastic1dThreads32), 0, s, h->s, h->npts,
                          h->bn, h->b0, (const unsigned *)&h->st->halt));
     return PF5D_OK;
+  }
+  if (h->use_colpass) {
+    pf5d_status st;
+    if ((st = colpass_rows_forward32(&h->colp, h->s, h->k, s)) != PF5D_OK) return st;
+    if ((st = colpass_columns32(&h->colp, h->k, h->bk, &h->st->halt, s)) != PF5D_OK) return st;
+    return colpass_rows_inverse32(&h->colp, h->k, h->s, s);
   }
     PF5D_CUFFT32(cufftSetStream(h->fwd, s));
     PF5D_CUFFT32(cufftExecR2C(h->fwd, h->s, h->k));
@@ -1088,6 +1097,11 @@ pf5d_status s32_create(const pf5d_stepper_desc *desc, const double *X_init, void
         cudaMemcpy(h->bk, b.data(), h->nk * sizeof(float), cudaMemcpyHostToDevice) != cudaSuccess) {
       set_error("device allocation failed");
       return fail(PF5D_ERR_CUDA);
+    }
+    const int64_t n0 = h->shape[0];
+    if (desc->dim == 2 && n0 >= 8 && n0 <= 1024 && (n0 & (n0 - 1)) == 0) {
+      h->use_colpass = colpass_create(h->shape, &h->colp, true) == PF5D_OK;
+      if (!h->use_colpass) colpass_destroy(&h->colp);
     }
   }
   Rate32 &P = h->rp;
@@ -1361,18 +1375,21 @@ pf5d_status s32_launch_stage(Stepper32 *h, int32_t stage, void *stream) {
     case PF5D_STAGE_FFT_FWD:
       PF5D_REQUIRE(h->d.elastic, PF5D_ERR_ARG, "elasticity is off");
       if (h->closed1d) return elastic32(h, s);
+      if (h->use_colpass) return colpass_rows_forward32(&h->colp, h->s, h->k, s);
       PF5D_CUFFT32(cufftSetStream(h->fwd, s));
       PF5D_CUFFT32(cufftExecR2C(h->fwd, h->s, h->k));
       return PF5D_OK;
     case PF5D_STAGE_BMUL:
       PF5D_REQUIRE(h->d.elastic, PF5D_ERR_ARG, "elasticity is off");
       if (h->closed1d) return PF5D_OK;
+      if (h->use_colpass) return colpass_columns32(&h->colp, h->k, h->bk, &h->st->halt, s);
       k32_bmul<<<grid_for(h->nk, 256), 256, 0, s>>>(h->k, h->bk, h->nk, &h->st->halt);
       PF5D_LAUNCHED();
       return PF5D_OK;
     case PF5D_STAGE_FFT_INV:
       PF5D_REQUIRE(h->d.elastic, PF5D_ERR_ARG, "elasticity is off");
       if (h->closed1d) return PF5D_OK;
+      if (h->use_colpass) return colpass_rows_inverse32(&h->colp, h->k, h->s, s);
       PF5D_CUFFT32(cufftSetStream(h->inv, s));
       PF5D_CUFFT32(cufftExecC2R(h->inv, h->k, h->s));
       return PF5D_OK;
@@ -1396,6 +1413,7 @@ void s32_destroy(Stepper32 *h) {
   cudaFree(h->dX);
   cudaFree(h->s);
   cudaFree(h->bk);
+  colpass_destroy(&h->colp);
   cudaFree(h->k);
   cudaFree(h->st);
   cudaFree(h->mass_ws);

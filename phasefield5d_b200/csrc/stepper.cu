@@ -2206,7 +2206,7 @@ pf5d_status pf5d_stepper_create(const pf5d_stepper_desc *desc, double *X, void *
     if ((st = upload_bk_scaled(desc->bk, h->fft.nk, npts, &h->bk)) != PF5D_OK) return fail(st);
     const int64_t n0 = h->shape[0];
     if (desc->dim == 2 && n0 >= 8 && n0 <= 1024 && (n0 & (n0 - 1)) == 0) {
-      h->use_colpass = colpass_create(h->shape, &h->colp) == PF5D_OK;
+      h->use_colpass = colpass_create(h->shape, &h->colp, false) == PF5D_OK;
       if (!h->use_colpass) colpass_destroy(&h->colp);
     }
     if (cudaMalloc(&h->s, npts * sizeof(double)) != cudaSuccess ||
