@@ -275,8 +275,10 @@ pf5d_status pf5d_stepper_step_save(pf5d_stepper *h, pf5d_save_diag *out, void *s
  * pf5d_stepper_set_variant are 0 .. count-1); 0 for a null stepper. */
 int32_t pf5d_stepper_variant_count(const pf5d_stepper *h);
 /* Kernels of this library that one step launches with the current variant
- * (rate kernel(s), dt controller, update, and the B(k) multiply when
- * elasticity is on; cuFFT's own kernels not counted); 0 for a null stepper. */
+ * (rate kernel(s), dt controller, update, and when elasticity is on the B(k)
+ * multiply -- the column kernel in 2D with a power-of-two axis 0, the
+ * closed-form kernel in 1D; cuFFT's own kernels not counted); 0 for a null
+ * stepper. */
 int32_t pf5d_stepper_launches_per_step(const pf5d_stepper *h);
 /* The kernel instances one rate stage of the current variant launches, as
  * profilers name them ("k_rate_tile2d<32, 8, 2, 1, 1, 0, 352, 1, 0> +
