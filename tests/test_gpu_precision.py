@@ -34,6 +34,23 @@ def test_fp32c_2d_512_vs_fp64(torch_cuda):
     _check(rep)
 
 
+@pytest.mark.parametrize("shape", [(8, 30), (16, 24), (128, 18), (1024, 6)])
+def test_fp32c_column_pass_lengths_vs_fp64(torch_cuda, shape):
+    """The FP32 column kernel (float2 spectrum) at transform lengths with
+    each kind of final radix stage, against the plain FP64 form: the field
+    within the precision target.  (Mass conservation belongs to the flux
+    form, not to the elastic transform; its bound is checked on the named
+    workloads above.)"""
+    from phasefield5d_b200 import workload as W
+    from phasefield5d_b200.precision import compare_forms
+    cfg = W.SolveConfig(system_dim=2, initial_composition=(0.1, 0.2, 0.2, 0.25), resolution=0.05,
+                        kappa_value=5e-16, mw=4, ppw=16, shape=shape, adaptive=True, n_k=2000,
+                        fluctuation=3e-2)
+    rep = compare_forms(W.build_problem(cfg), 200)
+    assert not rep["halted"], rep
+    assert rep["max_rel_err_X"] <= FIELD_RTOL_FP32C, rep
+
+
 def test_fp32c_1d_1280_fixed_dt_vs_fp64(torch_cuda):
     from phasefield5d_b200 import workload as W
     from phasefield5d_b200.precision import compare_forms

@@ -171,6 +171,30 @@ def test_odd_shapes_vs_oracle(torch_cuda, shape, n):
     gpu.close()
 
 
+@pytest.mark.parametrize("shape", [(8, 30), (16, 24), (32, 40), (64, 22), (128, 18), (256, 10),
+                                   (1024, 6)])
+def test_column_pass_lengths_vs_oracle(torch_cuda, shape):
+    """2D fields whose axis 0 is a power of two run the elastic term through
+    cuFFT's row transforms and the column kernel (mixed-radix transform
+    along axis 0, B(k)/N, inverse): every transform length from 8 to 1024
+    (radix-8 stages with a radix-4 or radix-2 tail) against the oracle's
+    pocketfft path, 25 steps at the parity tolerance."""
+    from oracle.oracle import OracleStepper
+    from phasefield5d_b200 import workload as W
+    from phasefield5d_b200.stepper import Stepper
+    cfg = W.SolveConfig(system_dim=2, initial_composition=(0.1, 0.2, 0.2, 0.25), resolution=0.05,
+                        kappa_value=5e-16, mw=4, ppw=16, shape=shape, adaptive=True, n_k=2000,
+                        fluctuation=3e-2)
+    prob = W.build_problem(cfg)
+    gpu = Stepper.from_problem(prob)
+    gpu.run(25)
+    ref = OracleStepper.from_problem(prob)
+    ref.run(25)
+    r_field, r_dev = _rel(gpu.X.cpu().numpy(), ref.X, prob.X0)
+    assert r_field <= FIELD_RTOL, f"{shape}: field rel {r_field:.2e} (X-X0 rel {r_dev:.2e})"
+    gpu.close()
+
+
 def test_nearest_row_fallback_inside_step(torch_cuda):
     """Composition straddling the linear-region threshold: part of the field
     takes the nearest-row branch every step."""
